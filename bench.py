@@ -1,0 +1,313 @@
+"""Benchmark: synaptic events/s of Brunel's model A at config 1's size
+(N_E 10,000, N_I 2,500, C_E 1,000, C_I 250: 15.6M synapses, per-link delays
+of 1-20 steps, dt 0.1 ms), stepped by the fused CUDA step kernel.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl naer2_b200|reference]
+
+One bench step = 1,000 simulation steps (100 ms of network time); the
+config's 10,000 steps are 10 bench steps (the default K). Printed: one JSON
+line (rank 0).
+  value   events delivered in the timed steps / device time (CUDA events on
+          the runtime's stream, L2 flushed before every timed step), summed
+          over ranks, time the max over ranks
+  e2e     the same metric through the public API with host buffers: every
+          step copies the network state in from pinned host memory, runs
+          Network.step, and reads the spike raster and state back
+  roofline  the step kernel's algorithmic bytes (9 B per synaptic event +
+          16 B per neuron per step) over its average launch time, against the
+          measured HBM copy bandwidth
+  cpu_baseline  the oracle (a C restatement of the reference's time-driven
+          loop, all host threads) on a bounded sample of the same network
+--impl reference times that CPU implementation alone (rank 0; others exit).
+Multi-GPU: independent replicas (one network per rank, its own seed).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import subprocess
+import sys
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SIM_STEPS_PER_STEP = 1000
+BYTES_PER_EVENT = 9  # int32 target + int8 delay + fp32 weight
+BYTES_PER_NEURON_STEP = 16  # V read + write, arrival slot read + clear
+METRIC = "synaptic events/s"
+UNIT = "events/s"
+WORKLOAD = "brunel_A_config1"
+
+
+def measured_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def config(n_gpus: int) -> dict:
+    return {"workload": WORKLOAD, "neurons": 12500, "synapses": 15_625_000, "delays_steps": "U{1..20}", "dt_ms": 0.1,
+            "sim_steps_per_step": SIM_STEPS_PER_STEP, "l2": "flushed before every timed step (256 MiB write)",
+            "parallelism": f"replicas x{n_gpus}" if n_gpus > 1 else "single GPU"}
+
+
+class Clocks:
+    """nvidia-smi samples (200 ms) while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in getattr(self, "lines", []):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_sample(desc, states, target_s: float = 12.0, threads: int = 0) -> dict:
+    """The oracle on the host cores: a bounded sample of the same network (first steps from the same state)."""
+    import oracle
+
+    used = oracle.set_threads(threads)
+    probe = 50
+    t0 = time.perf_counter()
+    _, ev = oracle.run(desc, states, 0, probe, record=False)
+    t_probe = time.perf_counter() - t0
+    steps = max(50, min(10_000, int(probe * target_s / max(t_probe, 1e-3))))
+    t0 = time.perf_counter()
+    _, ev2 = oracle.run(desc, states, probe, steps, record=False)
+    el = time.perf_counter() - t0
+    return {"value": ev2 / el, "unit": UNIT, "cores": used, "kind": "port",
+            "sample": f"{WORKLOAD}: simulation steps {probe}-{probe + steps} ({steps * 0.1:.0f} ms of network time, "
+                      f"{ev2} events) in {el:.1f} s, C oracle, {used} OpenMP threads, nproc {os.cpu_count()}",
+            "realtime_factor": el / (steps * 1e-4)}
+
+
+def run_reference(args) -> None:
+    """The reference arm: the CPU implementation (the oracle port, all host threads) on the same workload."""
+    import oracle
+    from naer2_b200.networks import brunel
+    from naer2_b200.runtime import describe
+
+    net, _ = brunel.build(**brunel.CONFIG1, seed=1)
+    desc = describe(net)
+    states = oracle.states_of(net, desc)
+    used = oracle.set_threads(0)
+    per_step = 100  # simulation steps per bench step: a bounded sample of the 1,000 of ours
+    n = 0
+    for _ in range(args.warmup):
+        oracle.run(desc, states, n, per_step, record=False)
+        n += per_step
+    t0 = time.perf_counter()
+    events = 0
+    for _ in range(args.steps):
+        _, ev = oracle.run(desc, states, n, per_step, record=False)
+        events += ev
+        n += per_step
+    el = time.perf_counter() - t0
+    value = events / el
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox network)",
+            "config": {**config(1), "sim_steps_per_step": per_step}, "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "port",
+                             "sample": f"{args.steps} x {per_step} simulation steps of {WORKLOAD} after "
+                                       f"{args.warmup} x {per_step} warm-up, C oracle, {used} OpenMP threads"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "realtime_factor": el / (args.steps * per_step * 1e-4)}
+    print(json.dumps(line))
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="naer2_b200", choices=["naer2_b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return 0
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from naer2_b200.networks import brunel
+    from naer2_b200.runtime import describe
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    net, pops = brunel.build(**brunel.CONFIG1, seed=1 + rank)
+    desc = describe(net) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
+    import oracle as _oracle_for_baseline_only  # noqa: F401  (the CPU baseline leg below)
+
+    cpu_states = _oracle_for_baseline_only.states_of(net, desc) if desc is not None else None
+    net.record(SIM_STEPS_PER_STEP)
+    rt = net.runtime
+    n_neurons = sum(len(p.shape) for p in net.populations)
+
+    # ---- device-resident timing
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        net.run_steps(SIM_STEPS_PER_STEP)
+    barrier()
+    ev0 = rt.counters()["events"]
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with Clocks(local) as clocks:
+        barrier()
+        for k in range(args.steps):
+            flush.zero_()
+            rt._enter()  # the runtime's stream after the flush
+            starts[k].record(rt.stream)
+            net.run_steps(SIM_STEPS_PER_STEP)
+            ends[k].record(rt.stream)
+        barrier()
+    dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    events = rt.counters()["events"] - ev0
+    launches = args.steps * SIM_STEPS_PER_STEP  # step kernels
+    launches_all = launches + args.steps * (SIM_STEPS_PER_STEP // max(net.window, 1))  # + counter advances
+    net.check()
+
+    # ---- end to end through the public API, host buffers
+    hosts = []
+    for p in net.populations:
+        for attr in ("V", "ref"):
+            t = p.state_tensor(attr)
+            hosts.append((p, attr, torch.empty(t.shape, dtype=t.dtype, pin_memory=True)))
+    for p, attr, h in hosts:
+        h.copy_(p.state_tensor(attr))
+    raster_host = [torch.empty(r.shape, dtype=r.dtype, pin_memory=True) for r in rt.rasters]
+    h2d = sum(h.numel() * h.element_size() for _, _, h in hosts)
+    d2h = h2d + sum(r.numel() * r.element_size() for r in raster_host)
+    barrier()
+    ev1 = rt.counters()["events"]
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for p, attr, h in hosts:  # inputs: the network state, from pinned host memory
+            p.state_tensor(attr).copy_(h, non_blocking=True)
+        net.record(SIM_STEPS_PER_STEP)
+        net.step(SIM_STEPS_PER_STEP * net.resolution)
+        for r, h in zip(rt.rasters, raster_host):  # results: the spike raster and the state
+            h.copy_(r, non_blocking=True)
+        for p, attr, h in hosts:
+            h.copy_(p.state_tensor(attr), non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_events = rt.counters()["events"] - ev1
+
+    # ---- max over ranks
+    stats = torch.tensor([dev_ms, e2e_s, float(events), float(e2e_events)], dtype=torch.float64, device=dev)
+    if world > 1:
+        t_max = stats[:2].clone()
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        ev_sum = stats[2:].clone()
+        dist.all_reduce(ev_sum, op=dist.ReduceOp.SUM)
+        stats = torch.cat([t_max, ev_sum])
+    dev_ms, e2e_s, events_all, e2e_events_all = stats.tolist()
+
+    cpu = None
+    if desc is not None:
+        cpu = cpu_sample(desc, cpu_states)
+
+    if rank == 0:
+        value = events_all / (dev_ms / 1e3)
+        ms_per_launch = dev_ms / launches
+        ev_per_launch = events / launches
+        alg_bytes = ev_per_launch * BYTES_PER_EVENT + n_neurons * BYTES_PER_NEURON_STEP
+        achieved = alg_bytes / (ms_per_launch / 1e3) / 1e9
+        peak, peak_kind = measured_peaks()
+        traffic = None
+        prof = ROOT / "profiles" / "step_kernel_brunel_config1.json"
+        if prof.exists():
+            traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox network, Brunel model A)",
+            "config": config(world),
+            "realtime_factor": (dev_ms / 1e3) / (args.steps * SIM_STEPS_PER_STEP * 1e-4),
+            "e2e": {"value": e2e_events_all / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "n2b::step_kernel<128>", "bytes_per_launch": alg_bytes,
+                         "us_per_launch": ms_per_launch * 1e3,
+                         "note": "launch time = timed device time / step-kernel launches (graph gaps included)"},
+            "gpu_launches": launches_all,
+            "clocks": clocks.summary(),
+            "events_per_sim_step": ev_per_launch,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    net.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -1,0 +1,167 @@
+/*
+ * naer2b -- the C ABI of the B200 hot path of naer2's per-timestep loop:
+ * membrane update, spike-ring write and read, pull intake and push delivery,
+ * stepped at a fixed dt and captured in CUDA graphs.
+ *
+ * Plain C: pointers, sizes and integers only. PyTorch (or any caller) owns
+ * every device buffer; the library borrows the pointers for the lifetime of
+ * a handle and allocates no device memory of its own (its tables live in the
+ * caller's workspace, n2b_workspace_bytes). One handle = one network on one
+ * device; calls on one handle are not thread-safe and must be serialised by
+ * the caller; the work runs on the stream passed to each call.
+ *
+ * Error convention: every entry point returns 0 on success or a negative
+ * N2B_E* code; n2b_last_error() returns the message of the calling thread's
+ * last failure. Device-side faults of the data (an arrival slot or target
+ * index out of range) are counted in the handle's error words
+ * (n2b_status) instead of trapping.
+ *
+ * Each entry point names the reference interface it replaces
+ * (MatteoSchmider/naer2, paths within that project).
+ */
+#ifndef NAER2B_H
+#define NAER2B_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define N2B_ABI_VERSION 1
+
+/* return codes */
+#define N2B_OK 0
+#define N2B_EINVAL (-1)   /* an argument or description is invalid */
+#define N2B_ECUDA (-2)    /* a CUDA call failed */
+#define N2B_ESTATE (-3)   /* the call does not fit the handle's state */
+#define N2B_ESPACE (-4)   /* the workspace is too small */
+
+/* neuron models of the built-in kernels (a population's update and send) */
+#define N2B_MODEL_LIF_DELTA 1      /* Brunel's time-driven LIF, delta synapses */
+#define N2B_MODEL_PD14 2           /* PD14 LIF, exponential current synapses  */
+#define N2B_MODEL_POISSON_SOURCE 3 /* independent Poisson spike source        */
+
+/* how a connection's spikes reach its target */
+#define N2B_PUSH 0 /* the source's block scatters its spikes into the target's arrival slots */
+#define N2B_PULL 1 /* the target gathers its incoming links against the source's spike-bit ring */
+
+/* error words (n2b_status) */
+#define N2B_ERR_PUSH_LINK 0 /* push links with delay 0, delay >= arrival depth, or target >= n */
+#define N2B_ERR_PULL_LINK 1 /* pull links with delay 0, delay >= bit depth, or source >= n */
+#define N2B_ERR_WORDS 8
+
+/* One population: the state arrays and rings of the reference's
+ * PopulationRuntime (naer2/runtime.py:213-290) at a fixed dt.
+ * Model constants p[]:
+ *   LIF_DELTA: p[0] decay = exp(-dt/tau_m) (fp32), p[1] theta, p[2] V_reset
+ *   PD14:      p[0] P_V, p[1] P_I, p[2] P_VI, p[3] V_rest, p[4] V_thresh, p[5] V_reset
+ *   POISSON_SOURCE: none (fire_threshold: fires when its uniform draw < it) */
+typedef struct n2b_population {
+    int32_t model;
+    int32_t n;               /* neurons; at most 2^24 */
+    int32_t acc_depth;       /* arrival slots: a power of two > every incoming delay (steps) */
+    int32_t bit_depth;       /* spike-bit ring rows: a power of two > every outgoing pull delay, or 0 */
+    int32_t shift;           /* fixed-point exponent of the summed input (0..62) */
+    int32_t ref_steps;       /* refractory steps after a spike */
+    uint32_t fire_threshold; /* POISSON_SOURCE only */
+    int32_t ext_len;         /* entries of ext_table (0: no external Poisson drive) */
+    uint64_t seed;           /* Philox key of the population's draws */
+    int64_t ext_wfx;         /* fixed-point weight of one external Poisson event */
+    float p[8];
+    float *v;                /* [n] membrane potential (LIF_DELTA, PD14) */
+    float *i;                /* [n] synaptic current (PD14) */
+    int32_t *ref;            /* [n] refractory steps left (LIF_DELTA, PD14) */
+    int64_t *acc;            /* [acc_depth][n] arrival slots, fixed point, zero at creation */
+    uint32_t *bits;          /* [bit_depth][ceil(n/32)] spike-bit ring, or NULL */
+    const uint32_t *ext_table; /* [ext_len] inverse-CDF table of the external Poisson count */
+    uint32_t *raster;        /* [raster_steps][ceil(n/32)] recorded spike bits, or NULL */
+    int64_t raster_steps;
+} n2b_population;
+
+/* One connection: the reference's SimulationTopology of one Connection
+ * (naer2/topology.py:291-438, built by naer2/fabric.py:100-143), as CSR.
+ * link[l] = (delay_steps << 24) | index, delay_steps in 1..255, index < 2^24:
+ *   PUSH: rows per source neuron (ptr[n_src + 1]), index = target neuron;
+ *   PULL: rows per target neuron (ptr[n_tgt + 1]), index = source neuron.
+ * w: per-link weight, or NULL for `weight` on every link. */
+typedef struct n2b_connection {
+    int32_t src;
+    int32_t tgt;
+    int32_t mode;
+    int32_t n_links;
+    float weight;
+    int32_t reserved;
+    const int32_t *ptr;
+    const uint32_t *link;
+    const float *w;
+} n2b_connection;
+
+typedef struct n2b_options {
+    int32_t block;   /* neurons (threads) per block: 64, 128 or 256 (0: 128) */
+    int32_t device;  /* CUDA device ordinal of every pointer */
+} n2b_options;
+
+typedef struct n2b_net n2b_net;
+
+/* The ABI version this library was built with (N2B_ABI_VERSION). */
+int32_t n2b_abi_version(void);
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char *n2b_last_error(void);
+
+/* Device workspace bytes a network of this description needs (its tables,
+ * step counter, error words and counters); 256-byte alignment required. */
+int n2b_workspace_bytes(const n2b_population *pops, int32_t n_pops, const n2b_connection *conns,
+                        int32_t n_conns, const n2b_options *opt, size_t *bytes);
+
+/* Build a network handle over the caller's buffers. Replaces
+ * PopulationRuntime.__init__ + connect (naer2/runtime.py:216-311) and the
+ * kernel build of FusedKernelTemplate.build (naer2/transpiler/templates/
+ * fused_template.py:166-230): the kernels are compiled into this library.
+ * The step counter starts at 0; the workspace is initialised on `stream`. */
+int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection *conns, int32_t n_conns,
+               const n2b_options *opt, void *workspace, size_t workspace_bytes, void *stream, n2b_net **out);
+
+/* Advance n_steps steps of dt, one fused step kernel each. Replaces
+ * PopulationRuntime.run / _launch (naer2/runtime.py:325-353, 506-526) as
+ * Network.step drives them (naer2/network.py:80-152). */
+int n2b_step(n2b_net *net, int64_t n_steps, void *stream);
+
+/* Capture a window of `window_steps` steps into a CUDA graph (replacing any
+ * earlier capture). Replaces WindowGraph's capture (naer2/graph.py:35-118). */
+int n2b_capture(n2b_net *net, int32_t window_steps, void *stream);
+
+/* Replay the captured window n_windows times (each advances window_steps
+ * steps). Replaces WindowGraph.replay (naer2/graph.py:120-136). */
+int n2b_replay(n2b_net *net, int64_t n_windows, void *stream);
+
+/* Set the step counter (asynchronously, on `stream`). */
+int n2b_set_step(n2b_net *net, int64_t step, void *stream);
+
+/* Start recording: raster row r of every population holds step step0 + r
+ * (rows past raster_steps are not written). */
+int n2b_record(n2b_net *net, int64_t step0, void *stream);
+
+/* Copy the error words (N2B_ERR_*) into words[0 .. n_words) after the work
+ * on `stream` (a synchronisation). Replaces PopulationRuntime.check and
+ * Ring.check (naer2/runtime.py:724-735, naer2/ring.py:390-408). */
+int n2b_status(n2b_net *net, int32_t *words, int32_t n_words, void *stream);
+
+/* Copy the counters after the work on `stream` (a synchronisation):
+ * out[0] synaptic events delivered, out[1] spikes, out[2 + p] spikes of
+ * population p; n_out entries at most. Replaces the reference's
+ * count_received counters (naer2/population.py:134-136). */
+int n2b_counters(n2b_net *net, uint64_t *out, int32_t n_out, void *stream);
+
+/* Zero the error words and counters (on `stream`). */
+int n2b_reset_counters(n2b_net *net, void *stream);
+
+/* Release the handle (its graph; the caller's buffers stay the caller's). */
+int n2b_destroy(n2b_net *net);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,399 @@
+// naer2b: the C ABI of the fixed-dt hot path (include/naer2b.h).
+//
+// Host side: validates the caller's description, lays the device tables out
+// in the caller's workspace (PopDev per population, ConnDev per connection
+// grouped by source for push and by target for pull, one tile per block),
+// launches the step kernel once per step (plus one counter advance per
+// call), and captures windows of steps into CUDA graphs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/naer2b.h"
+#include "n2b_device.cuh"
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string &msg) {
+    g_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+    return fail(N2B_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define N2B_CUDA(call)                                      \
+    do {                                                    \
+        cudaError_t _e = (call);                            \
+        if (_e != cudaSuccess) return cuda_fail(_e, #call); \
+    } while (0)
+
+bool pow2(int32_t x) { return x > 0 && (x & (x - 1)) == 0; }
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct Layout {
+    size_t pops, push, pull, tiles, step, rec0, err, counters, total;
+    int32_t n_push, n_pull, n_tiles;
+};
+
+int32_t block_of(const n2b_options *opt) {
+    int32_t b = opt && opt->block ? opt->block : 128;
+    return b;
+}
+
+Layout layout(const n2b_population *pops, int32_t n_pops, const n2b_connection *conns, int32_t n_conns,
+              int32_t block) {
+    Layout L{};
+    for (int32_t c = 0; c < n_conns; ++c) (conns[c].mode == N2B_PULL ? L.n_pull : L.n_push) += 1;
+    for (int32_t p = 0; p < n_pops; ++p) L.n_tiles += (pops[p].n + block - 1) / block;
+    size_t o = 0;
+    L.pops = o; o = align256(o + sizeof(n2b::PopDev) * std::max(n_pops, 1));
+    L.push = o; o = align256(o + sizeof(n2b::ConnDev) * std::max(L.n_push, 1));
+    L.pull = o; o = align256(o + sizeof(n2b::ConnDev) * std::max(L.n_pull, 1));
+    L.tiles = o; o = align256(o + sizeof(int4) * std::max(L.n_tiles, 1));
+    L.step = o; o = align256(o + sizeof(long long));
+    L.rec0 = o; o = align256(o + sizeof(long long));
+    L.err = o; o = align256(o + sizeof(int32_t) * N2B_ERR_WORDS);
+    L.counters = o; o = align256(o + sizeof(unsigned long long) * (2 + std::max(n_pops, 1)));
+    L.total = o;
+    return L;
+}
+
+int validate(const n2b_population *pops, int32_t n_pops, const n2b_connection *conns, int32_t n_conns,
+             const n2b_options *opt) {
+    if (n_pops < 0 || n_conns < 0 || (n_pops > 0 && !pops) || (n_conns > 0 && !conns))
+        return fail(N2B_EINVAL, "negative counts or missing arrays");
+    const int32_t block = block_of(opt);
+    if (block != 64 && block != 128 && block != 256) return fail(N2B_EINVAL, "block must be 64, 128 or 256");
+    for (int32_t p = 0; p < n_pops; ++p) {
+        const n2b_population &P = pops[p];
+        const std::string at = "population " + std::to_string(p) + ": ";
+        if (P.n < 0 || P.n > (1 << 24)) return fail(N2B_EINVAL, at + "n must be in [0, 2^24]");
+        if (P.model != N2B_MODEL_LIF_DELTA && P.model != N2B_MODEL_PD14 && P.model != N2B_MODEL_POISSON_SOURCE)
+            return fail(N2B_EINVAL, at + "unknown model");
+        if (P.shift < 0 || P.shift > 62) return fail(N2B_EINVAL, at + "shift must be in [0, 62]");
+        if (P.bit_depth != 0 && (!pow2(P.bit_depth) || P.bit_depth > 256 || !P.bits))
+            return fail(N2B_EINVAL, at + "bit_depth must be 0 or a power of two <= 256 with bits");
+        if (P.raster_steps < 0 || (P.raster_steps > 0 && !P.raster))
+            return fail(N2B_EINVAL, at + "raster_steps > 0 needs a raster");
+        if (P.n == 0) continue;
+        if (P.model != N2B_MODEL_POISSON_SOURCE) {
+            if (!pow2(P.acc_depth) || P.acc_depth > 256 || !P.acc)
+                return fail(N2B_EINVAL, at + "acc_depth must be a power of two <= 256 with acc");
+            if (!P.v || !P.ref || (P.model == N2B_MODEL_PD14 && !P.i))
+                return fail(N2B_EINVAL, at + "missing state arrays");
+            if (P.ext_len < 0 || (P.ext_len > 0 && !P.ext_table))
+                return fail(N2B_EINVAL, at + "ext_len > 0 needs ext_table");
+        }
+    }
+    for (int32_t c = 0; c < n_conns; ++c) {
+        const n2b_connection &C = conns[c];
+        const std::string at = "connection " + std::to_string(c) + ": ";
+        if (C.src < 0 || C.src >= n_pops || C.tgt < 0 || C.tgt >= n_pops)
+            return fail(N2B_EINVAL, at + "src/tgt out of range");
+        if (C.mode != N2B_PUSH && C.mode != N2B_PULL) return fail(N2B_EINVAL, at + "unknown mode");
+        if (C.n_links < 0 || !C.ptr || (C.n_links > 0 && !C.link))
+            return fail(N2B_EINVAL, at + "missing CSR arrays");
+        const n2b_population &T = pops[C.tgt];
+        const n2b_population &S = pops[C.src];
+        if (T.model == N2B_MODEL_POISSON_SOURCE) return fail(N2B_EINVAL, at + "a Poisson source takes no input");
+        if (T.n > 0 && (!T.acc || !pow2(T.acc_depth))) return fail(N2B_EINVAL, at + "target has no arrival slots");
+        if (C.mode == N2B_PULL && S.n > 0 && (!S.bits || !pow2(S.bit_depth)))
+            return fail(N2B_EINVAL, at + "a pull connection needs the source's spike-bit ring");
+    }
+    return N2B_OK;
+}
+
+}  // namespace
+
+struct n2b_net {
+    int device = 0;
+    int32_t block = 128;
+    int32_t n_pops = 0;
+    Layout L{};
+    char *ws = nullptr;
+    n2b::StepArgs args{};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int32_t window = 0;
+};
+
+namespace {
+
+cudaError_t launch_steps(n2b_net *net, int64_t n_steps, cudaStream_t s) {
+    if (net->L.n_tiles > 0) {
+        n2b::StepArgs a = net->args;
+        for (int64_t k = 0; k < n_steps; ++k) {
+            a.offset = (int32_t)k;
+            switch (net->block) {
+                case 64: n2b::step_kernel<64><<<net->L.n_tiles, 64, 0, s>>>(a); break;
+                case 256: n2b::step_kernel<256><<<net->L.n_tiles, 256, 0, s>>>(a); break;
+                default: n2b::step_kernel<128><<<net->L.n_tiles, 128, 0, s>>>(a); break;
+            }
+        }
+    }
+    n2b::advance_kernel<<<1, 1, 0, s>>>(reinterpret_cast<long long *>(net->ws + net->L.step), n_steps);
+    return cudaGetLastError();
+}
+
+void drop_graph(n2b_net *net) {
+    if (net->exec) cudaGraphExecDestroy(net->exec);
+    if (net->graph) cudaGraphDestroy(net->graph);
+    net->exec = nullptr;
+    net->graph = nullptr;
+    net->window = 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t n2b_abi_version(void) { return N2B_ABI_VERSION; }
+
+const char *n2b_last_error(void) { return g_error.c_str(); }
+
+int n2b_workspace_bytes(const n2b_population *pops, int32_t n_pops, const n2b_connection *conns, int32_t n_conns,
+                        const n2b_options *opt, size_t *bytes) {
+    if (!bytes) return fail(N2B_EINVAL, "bytes is NULL");
+    int rc = validate(pops, n_pops, conns, n_conns, opt);
+    if (rc) return rc;
+    *bytes = layout(pops, n_pops, conns, n_conns, block_of(opt)).total;
+    return N2B_OK;
+}
+
+int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection *conns, int32_t n_conns,
+               const n2b_options *opt, void *workspace, size_t workspace_bytes, void *stream, n2b_net **out) {
+    if (!out) return fail(N2B_EINVAL, "out is NULL");
+    *out = nullptr;
+    int rc = validate(pops, n_pops, conns, n_conns, opt);
+    if (rc) return rc;
+    const int32_t block = block_of(opt);
+    Layout L = layout(pops, n_pops, conns, n_conns, block);
+    if (!workspace || (reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
+        return fail(N2B_EINVAL, "workspace must be a 256-byte aligned device pointer");
+    if (workspace_bytes < L.total)
+        return fail(N2B_ESPACE, "workspace too small: need " + std::to_string(L.total) + " bytes");
+    const int device = opt ? opt->device : 0;
+    N2B_CUDA(cudaSetDevice(device));
+
+    // host images of the tables
+    std::vector<n2b::PopDev> pd(std::max(n_pops, 1));
+    std::vector<n2b::ConnDev> push, pull;
+    std::vector<int4> tiles;
+    for (int32_t p = 0; p < n_pops; ++p) {
+        const n2b_population &P = pops[p];
+        n2b::PopDev &D = pd[p];
+        std::memset(&D, 0, sizeof(D));
+        D.model = P.model;
+        D.n = P.n;
+        D.acc_mask = P.acc_depth > 0 ? P.acc_depth - 1 : 0;
+        D.bit_mask = P.bit_depth > 0 ? P.bit_depth - 1 : 0;
+        D.words = (P.n + 31) / 32;
+        D.shift = P.shift;
+        D.ref_steps = P.ref_steps;
+        D.ext_len = P.ext_len;
+        D.fire_threshold = P.fire_threshold;
+        D.seed_lo = (uint32_t)P.seed;
+        D.seed_hi = (uint32_t)(P.seed >> 32);
+        D.index = (uint32_t)p;
+        D.ext_wfx = P.ext_wfx;
+        D.inv_scale = std::ldexp(1.0f, -P.shift);
+        for (int k = 0; k < 8; ++k) D.p[k] = P.p[k];
+        D.v = P.v;
+        D.i = P.i;
+        D.ref = P.ref;
+        D.acc = reinterpret_cast<long long *>(P.acc);
+        D.bits = P.bits;
+        D.ext_table = P.ext_table;
+        D.raster = P.raster;
+        D.raster_steps = P.raster_steps;
+    }
+    auto conn_dev = [&](const n2b_connection &C) {
+        n2b::ConnDev D;
+        std::memset(&D, 0, sizeof(D));
+        const n2b_population &S = pops[C.src], &T = pops[C.tgt];
+        D.homogeneous = C.w == nullptr;
+        D.src_n = S.n;
+        D.tgt_n = T.n;
+        D.tgt_acc_mask = T.acc_depth > 0 ? T.acc_depth - 1 : 0;
+        D.src_bit_mask = S.bit_depth > 0 ? S.bit_depth - 1 : 0;
+        D.src_words = (S.n + 31) / 32;
+        D.wscale = std::ldexp(1.0f, T.shift);
+        D.wfx = (long long)std::nearbyint((double)std::ldexp(C.weight, T.shift));
+        D.ptr = C.ptr;
+        D.link = C.link;
+        D.w = C.w;
+        D.tgt_acc = reinterpret_cast<long long *>(T.acc);
+        D.src_bits = S.bits;
+        return D;
+    };
+    for (int32_t p = 0; p < n_pops; ++p) {
+        pd[p].out_first = (int32_t)push.size();
+        for (int32_t c = 0; c < n_conns; ++c)
+            if (conns[c].mode == N2B_PUSH && conns[c].src == p) push.push_back(conn_dev(conns[c]));
+        pd[p].n_out = (int32_t)push.size() - pd[p].out_first;
+        pd[p].pull_first = (int32_t)pull.size();
+        for (int32_t c = 0; c < n_conns; ++c)
+            if (conns[c].mode == N2B_PULL && conns[c].tgt == p) pull.push_back(conn_dev(conns[c]));
+        pd[p].n_pull = (int32_t)pull.size() - pd[p].pull_first;
+    }
+    // tiles: the largest populations' first (their blocks start first)
+    std::vector<int32_t> order(n_pops);
+    for (int32_t p = 0; p < n_pops; ++p) order[p] = p;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return pops[x].n > pops[y].n; });
+    for (int32_t p : order)
+        for (int32_t f = 0; f < pops[p].n; f += block) tiles.push_back(make_int4(p, f, std::min(block, pops[p].n - f), 0));
+
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    char *ws = static_cast<char *>(workspace);
+    if (n_pops) N2B_CUDA(cudaMemcpyAsync(ws + L.pops, pd.data(), sizeof(n2b::PopDev) * n_pops, cudaMemcpyHostToDevice, s));
+    if (!push.empty())
+        N2B_CUDA(cudaMemcpyAsync(ws + L.push, push.data(), sizeof(n2b::ConnDev) * push.size(), cudaMemcpyHostToDevice, s));
+    if (!pull.empty())
+        N2B_CUDA(cudaMemcpyAsync(ws + L.pull, pull.data(), sizeof(n2b::ConnDev) * pull.size(), cudaMemcpyHostToDevice, s));
+    if (!tiles.empty())
+        N2B_CUDA(cudaMemcpyAsync(ws + L.tiles, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, s));
+    n2b::set_kernel<<<1, 1, 0, s>>>(reinterpret_cast<long long *>(ws + L.step), 0);
+    n2b::set_kernel<<<1, 1, 0, s>>>(reinterpret_cast<long long *>(ws + L.rec0), 0);
+    n2b::zero_kernel<<<1, 64, 0, s>>>(reinterpret_cast<int32_t *>(ws + L.err), N2B_ERR_WORDS,
+                                      reinterpret_cast<unsigned long long *>(ws + L.counters), 2 + n_pops);
+    N2B_CUDA(cudaGetLastError());
+    // the host images are read by the copies above: wait for them before they go
+    N2B_CUDA(cudaStreamSynchronize(s));
+
+    n2b_net *net = new n2b_net();
+    net->device = device;
+    net->block = block;
+    net->n_pops = n_pops;
+    net->L = L;
+    net->ws = ws;
+    n2b::StepArgs &a = net->args;
+    a.pops = reinterpret_cast<const n2b::PopDev *>(ws + L.pops);
+    a.push = reinterpret_cast<const n2b::ConnDev *>(ws + L.push);
+    a.pull = reinterpret_cast<const n2b::ConnDev *>(ws + L.pull);
+    a.tiles = reinterpret_cast<const int4 *>(ws + L.tiles);
+    a.step = reinterpret_cast<const long long *>(ws + L.step);
+    a.rec0 = reinterpret_cast<const long long *>(ws + L.rec0);
+    a.err = reinterpret_cast<int32_t *>(ws + L.err);
+    a.counters = reinterpret_cast<unsigned long long *>(ws + L.counters);
+    a.offset = 0;
+    *out = net;
+    return N2B_OK;
+}
+
+int n2b_step(n2b_net *net, int64_t n_steps, void *stream) {
+    if (!net) return fail(N2B_EINVAL, "net is NULL");
+    if (n_steps < 0 || n_steps > (int64_t)1 << 30) return fail(N2B_EINVAL, "n_steps out of range");
+    N2B_CUDA(cudaSetDevice(net->device));
+    cudaError_t e = launch_steps(net, n_steps, reinterpret_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return cuda_fail(e, "step launch");
+    return N2B_OK;
+}
+
+int n2b_capture(n2b_net *net, int32_t window_steps, void *stream) {
+    if (!net) return fail(N2B_EINVAL, "net is NULL");
+    if (window_steps <= 0 || window_steps > (1 << 20)) return fail(N2B_EINVAL, "window_steps out of range");
+    N2B_CUDA(cudaSetDevice(net->device));
+    drop_graph(net);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    N2B_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    cudaError_t le = launch_steps(net, window_steps, s);
+    cudaGraph_t g = nullptr;
+    cudaError_t ee = cudaStreamEndCapture(s, &g);
+    if (le != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return cuda_fail(le, "capture launch");
+    }
+    if (ee != cudaSuccess) return cuda_fail(ee, "cudaStreamEndCapture");
+    cudaGraphExec_t x = nullptr;
+    cudaError_t ie = cudaGraphInstantiate(&x, g, 0);
+    if (ie != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return cuda_fail(ie, "cudaGraphInstantiate");
+    }
+    net->graph = g;
+    net->exec = x;
+    net->window = window_steps;
+    return N2B_OK;
+}
+
+int n2b_replay(n2b_net *net, int64_t n_windows, void *stream) {
+    if (!net) return fail(N2B_EINVAL, "net is NULL");
+    if (!net->exec) return fail(N2B_ESTATE, "no captured window: call n2b_capture first");
+    if (n_windows < 0) return fail(N2B_EINVAL, "n_windows < 0");
+    N2B_CUDA(cudaSetDevice(net->device));
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    for (int64_t k = 0; k < n_windows; ++k) N2B_CUDA(cudaGraphLaunch(net->exec, s));
+    return N2B_OK;
+}
+
+int n2b_set_step(n2b_net *net, int64_t step, void *stream) {
+    if (!net) return fail(N2B_EINVAL, "net is NULL");
+    if (step < 0) return fail(N2B_EINVAL, "step < 0");
+    N2B_CUDA(cudaSetDevice(net->device));
+    n2b::set_kernel<<<1, 1, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<long long *>(net->ws + net->L.step), step);
+    N2B_CUDA(cudaGetLastError());
+    return N2B_OK;
+}
+
+int n2b_record(n2b_net *net, int64_t step0, void *stream) {
+    if (!net) return fail(N2B_EINVAL, "net is NULL");
+    N2B_CUDA(cudaSetDevice(net->device));
+    n2b::set_kernel<<<1, 1, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<long long *>(net->ws + net->L.rec0), step0);
+    N2B_CUDA(cudaGetLastError());
+    return N2B_OK;
+}
+
+int n2b_status(n2b_net *net, int32_t *words, int32_t n_words, void *stream) {
+    if (!net || !words || n_words < 0) return fail(N2B_EINVAL, "bad arguments");
+    N2B_CUDA(cudaSetDevice(net->device));
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    int32_t host[N2B_ERR_WORDS];
+    N2B_CUDA(cudaMemcpyAsync(host, net->ws + net->L.err, sizeof(host), cudaMemcpyDeviceToHost, s));
+    N2B_CUDA(cudaStreamSynchronize(s));
+    for (int32_t k = 0; k < n_words && k < N2B_ERR_WORDS; ++k) words[k] = host[k];
+    return N2B_OK;
+}
+
+int n2b_counters(n2b_net *net, uint64_t *out, int32_t n_out, void *stream) {
+    if (!net || !out || n_out < 0) return fail(N2B_EINVAL, "bad arguments");
+    N2B_CUDA(cudaSetDevice(net->device));
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    std::vector<unsigned long long> host(2 + net->n_pops);
+    N2B_CUDA(cudaMemcpyAsync(host.data(), net->ws + net->L.counters, sizeof(unsigned long long) * host.size(),
+                             cudaMemcpyDeviceToHost, s));
+    N2B_CUDA(cudaStreamSynchronize(s));
+    for (int32_t k = 0; k < n_out && k < (int32_t)host.size(); ++k) out[k] = host[k];
+    return N2B_OK;
+}
+
+int n2b_reset_counters(n2b_net *net, void *stream) {
+    if (!net) return fail(N2B_EINVAL, "net is NULL");
+    N2B_CUDA(cudaSetDevice(net->device));
+    n2b::zero_kernel<<<1, 64, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<int32_t *>(net->ws + net->L.err), N2B_ERR_WORDS,
+        reinterpret_cast<unsigned long long *>(net->ws + net->L.counters), 2 + net->n_pops);
+    N2B_CUDA(cudaGetLastError());
+    return N2B_OK;
+}
+
+int n2b_destroy(n2b_net *net) {
+    if (!net) return N2B_OK;
+    cudaSetDevice(net->device);
+    drop_graph(net);
+    delete net;
+    return N2B_OK;
+}
+
+}  // extern "C"

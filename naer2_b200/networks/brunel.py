@@ -1,0 +1,52 @@
+"""Brunel (2000) model A, time-driven: a sparse balanced network of N_E
+excitatory and N_I inhibitory LIF neurons with delta synapses, fixed
+in-degree (C_E from E, C_I from I, drawn uniformly without autapses), PSP J
+and -g J, an external Poisson drive of eta * nu_thr per external source
+(nu_thr = theta / (J C_E tau)) from C_E sources, i.e. C_E eta nu_thr events
+per ms of weight J into every neuron -- the reference's
+tools/brunel_reference.py (time-driven) and test/networks/Brunel/net.py
+(event-driven) at a fixed dt.
+
+delay: one delay in ms for every link, or "uniform" -- integer delays drawn
+uniformly in [1, max_delay_steps] steps per link.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .. import philox
+from ..models import LIF
+from ..patterns import fixed_indegree
+
+CONFIG0 = dict(NE=800, NI=200, CE=80, CI=20, delay=1.5)
+CONFIG1 = dict(NE=10000, NI=2500, CE=1000, CI=250, delay="uniform", max_delay_steps=20)
+
+
+def build(NE: int = 800, NI: int = 200, CE: int = 80, CI: int = 20, J: float = 0.1, g: float = 5.0,
+          eta: float = 2.0, delay="uniform", max_delay_steps: int = 20, tau: float = 20.0, theta: float = 20.0,
+          V_r: float = 10.0, t_ref: float = 2.0, dt: float = 0.1, seed: int = 0, group_size: int = 128):
+    """(network, {"E": E, "I": I}) of Brunel's model A at step dt."""
+    nu_thr = theta / (J * CE * tau)
+    ext_rate = CE * eta * nu_thr  # external events per ms into each neuron
+    E = LIF(tau=tau, theta=theta, V_r=V_r, t_ref=t_ref, ext_rate=ext_rate, ext_weight=J) * NE
+    I = LIF(tau=tau, theta=theta, V_r=V_r, t_ref=t_ref, ext_rate=ext_rate, ext_weight=J) * NI
+    E.seed, I.seed = (seed << 8) | 1, (seed << 8) | 2
+    E.group_size = I.group_size = group_size
+    E.V = torch.from_numpy((philox.uniform(seed, NE, stream=1) * theta).astype(np.float32))
+    I.V = torch.from_numpy((philox.uniform(seed, NI, stream=2) * theta).astype(np.float32))
+    k = 0
+    for tgt in (E, I):
+        for src, C, w in ((E, CE, J), (I, CI, -g * J)):
+            k += 1
+            conn = src >> fixed_indegree(C, autapses=False, seed=(seed << 8) | (16 + k)) >> tgt
+            conn.weight = w
+            if delay == "uniform":
+                steps = philox.generator((seed << 8) | (32 + k)).integers(1, max_delay_steps + 1, conn.shape[0])
+                conn.delay = torch.from_numpy((steps * dt).astype(np.float32))
+            else:
+                conn.delay = float(delay)
+    net = E.network
+    net.resolution = dt
+    return net, {"E": E, "I": I}

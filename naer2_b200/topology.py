@@ -1,0 +1,172 @@
+"""Connectivity: the canonical CSR a pattern builds (reference
+naer2/topology.py:98-199), and the two device forms the hot path walks.
+
+Canonical form (what a pattern gives, what per-link tensors are indexed by):
+one row per source neuron, its links in the order the pattern returned them.
+
+Device forms, one packed 32-bit word per link, `(delay_steps << 24) | index`:
+  push  rows per SOURCE (the canonical order itself), index = target neuron;
+        the source's block scatters its spikes along them;
+  pull  rows per TARGET (a stable sort of the canonical links by target),
+        index = source neuron; the target's block gathers them against the
+        source's spike-bit ring.
+Per-link weights (fp32) follow the same orders. The reference restructures
+its canonical links into (source, target group, delay bucket) segments
+(naer2/topology.py:291-438); at a fixed dt every delay is a whole number of
+steps, so the delay rides in the link word instead and no bucket is needed.
+"""
+
+from __future__ import annotations
+
+import inspect
+
+import numpy as np
+import torch
+
+from .types import IndexBox, Region, _BaseBox, _BasePoints
+
+MAX_INDEX = 1 << 24  # a link word's index field
+MAX_DELAY_STEPS = 255  # its delay field
+
+
+def _index_fn(target_region):
+    """Coordinates [n, ndim] -> linear indices into target_region (row-major for a box, a lookup for points)."""
+    if isinstance(target_region, _BaseBox):
+        starts, steps, sizes = target_region.start.long(), target_region.step.long(), target_region.sizes
+        strides = torch.ones(len(sizes), dtype=torch.int64)
+        for d in range(len(sizes) - 2, -1, -1):
+            strides[d] = strides[d + 1] * sizes[d + 1]
+
+        def to_index(coords):
+            if len(coords) == 0:
+                return torch.zeros(0, dtype=torch.int64)
+            return (((coords.long() - starts) // steps) * strides).sum(dim=1)
+
+        return to_index
+    if isinstance(target_region, _BasePoints):
+        lookup = {tuple(c.tolist()): i for i, c in enumerate(target_region.coords)}
+        return lambda coords: torch.tensor([lookup[tuple(c.tolist())] for c in coords], dtype=torch.int64)
+    raise TypeError(f"Cannot index {type(target_region).__name__}")
+
+
+def _coords(result) -> torch.Tensor:
+    if isinstance(result, _BasePoints):
+        return result.coords
+    if isinstance(result, _BaseBox):
+        return result.points
+    return torch.zeros((0, 1), dtype=torch.int64)
+
+
+def _flat_size(region) -> int | None:
+    """n for a flat 0-based index box [[0, n, 1]], else None."""
+    if isinstance(region, IndexBox) and region.coords.shape[0] == 1:
+        start, _, step = region.coords[0].tolist()
+        if start == 0 and step == 1:
+            return len(region)
+    return None
+
+
+class Topology:
+    """Canonical CSR: source_offsets [n_src + 1] int64, target_indices [n_links] int64.
+    Multapses are kept as separate links."""
+
+    def __init__(self, source_offsets: torch.Tensor, target_indices: torch.Tensor):
+        self.source_offsets = source_offsets
+        self.target_indices = target_indices
+
+    @property
+    def shape(self) -> tuple:
+        return (len(self.target_indices),)
+
+    def __len__(self) -> int:
+        return len(self.target_indices)
+
+    @property
+    def n_sources(self) -> int:
+        return len(self.source_offsets) - 1
+
+    @staticmethod
+    def build(pattern, source_region, target_region=None, same: bool = False):
+        """Run the pattern for every source point (reference naer2/topology.py:130-199); a Topology, or
+        (Topology, inferred target region) without target_region. A pattern exposing
+        links(n_src, n_tgt) -> (offsets, targets) is asked for the whole CSR at once when both regions are
+        flat index ranges (the built-in patterns; same links as the per-point calls). same: source and target
+        are one population (a pattern may exclude autapses then)."""
+        n_src, n_tgt = _flat_size(source_region), (_flat_size(target_region) if target_region is not None else None)
+        if hasattr(pattern, "links") and n_src is not None and (target_region is None or n_tgt is not None):
+            offsets, targets = pattern.links(n_src, n_tgt if n_tgt is not None else n_src,
+                                             same=same or target_region is None)
+            topo = Topology(torch.as_tensor(offsets, dtype=torch.int64), torch.as_tensor(targets, dtype=torch.int64))
+            if target_region is None:
+                size = int(topo.target_indices.max()) + 1 if len(topo) else 0
+                return topo, Region(size)
+            return topo
+        takes_target = len(inspect.signature(pattern).parameters) > 2
+
+        def call(pos):
+            return pattern(pos, source_region, target_region) if takes_target else pattern(pos, source_region)
+
+        rows = [_coords(call(pos)) for pos in source_region]
+        if target_region is None:
+            nonempty = [r for r in rows if len(r)]
+            if nonempty:
+                maxes = torch.cat(nonempty).max(dim=0).values.tolist()
+                sizes = tuple(int(m) + 1 for m in maxes)
+                inferred = Region(sizes[0] if len(sizes) == 1 else sizes)
+            else:
+                inferred = Region(0)
+        else:
+            inferred = target_region
+        to_index = _index_fn(inferred)
+        idx = [to_index(r) for r in rows]
+        off = np.zeros(len(idx) + 1, dtype=np.int64)
+        off[1:] = np.cumsum([len(r) for r in idx])
+        targets = torch.cat(idx) if off[-1] else torch.zeros(0, dtype=torch.int64)
+        topo = Topology(torch.from_numpy(off), targets)
+        return (topo, inferred) if target_region is None else topo
+
+
+def delay_steps(delay, n_links: int, dt: float) -> np.ndarray:
+    """Per-link delays in whole steps of dt: round(delay / dt), at least 1 (a spike is delivered from the
+    next step on; the reference clamps delays to >= its 0.1 ms resolution, test/networks/PD14/net.py:102)."""
+    if delay is None:
+        return np.ones(n_links, dtype=np.int64)
+    if isinstance(delay, torch.Tensor):
+        d = delay.detach().cpu().double().numpy().reshape(-1)
+        if len(d) != n_links:
+            raise ValueError(f"delay has {len(d)} values for {n_links} links")
+    else:
+        d = np.full(n_links, float(delay))
+    steps = np.rint(d / dt).astype(np.int64)
+    steps = np.maximum(steps, 1)
+    if len(steps) and steps.max() > MAX_DELAY_STEPS:
+        raise ValueError(f"a delay of {int(steps.max())} steps exceeds {MAX_DELAY_STEPS}")
+    return steps
+
+
+def pack_links(index: np.ndarray, steps: np.ndarray) -> np.ndarray:
+    """(delay_steps << 24) | index as uint32."""
+    if len(index) and (index.min() < 0 or index.max() >= MAX_INDEX):
+        raise ValueError("a link index outside [0, 2^24)")
+    return ((steps.astype(np.uint32) << np.uint32(24)) | index.astype(np.uint32)).astype(np.uint32)
+
+
+def push_form(topo: Topology, steps: np.ndarray, n_tgt: int):
+    """(ptr int32 [n_src + 1], link uint32 [n_links]) in canonical order."""
+    tgt = topo.target_indices.numpy()
+    if len(tgt) and (tgt.min() < 0 or tgt.max() >= n_tgt):
+        raise ValueError("a link targets a neuron outside the target population")
+    return topo.source_offsets.numpy().astype(np.int32), pack_links(tgt, steps)
+
+
+def pull_form(topo: Topology, steps: np.ndarray, n_tgt: int):
+    """(ptr int32 [n_tgt + 1], link uint32 [n_links], perm int64 [n_links]): the links sorted by target
+    (stable: canonical order within a target); perm[k] is the canonical link at pull position k."""
+    off = topo.source_offsets.numpy()
+    tgt = topo.target_indices.numpy()
+    src = np.repeat(np.arange(len(off) - 1, dtype=np.int64), np.diff(off))
+    perm = np.argsort(tgt, kind="stable")
+    counts = np.bincount(tgt, minlength=n_tgt) if len(tgt) else np.zeros(n_tgt, dtype=np.int64)
+    ptr = np.zeros(n_tgt + 1, dtype=np.int64)
+    ptr[1:] = np.cumsum(counts)
+    return ptr.astype(np.int32), pack_links(src[perm], steps[perm]), perm

@@ -1,0 +1,202 @@
+"""Regenerate the golden fixtures of this directory from the reference itself.
+
+    python tests/golden/make_golden.py [--reference PATH]
+
+Runs only where the reference source tree is available (default
+/root/reference); the fixtures it writes are committed, and the tests read
+only them. What each fixture pins:
+
+brunel_reference_c0.npz
+    The reference's time-driven Brunel loop, tools/brunel_reference.py:34-48,
+    executed here on CPU from its own source text with these substitutions:
+    dev "cpu", dt 0.1, T 100 ms, N_E/N_I 800/200, C_E/C_I 80/20, the
+    connectivity (`src`) drawn here (fixed in-degree, no autapses), V0 drawn
+    here, and the Poisson counts `torch.poisson(...)` replaced by the counts
+    the hot path draws itself (Philox4x32-10 key `seed`, counter
+    (j, step, 0, 0), inverted against the fp64 table `table`). Everything
+    else -- the delay buffer, refractory test, update, reset, the sparse
+    matvec -- is the reference's code as written. Outputs: the spike raster
+    (packed bits) and V after every 100 steps.
+
+pd14_neuron.npz
+    The PD14 neuron update + send restated in torch by the reference's own
+    GPU test, _neuron_reference in test/test_fused_models_gpu.py:32-52,
+    extracted from its source and run here on CPU step by step over a fixed
+    dt of 0.1 ms, with a per-step input current (count * J) injected as
+    `received`. Outputs: the raster and the state after every 10th step.
+
+philox_triton.json
+    tl.randint4x / tl.rand of Triton (the reference's random lowering calls
+    tl.rand, naer2/transpiler/transformers/random_lowering_transformer.py:
+    74-86) under TRITON_INTERPRET=1 on CPU, for a few seeds and offsets.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ast
+import json
+import math
+import os
+import pathlib
+import sys
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+sys.path.insert(0, str(ROOT))
+
+import oracle  # noqa: E402  (test infrastructure: the shared Philox counts and tables)
+from naer2_b200.poisson import cdf_table  # noqa: E402
+
+SEED_C0 = 0x0C0FFEE
+SEED_PD14 = 0x0D14
+
+
+def _sub(src: str, old: str, new: str) -> str:
+    if src.count(old) != 1:
+        raise RuntimeError(f"expected exactly one {old!r} in the reference source")
+    return src.replace(old, new)
+
+
+def brunel_c0(reference: pathlib.Path, steps: int = 1000):
+    import torch
+
+    NE, NI, CE, CI = 800, 200, 80, 20
+    N = NE + NI
+    rng = np.random.Generator(np.random.Philox(key=7))
+    # fixed in-degree without autapses, per target: CE sources from E, CI from I (with replacement)
+    tgt = np.arange(N)
+    e_src = rng.integers(0, NE - 1, size=(N, CE))
+    e_src += (e_src >= tgt[:, None]) & (tgt[:, None] < NE)
+    i_src = rng.integers(0, NI - 1, size=(N, CI))
+    i_src += (i_src >= (tgt[:, None] - NE)) & (tgt[:, None] >= NE)
+    src = np.concatenate([e_src, NE + i_src], axis=1).astype(np.int64)
+    V0 = (rng.random(N, dtype=np.float32) * np.float32(20.0)).astype(np.float32)
+    table = cdf_table(2.0)  # lam = C_E nu_ext dt = 2.0 per step at eta 2 (brunel_reference.py:24-25)
+    counts = oracle.poisson_counts(table, SEED_C0, 0, steps, N)
+
+    text = (reference / "tools" / "brunel_reference.py").read_text()
+    text = text[: text.index("times = torch.cat")]  # the statistics after the loop are not needed
+    text = _sub(text, 'dt = float(sys.argv[1]) if len(sys.argv) > 1 else 0.05', "dt = 0.1")
+    text = _sub(text, "T = 400.0", f"T = {steps * 0.1!r}")
+    text = _sub(text, 'dev = "cuda"', 'dev = "cpu"')
+    text = _sub(text, "NE, NI = 10000, 2500", f"NE, NI = {NE}, {NI}")
+    text = _sub(text, "CE, CI = 1000, 250", f"CE, CI = {CE}, {CI}")
+    text = _sub(text, "src = torch.cat([torch.randint(0, NE, (N, CE), generator=gen), NE + torch.randint(0, NI, "
+                      "(N, CI), generator=gen)], 1).flatten()", "src = _golden_src.flatten()")
+    text = _sub(text, "V = torch.rand(N, generator=gen).to(dev) * theta", "V = _golden_V0.clone()")
+    text = _sub(text, "torch.poisson(torch.full((N,), lam, device=dev))", "_golden_counts[n]")
+    text = _sub(text, "torch.cuda.synchronize()", "pass")
+    # V every 100 steps, taken inside the loop after the reference's own statements
+    text = _sub(text, "        spk_t.append(torch.full((len(idx),), t, device=dev)); spk_i.append(idx)",
+                "        spk_t.append(torch.full((len(idx),), t, device=dev)); spk_i.append(idx)\n"
+                "    if (n + 1) % 100 == 0:\n        _golden_V.append(V.clone())")
+    ns = {"_golden_src": torch.from_numpy(src), "_golden_V0": torch.from_numpy(V0),
+          "_golden_counts": torch.from_numpy(counts.astype(np.float32)), "_golden_V": [], "__name__": "golden"}
+    exec(compile(text, str(reference / "tools" / "brunel_reference.py"), "exec"), ns)
+    raster = np.zeros((steps, N), dtype=bool)
+    for t_, idx in zip(ns["spk_t"], ns["spk_i"]):
+        n = int(round(float(t_[0]) / 0.1)) - 1  # the reference stamps step n with t = (n + 1) dt
+        raster[n, idx.numpy()] = True
+    V = np.stack([v.numpy() for v in ns["_golden_V"]]).astype(np.float32)
+    np.savez_compressed(HERE / "brunel_reference_c0.npz", src=src.astype(np.int32), V0=V0, seed=np.uint64(SEED_C0),
+                        table=table, steps=np.int64(steps), NE=np.int64(NE), NI=np.int64(NI), J=np.float32(0.1),
+                        g=np.float32(5.0), delay_steps=np.int64(15), raster=np.packbits(raster, axis=1), V=V)
+    print(f"brunel_reference_c0: {raster.sum()} spikes in {steps} steps")
+
+
+def _reference_function(path: pathlib.Path, name: str):
+    """A top-level function of a reference module, compiled from its source alone (its imports not run)."""
+    tree = ast.parse(path.read_text())
+    fn = next(n for n in tree.body if isinstance(n, ast.FunctionDef) and n.name == name)
+    mod = ast.Module(body=[fn], type_ignores=[])
+    import torch
+
+    ns = {"torch": torch, "math": math}
+    exec(compile(mod, str(path), "exec"), ns)
+    return ns[name]
+
+
+def pd14_neuron(reference: pathlib.Path, steps: int = 400, n: int = 256, every: int = 10):
+    import torch
+
+    sys.path.insert(0, str(reference))
+    try:
+        from test.networks.PD14.neuron import PD14_neuron
+    finally:
+        sys.path.pop(0)
+    neuron = PD14_neuron(K_cortical=2100)  # the reference's own class: its parameters and V_rest
+    ref_fn = _reference_function(reference / "test" / "test_fused_models_gpu.py", "_neuron_reference")
+    rng = np.random.Generator(np.random.Philox(key=11))
+    V0 = rng.normal(-58.0, 4.0, n).astype(np.float32)
+    I0 = (rng.random(n) * 0.5).astype(np.float32)
+    J = np.float32(0.08781)
+    table = cdf_table(8e-3 * 2100 * 0.1 * 4.0)  # a strong drive: ~6.7 events a step
+    counts = oracle.poisson_counts(table, SEED_PD14, 0, steps, n)
+    state = dict(potential=torch.from_numpy(V0), current=torch.from_numpy(I0),
+                 t_ref_end=torch.zeros(n), last_time=torch.zeros(n))
+    raster = np.zeros((steps, n), dtype=bool)
+    Vs, Is = [], []
+    for k in range(steps):
+        time = float(np.float32((k + 1) * 0.1))
+        received = torch.from_numpy(counts[k].astype(np.float32)) * torch.tensor(J)
+        state, fires = ref_fn(neuron, state, time, received)
+        raster[k] = fires.numpy()
+        if (k + 1) % every == 0:
+            Vs.append(state["potential"].numpy().copy())
+            Is.append(state["current"].numpy().copy())
+    np.savez_compressed(HERE / "pd14_neuron.npz", V0=V0, I0=I0, seed=np.uint64(SEED_PD14), table=table,
+                        J=J, steps=np.int64(steps), every=np.int64(every), raster=np.packbits(raster, axis=1),
+                        V=np.stack(Vs).astype(np.float32), I=np.stack(Is).astype(np.float32),
+                        K_cortical=np.int64(2100))
+    print(f"pd14_neuron: {raster.sum()} spikes in {steps} steps")
+
+
+def philox_triton():
+    os.environ["TRITON_INTERPRET"] = "1"
+    import torch
+    import triton
+    import triton.language as tl
+
+    @triton.jit
+    def kernel(out_ptr, f_ptr, seed, N: tl.constexpr):
+        offs = tl.arange(0, N)
+        a, b, c, d = tl.randint4x(seed, offs)
+        tl.store(out_ptr + offs * 4 + 0, a)
+        tl.store(out_ptr + offs * 4 + 1, b)
+        tl.store(out_ptr + offs * 4 + 2, c)
+        tl.store(out_ptr + offs * 4 + 3, d)
+        tl.store(f_ptr + offs, tl.rand(seed, offs))
+
+    cases = []
+    for seed in (0, 1, 0x1234567890, 0xDEADBEEF00C0FFEE & 0x7FFFFFFFFFFFFFFF):
+        out = torch.zeros(16 * 4, dtype=torch.int32)
+        f = torch.zeros(16, dtype=torch.float32)
+        kernel[(1,)](out, f, seed, 16)
+        words = [[int(x) & 0xFFFFFFFF for x in out[4 * i:4 * i + 4].tolist()] for i in range(16)]
+        cases.append({"seed": seed, "offsets": list(range(16)), "words": words,
+                      "rand": [float(x) for x in f.tolist()]})
+    (HERE / "philox_triton.json").write_text(json.dumps({"triton": triton.__version__, "cases": cases}, indent=1))
+    print(f"philox_triton: {len(cases)} seeds x 16 offsets (triton {triton.__version__})")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", choices=["brunel", "pd14", "philox"])
+    args = ap.parse_args()
+    ref = pathlib.Path(args.reference)
+    if not ref.exists():
+        raise SystemExit(f"the reference tree is not at {ref}: the committed fixtures stand")
+    if args.only in (None, "philox"):
+        philox_triton()
+    if args.only in (None, "brunel"):
+        brunel_c0(ref)
+    if args.only in (None, "pd14"):
+        pd14_neuron(ref)
+
+
+if __name__ == "__main__":
+    main()
