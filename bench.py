@@ -41,6 +41,7 @@ BYTES_PER_NEURON_STEP = 16  # V read + write, arrival slot read + clear
 METRIC = "synaptic events/s"
 UNIT = "events/s"
 WORKLOAD = "brunel_A_config1"
+MODE = "persistent"
 
 
 def measured_peaks() -> tuple[float, str]:
@@ -53,7 +54,7 @@ def measured_peaks() -> tuple[float, str]:
 def config(n_gpus: int) -> dict:
     return {"workload": WORKLOAD, "neurons": 12500, "synapses": 15_625_000, "delays_steps": "U{1..20}", "dt_ms": 0.1,
             "sim_steps_per_step": SIM_STEPS_PER_STEP, "l2": "flushed before every timed step (256 MiB write)",
-            "parallelism": f"replicas x{n_gpus}" if n_gpus > 1 else "single GPU"}
+            "parallelism": f"replicas x{n_gpus}" if n_gpus > 1 else "single GPU", "launch": MODE}
 
 
 class Clocks:
@@ -169,7 +170,14 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="naer2_b200", choices=["naer2_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", choices=["persistent", "per-step"], default="persistent",
+                    help="a window of steps per cooperative launch, or one launch per step")
+    ap.add_argument("--sim-steps", type=int, default=1000,
+                    help="simulation steps per bench step (default 1000; small values for profiling runs)")
     args = ap.parse_args()
+    global SIM_STEPS_PER_STEP, MODE
+    SIM_STEPS_PER_STEP = args.sim_steps
+    MODE = args.mode
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -200,6 +208,7 @@ def main() -> int:
         torch.cuda.synchronize(dev)
 
     net, pops = brunel.build(**brunel.CONFIG1, seed=1 + rank)
+    net.persistent = args.mode == "persistent"
     desc = describe(net) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
     import oracle as _oracle_for_baseline_only  # noqa: F401  (the CPU baseline leg below)
 
@@ -227,8 +236,10 @@ def main() -> int:
         barrier()
     dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     events = rt.counters()["events"] - ev0
-    launches = args.steps * SIM_STEPS_PER_STEP  # step kernels
-    launches_all = launches + args.steps * (SIM_STEPS_PER_STEP // max(net.window, 1))  # + counter advances
+    launches = args.steps * SIM_STEPS_PER_STEP  # simulation steps (one step kernel each, or one window iteration)
+    windows = args.steps * (SIM_STEPS_PER_STEP // max(net.window, 1) + (SIM_STEPS_PER_STEP % max(net.window, 1) > 0))
+    # kernels launched: per-step mode one per step; persistent mode one per window; + one counter advance per window
+    launches_all = (launches if MODE == "per-step" else windows) + windows
     net.check()
 
     # ---- end to end through the public API, host buffers
@@ -293,9 +304,10 @@ def main() -> int:
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "n2b::step_kernel<128>", "bytes_per_launch": alg_bytes,
-                         "us_per_launch": ms_per_launch * 1e3,
-                         "note": "launch time = timed device time / step-kernel launches (graph gaps included)"},
+                         "kernel": ("n2b::persistent_kernel<128>" if MODE == "persistent" else "n2b::step_kernel<128>"),
+                         "bytes_per_launch": alg_bytes, "us_per_launch": ms_per_launch * 1e3,
+                         "note": "per simulation step: timed device time / steps (launch gaps and grid barriers "
+                                 "included)"},
             "gpu_launches": launches_all,
             "clocks": clocks.summary(),
             "events_per_sim_step": ev_per_launch,

@@ -50,6 +50,9 @@ extern "C" {
 /* error words (n2b_status) */
 #define N2B_ERR_PUSH_LINK 0 /* push links with delay 0, delay >= arrival depth, or target >= n */
 #define N2B_ERR_PULL_LINK 1 /* pull links with delay 0, delay >= bit depth, or source >= n */
+#define N2B_ERR_SPLIT 2     /* push links past a row's split with a delay below 2 steps (skipped) */
+#define N2B_ERR_ITEMS 3     /* work-list entries past its capacity (skipped; cannot happen for a valid split) */
+#define N2B_ERR_BARRIER 4   /* persistent windows: a grid barrier wait that gave up after 2 s (the window stopped) */
 #define N2B_ERR_WORDS 8
 
 /* One population: the state arrays and rings of the reference's
@@ -85,7 +88,12 @@ typedef struct n2b_population {
  * link[l] = (delay_steps << 24) | index, delay_steps in 1..255, index < 2^24:
  *   PUSH: rows per source neuron (ptr[n_src + 1]), index = target neuron;
  *   PULL: rows per target neuron (ptr[n_tgt + 1]), index = source neuron.
- * w: per-link weight, or NULL for `weight` on every link. */
+ * w: per-link weight, or NULL for `weight` on every link.
+ * split (PUSH only, optional): per source row, the first link of delay >= 2
+ *   steps, the row's delay-1 links all before it. The spiking neuron's block
+ *   delivers [ptr[s], split[s]) in the step itself; [split[s], ptr[s+1]) goes
+ *   to a work list every block of the next step's launch shares. NULL: the
+ *   spiking neuron's block delivers the whole row. */
 typedef struct n2b_connection {
     int32_t src;
     int32_t tgt;
@@ -96,11 +104,16 @@ typedef struct n2b_connection {
     const int32_t *ptr;
     const uint32_t *link;
     const float *w;
+    const int32_t *split;
 } n2b_connection;
 
 typedef struct n2b_options {
     int32_t block;   /* neurons (threads) per block: 64, 128 or 256 (0: 128) */
     int32_t device;  /* CUDA device ordinal of every pointer */
+    int32_t grid;    /* blocks per launch (0: two per SM; per-step launches: at least one per tile;
+                        persistent: at most the co-resident blocks, each looping over its tiles) */
+    int32_t persistent; /* 1: a window of steps is one cooperative launch, steps separated by a grid
+                           barrier; 0: one launch per step */
 } n2b_options;
 
 typedef struct n2b_net n2b_net;
@@ -137,7 +150,8 @@ int n2b_capture(n2b_net *net, int32_t window_steps, void *stream);
  * steps). Replaces WindowGraph.replay (naer2/graph.py:120-136). */
 int n2b_replay(n2b_net *net, int64_t n_windows, void *stream);
 
-/* Set the step counter (asynchronously, on `stream`). */
+/* Set the step counter (asynchronously, on `stream`); work of the previous
+ * step still in the work list is dropped. */
 int n2b_set_step(n2b_net *net, int64_t step, void *stream);
 
 /* Start recording: raster row r of every population holds step step0 + r
@@ -155,7 +169,8 @@ int n2b_status(n2b_net *net, int32_t *words, int32_t n_words, void *stream);
  * count_received counters (naer2/population.py:134-136). */
 int n2b_counters(n2b_net *net, uint64_t *out, int32_t n_out, void *stream);
 
-/* Zero the error words and counters (on `stream`). */
+/* Zero the error words and counters, and clear a persistent window's abort
+ * (on `stream`). */
 int n2b_reset_counters(n2b_net *net, void *stream);
 
 /* Release the handle (its graph; the caller's buffers stay the caller's). */

@@ -12,7 +12,7 @@ LIB_PATH = pathlib.Path(__file__).resolve().parent / "libnaer2b.so"
 ABI_VERSION = 1
 MODEL_LIF_DELTA, MODEL_PD14, MODEL_POISSON_SOURCE = 1, 2, 3
 PUSH, PULL = 0, 1
-ERR_PUSH_LINK, ERR_PULL_LINK, ERR_WORDS = 0, 1, 8
+ERR_PUSH_LINK, ERR_PULL_LINK, ERR_SPLIT, ERR_ITEMS, ERR_BARRIER, ERR_WORDS = 0, 1, 2, 3, 4, 8
 
 
 class Population(ctypes.Structure):
@@ -31,12 +31,13 @@ class Connection(ctypes.Structure):
     _fields_ = [
         ("src", ctypes.c_int32), ("tgt", ctypes.c_int32), ("mode", ctypes.c_int32), ("n_links", ctypes.c_int32),
         ("weight", ctypes.c_float), ("reserved", ctypes.c_int32),
-        ("ptr", ctypes.c_void_p), ("link", ctypes.c_void_p), ("w", ctypes.c_void_p),
+        ("ptr", ctypes.c_void_p), ("link", ctypes.c_void_p), ("w", ctypes.c_void_p), ("split", ctypes.c_void_p),
     ]
 
 
 class Options(ctypes.Structure):
-    _fields_ = [("block", ctypes.c_int32), ("device", ctypes.c_int32)]
+    _fields_ = [("block", ctypes.c_int32), ("device", ctypes.c_int32), ("grid", ctypes.c_int32),
+                ("persistent", ctypes.c_int32)]
 
 
 # every entry point include/naer2b.h declares: (name, restype, argtypes)

@@ -1,8 +1,11 @@
 // Device side of the fixed-dt hot path: Philox draws, the built-in neuron
-// models, pull intake, and the fused step kernel (update -> spike ring ->
-// push delivery). Written for sm_100a; included by naer2b.cu.
+// models, pull intake, and the fused step kernel. Written for sm_100a;
+// included by naer2b.cu.
 //
-// Layout of one step of one block (a tile of NPB neurons of one population):
+// One step n of a network, in one launch (step_kernel) or as one iteration of
+// a persistent cooperative launch (persistent_kernel, steps separated by a
+// bounded grid barrier). Tiles of NPB neurons of one population are spread
+// over the blocks; every block then shares the far deliveries of step n - 1.
 //   1. intake: each neuron's due arrival slot acc[n mod D][j] (int64 fixed
 //      point, read and cleared), plus every pull connection's gather of its
 //      incoming links against the source's spike-bit ring, plus the external
@@ -11,19 +14,35 @@
 //   3. spike-ring write: one __ballot_sync word per warp into the bit ring
 //      (and the raster), the warp's spikes compacted with __popc into the
 //      block's shared spike list;
-//   4. push delivery: the block walks the outgoing CSR rows of its own
-//      spikes as one flat (spike, link) range and adds each link's weight
-//      into the target's arrival slot (n + delay) mod D with a 64-bit
-//      red.global.add -- exact and order-free, so any interleaving of the
-//      blocks gives the same sums.
-// The next step's kernel starts after this one ends (stream order): every
-// arrival of delay >= 1 is in place before it is read.
+//   4. near delivery: the block walks the delay-1 links of its own spikes
+//      (the head of each outgoing row) as one flat (spike, link) range and
+//      adds each weight into the target's slot (n + 1) mod D with a 64-bit
+//      red.global.add; the rest of each row (delay >= 2) is cut into work
+//      items of NPB links appended to this step's work list;
+//   5. far delivery: every block takes items of step n - 1's list (grid
+//      stride, from the last block down: blocks without a tile first), one
+//      link per thread, into slots (n - 1 + delay) mod D, all >= n + 1:
+//      never the slot this step reads.
+// Integer adds make every interleaving give the same sums. A step's slot is
+// complete when it is read: the previous step ended (launch boundary or grid
+// barrier) after every add into it.
+//
+// Latency is the budget here (a step moves ~1 MB): the tables of small
+// networks ride in the kernel parameters (no dependent load before the state
+// loads), each neuron's outgoing row bounds are loaded with its state, the
+// Poisson inversion is a branch-free count over an inline table, and the far
+// items are taken two at a time.
 #pragma once
 #include <stdint.h>
 
 namespace n2b {
 
 constexpr unsigned FULL = 0xffffffffu;
+constexpr int INLINE_POPS = 16;   // populations whose tables fit the kernel parameters
+constexpr int INLINE_PUSH = 32;
+constexpr int INLINE_PULL = 16;
+constexpr int EXT_INLINE = 32;    // Poisson table entries kept inline
+constexpr int PREFETCH_OUT = 4;   // outgoing push connections whose row bounds are prefetched
 
 // ------------------------------------------------------------------ tables
 
@@ -43,11 +62,12 @@ struct alignas(16) PopDev {
     const uint32_t *ext_table;
     uint32_t *raster;
     long long raster_steps;
+    uint32_t ext_tab[EXT_INLINE];  // the table's first EXT_INLINE entries (all of it when ext_len <= EXT_INLINE)
 };
 
 struct alignas(16) ConnDev {
     int32_t homogeneous, src_n, tgt_n, tgt_acc_mask;
-    int32_t src_bit_mask, src_words, pad0, pad1;
+    int32_t src_bit_mask, src_words, has_split, pad1;
     long long wfx;        // homogeneous weight, fixed point of the target
     float wscale;         // 2^shift of the target (exact)
     float pad2;
@@ -56,19 +76,60 @@ struct alignas(16) ConnDev {
     const float *w;
     long long *tgt_acc;
     const uint32_t *src_bits;
+    const int32_t *split;  // push: per source, its row's first link of delay >= 2 (NULL: none deferred)
 };
 
 struct StepArgs {
-    const PopDev *pops;
+    const PopDev *pops;    // global tables (always valid)
     const ConnDev *push;   // push connections, grouped by source population
     const ConnDev *pull;   // pull connections, grouped by target population
-    const int4 *tiles;     // per block: population, first neuron, neurons
-    const long long *step; // the step counter (advanced after every window)
+    const int4 *tiles;     // per tile: population, first neuron, neurons
+    const long long *step; // the step counter (advanced after every launch)
     const long long *rec0; // raster row 0's step
     int32_t *err;
     unsigned long long *counters;
-    int32_t offset;        // this launch's step = *step + offset
+    int4 *items;           // 3 work lists of item_cap entries: (push connection, first link, end link, 0)
+    int32_t *item_count;   // their lengths; step n appends to list n mod 3, reads n - 1's
+    unsigned *barrier;     // persistent kernel: group counters (one per 128-byte line), then top, generation, abort
+    int32_t item_cap;
+    int32_t n_tiles;
+    int32_t offset;        // this launch's step = *step + offset (per-step launches)
+    int32_t n_pops;
+    int32_t tile_first[INLINE_POPS + 1];  // inline tables: population p owns tiles [tile_first[p], tile_first[p+1])
+    PopDev pops_i[INLINE_POPS];
+    ConnDev push_i[INLINE_PUSH];
+    ConnDev pull_i[INLINE_PULL];
 };
+
+template <bool INL>
+__device__ __forceinline__ const PopDev &pop_at(const StepArgs &a, int k) {
+    return INL ? a.pops_i[k] : a.pops[k];
+}
+template <bool INL>
+__device__ __forceinline__ const ConnDev &push_at(const StepArgs &a, int k) {
+    return INL ? a.push_i[k] : a.push[k];
+}
+template <bool INL>
+__device__ __forceinline__ const ConnDev &pull_at(const StepArgs &a, int k) {
+    return INL ? a.pull_i[k] : a.pull[k];
+}
+
+// (population, first neuron, neurons) of tile t
+template <bool INL, int NPB>
+__device__ __forceinline__ int4 tile_at(const StepArgs &a, int t) {
+    if (!INL) return a.tiles[t];
+    int p = 0;
+    while (p + 1 < a.n_pops && a.tile_first[p + 1] <= t) ++p;
+    const int first = (t - a.tile_first[p]) * NPB;
+    return make_int4(p, first, min(NPB, a.pops_i[p].n - first), 0);
+}
+
+constexpr int BAR_GROUP = 16;     // blocks per first-level barrier counter
+constexpr int BAR_STRIDE = 32;    // words between counters (a 128-byte line each)
+constexpr int BAR_MAX_GROUPS = 256;
+constexpr int BAR_TOP = BAR_MAX_GROUPS * BAR_STRIDE, BAR_GEN = BAR_TOP + BAR_STRIDE, BAR_ABORT = BAR_GEN + BAR_STRIDE;
+constexpr int BAR_WORDS = BAR_ABORT + BAR_STRIDE;
+constexpr unsigned long long BAR_LIMIT_NS = 2000000000ull;  // a barrier wait gives up after 2 s
 
 // ------------------------------------------------------------------ Philox
 
@@ -96,10 +157,16 @@ __device__ __forceinline__ uint32_t draw(const PopDev &P, int j, long long n, ui
                         (uint32_t)((unsigned long long)n >> 32), purpose, P.seed_lo, P.seed_hi);
 }
 
-// Poisson count by inversion against the population's uint32 CDF table.
-__device__ __forceinline__ int poisson_count(const uint32_t *__restrict__ table, int len, uint32_t u) {
+// Poisson count by inversion: how many of the table's first len - 1 entries the uniform word reaches (the
+// table is non-decreasing, so this is the first k with u < table[k]). Branch-free over the inline entries
+// (uniform addresses across the warp), the rest from global memory.
+__device__ __forceinline__ int poisson_count(const PopDev &P, uint32_t u) {
+    const int last = P.ext_len - 1;
     int k = 0;
-    while (k < len - 1 && u >= __ldg(table + k)) ++k;
+    const int m = min(last, EXT_INLINE);
+#pragma unroll 8
+    for (int q = 0; q < m; ++q) k += u >= P.ext_tab[q];
+    for (int q = EXT_INLINE; q < last; ++q) k += u >= __ldg(P.ext_table + q);
     return k;
 }
 
@@ -107,7 +174,7 @@ __device__ __forceinline__ long long weight_fx(float w, float wscale) {
     return __float2ll_rn(__fmul_rn(w, wscale));  // exact scale, nearest-even
 }
 
-// ------------------------------------------------------------------ warp helpers
+// ------------------------------------------------------------------ warp / block helpers
 
 __device__ __forceinline__ int warp_incl_scan(int v) {
     const int lane = threadIdx.x & 31;
@@ -125,49 +192,61 @@ __device__ __forceinline__ long long warp_sum64(long long v) {
     return v;
 }
 
+// Block-wide exclusive scan of one int per thread (NPB threads); the total in *total.
+template <int NPB>
+__device__ __forceinline__ int block_excl_scan(int v, int *s_wsum, int *total) {
+    constexpr int NW = NPB / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int incl = warp_incl_scan(v);
+    if (lane == 31) s_wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int x = lane < NW ? s_wsum[lane] : 0;
+        x = warp_incl_scan(x);
+        if (lane < NW) s_wsum[lane] = x;
+    }
+    __syncthreads();
+    *total = s_wsum[NW - 1];
+    return incl - v + (warp > 0 ? s_wsum[warp - 1] : 0);
+}
+
 // ------------------------------------------------------------------ models
 
 // Brunel's time-driven LIF (tools/brunel_reference.py:36-42 of the reference):
 // refractory neurons keep V and drop their input; otherwise V = V*decay + in,
 // fire at V >= theta, reset, refractory for ref_steps.
-__device__ __forceinline__ bool lif_delta(const PopDev &P, int j, float in) {
-    int ref = P.ref[j];
+__device__ __forceinline__ bool lif_delta(const PopDev &P, float in, float &v, int &ref) {
     if (ref > 0) {
-        P.ref[j] = ref - 1;
+        ref -= 1;
         return false;
     }
-    float v = __fadd_rn(__fmul_rn(P.v[j], P.p[0]), in);
+    v = __fadd_rn(__fmul_rn(v, P.p[0]), in);
     const bool fire = v >= P.p[1];
     if (fire) {
         v = P.p[2];
-        P.ref[j] = P.ref_steps;
+        ref = P.ref_steps;
     }
-    P.v[j] = v;
     return fire;
 }
 
 // PD14's LIF with exponential current synapses at fixed dt (reference
 // test/networks/PD14/neuron.py:166-186): receive adds into the current, the
 // exact propagators advance V and the current, threshold V > V_thresh.
-__device__ __forceinline__ bool pd14(const PopDev &P, int j, float in) {
-    float cur = __fadd_rn(P.i[j], in);
-    float v;
-    const int ref = P.ref[j];
+__device__ __forceinline__ bool pd14(const PopDev &P, float in, float &v, float &cur, int &ref) {
+    cur = __fadd_rn(cur, in);
     if (ref > 0) {
-        P.ref[j] = ref - 1;
+        ref -= 1;
         v = P.p[5];
     } else {
-        const float a = __fmul_rn(P.p[0], __fsub_rn(P.v[j], P.p[3]));
+        const float a = __fmul_rn(P.p[0], __fsub_rn(v, P.p[3]));
         v = __fadd_rn(__fadd_rn(P.p[3], a), __fmul_rn(P.p[2], cur));
     }
     cur = __fmul_rn(P.p[1], cur);
     const bool fire = v > P.p[4];
     if (fire) {
         v = P.p[5];
-        P.ref[j] = P.ref_steps;
+        ref = P.ref_steps;
     }
-    P.v[j] = v;
-    P.i[j] = cur;
     return fire;
 }
 
@@ -177,6 +256,7 @@ __device__ __forceinline__ bool pd14(const PopDev &P, int j, float in) {
 // rows of its 32 neurons one after another, the lanes striding a row
 // (coalesced link loads), testing each link's source bit in the ring row of
 // step n - delay; the warp's sum lands in the row's owner lane.
+template <bool INL>
 __device__ __forceinline__ long long pull_intake(const StepArgs &a, const PopDev &P, int first, int count,
                                                  long long n) {
     const int lane = threadIdx.x & 31;
@@ -184,7 +264,7 @@ __device__ __forceinline__ long long pull_intake(const StepArgs &a, const PopDev
     const int nq = min(32, first + count - wbase);
     long long mine = 0;
     for (int c = P.pull_first; c < P.pull_first + P.n_pull; ++c) {
-        const ConnDev C = a.pull[c];
+        const ConnDev &C = pull_at<INL>(a, c);
         for (int q = 0; q < nq; ++q) {
             const int jq = wbase + q;
             const int r0 = __ldg(C.ptr + jq), r1 = __ldg(C.ptr + jq + 1);
@@ -194,7 +274,7 @@ __device__ __forceinline__ long long pull_intake(const StepArgs &a, const PopDev
                 const int d = (int)(rec >> 24), s = (int)(rec & 0xFFFFFFu);
                 if (d >= 1 && d <= C.src_bit_mask && s < C.src_n) {
                     const uint32_t word =
-                        __ldg(C.src_bits + (size_t)((n - d) & C.src_bit_mask) * C.src_words + (s >> 5));
+                        __ldcg(C.src_bits + (size_t)((n - d) & C.src_bit_mask) * C.src_words + (s >> 5));
                     if ((word >> (s & 31)) & 1u)
                         part += C.homogeneous ? C.wfx : weight_fx(__ldg(C.w + l), C.wscale);
                 } else {
@@ -208,42 +288,140 @@ __device__ __forceinline__ long long pull_intake(const StepArgs &a, const PopDev
     return mine;
 }
 
-// ------------------------------------------------------------------ the step kernel
+// ------------------------------------------------------------------ delivery
 
+// One link word into the target's arrival slot (n + delay) mod D; out-of-range links counted, not written.
+__device__ __forceinline__ void deliver_rec(const StepArgs &a, const ConnDev &C, uint32_t rec, int l, long long n,
+                                            int min_delay) {
+    const int d = (int)(rec >> 24), t = (int)(rec & 0xFFFFFFu);
+    if (d < min_delay) {
+        atomicAdd(a.err + 2, 1);  // a deferred link below 2 steps would land in a slot already read
+        return;
+    }
+    if (d > C.tgt_acc_mask || t >= C.tgt_n) {
+        atomicAdd(a.err + 0, 1);
+        return;
+    }
+    const long long wfx = C.homogeneous ? C.wfx : weight_fx(__ldg(C.w + l), C.wscale);
+    atomicAdd(reinterpret_cast<unsigned long long *>(C.tgt_acc + (size_t)((n + d) & C.tgt_acc_mask) * (size_t)C.tgt_n + t),
+              (unsigned long long)wfx);
+}
+
+// Row bounds of neuron j in an outgoing push connection: first link, split, end.
+struct Row {
+    int r0, sp, r1;
+};
+
+__device__ __forceinline__ Row row_of(const ConnDev &C, int j) {
+    Row r;
+    r.r0 = __ldg(C.ptr + j);
+    r.r1 = __ldg(C.ptr + j + 1);
+    r.sp = C.has_split ? min(max(__ldg(C.split + j), r.r0), r.r1) : r.r1;
+    return r;
+}
+
+// The block's spikes of one outgoing push connection: the spiking threads append their far items (their
+// atomic's latency hidden under the near walk), the block walks the near links as one flat range.
 template <int NPB>
-__global__ void __launch_bounds__(NPB) step_kernel(const StepArgs a) {
-    constexpr int NW = NPB / 32;
+__device__ __forceinline__ void deliver_spikes(const StepArgs &a, const ConnDev &C, int c, const Row &row, bool fire,
+                                               int pos, int cnt, long long n, int *s_row, int *s_off, int *s_wsum) {
+    const int tid = threadIdx.x, lane = tid & 31;
+    // events are counted when they are emitted (here), near and far alike
+    const int row_len = fire ? row.r1 - row.r0 : 0;
+    const int warp_links = __reduce_add_sync(FULL, row_len);
+    if (lane == 0 && warp_links) atomicAdd(a.counters + 0, (unsigned long long)warp_links);
+    int n_items = 0, at = 0;
+    if (fire) {
+        s_row[pos] = row.r0;
+        s_off[pos] = row.sp - row.r0;  // near links, scanned below
+        n_items = (row.r1 - row.sp + NPB - 1) / NPB;
+        if (n_items > 0) at = atomicAdd(a.item_count + (int)(n % 3), n_items);
+    }
+    __syncthreads();
+    const int near = tid < cnt ? s_off[tid] : 0;
+    int total = 0;
+    const int off = block_excl_scan<NPB>(near, s_wsum, &total);
+    if (tid < cnt) s_off[tid] = off;
+    if (tid == 0) s_off[cnt] = total;
+    __syncthreads();
+    for (int idx = tid; idx < total; idx += NPB) {
+        int lo = 0, hi = cnt;  // s_off[lo] <= idx < s_off[hi]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_off[mid] <= idx) lo = mid; else hi = mid;
+        }
+        const int l = s_row[lo] + (idx - s_off[lo]);
+        deliver_rec(a, C, __ldg(C.link + l), l, n, 1);
+    }
+    if (n_items > 0) {
+        int4 *list = a.items + (size_t)(n % 3) * (size_t)a.item_cap;
+        for (int k = 0; k < n_items; ++k) {
+            if (at + k < a.item_cap) {
+                const int l0 = row.sp + k * NPB;
+                list[at + k] = make_int4(c, l0, min(l0 + NPB, row.r1), 0);
+            } else {
+                atomicAdd(a.err + 3, 1);
+            }
+        }
+    }
+    __syncthreads();  // s_row / s_off free for the next connection
+}
+
+// ------------------------------------------------------------------ one tile of one step
+
+template <int NPB, bool INL>
+__device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n, const int4 tile) {
     __shared__ int s_cnt;
-    __shared__ int s_spk[NPB];
     __shared__ int s_row[NPB];
     __shared__ int s_off[NPB + 1];
-    __shared__ int s_wsum[NW];
+    __shared__ int s_wsum[NPB / 32];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int4 tile = a.tiles[blockIdx.x];
-    const PopDev P = a.pops[tile.x];  // a register copy: the state stores cannot alias it
-    const long long n = *a.step + a.offset;
+    const PopDev &P = pop_at<INL>(a, tile.x);
     const int j = tile.y + tid;
     const bool live = tid < tile.z;
+    __syncthreads();  // a block's previous tile: every thread past its reads of the shared arrays
     if (tid == 0) s_cnt = 0;
+
+    // state and outgoing row bounds together: none of these loads waits for another
+    const int model = P.model;
+    float v = 0.f, cur = 0.f;
+    int ref = 0;
+    long long acc = 0;
+    long long *slot = nullptr;
+    Row rows[PREFETCH_OUT] = {};
+    const int n_out = P.n_out;
+    if (live) {
+        if (model != 3) {
+            slot = P.acc + (size_t)(n & P.acc_mask) * (size_t)P.n + j;
+            acc = __ldcg(slot);  // L2: other blocks' adds of this kernel are there, not in this SM's L1
+            v = P.v[j];
+            ref = P.ref[j];
+            if (model == 2) cur = P.i[j];
+        }
+#pragma unroll
+        for (int c = 0; c < PREFETCH_OUT; ++c)
+            if (c < n_out) rows[c] = row_of(push_at<INL>(a, P.out_first + c), j);
+    }
 
     // 1-2. intake and update
     bool fire = false;
-    const int model = P.model;
     if (model == 3) {  // N2B_MODEL_POISSON_SOURCE
         fire = live && draw(P, j, n, 1u) < P.fire_threshold;
     } else {
-        long long acc = 0;
+        if (P.n_pull > 0) acc += pull_intake<INL>(a, P, tile.y, tile.z, n);
         if (live) {
-            long long *slot = P.acc + (size_t)(n & P.acc_mask) * (size_t)P.n + j;
-            acc = *slot;
             *slot = 0;
-        }
-        if (P.n_pull > 0) acc += pull_intake(a, P, tile.y, tile.z, n);
-        if (live) {
-            if (P.ext_len > 0) acc += (long long)poisson_count(P.ext_table, P.ext_len, draw(P, j, n, 0u)) * P.ext_wfx;
+            if (P.ext_len > 0) acc += (long long)poisson_count(P, draw(P, j, n, 0u)) * P.ext_wfx;
             const float in = __fmul_rn(__ll2float_rn(acc), P.inv_scale);
-            fire = (model == 1) ? lif_delta(P, j, in) : pd14(P, j, in);
+            if (model == 1) {
+                fire = lif_delta(P, in, v, ref);
+            } else {
+                fire = pd14(P, in, v, cur, ref);
+                P.i[j] = cur;
+            }
+            P.v[j] = v;
+            P.ref[j] = ref;
         }
     }
 
@@ -261,7 +439,7 @@ __global__ void __launch_bounds__(NPB) step_kernel(const StepArgs a) {
     int base = 0;
     if (lane == 0 && b) base = atomicAdd(&s_cnt, __popc(b));
     base = __shfl_sync(FULL, base, 0);
-    if (fire) s_spk[base + __popc(b & ((1u << lane) - 1u))] = j;
+    const int pos = base + __popc(b & ((1u << lane) - 1u));
     __syncthreads();
     const int cnt = s_cnt;
     if (cnt == 0) return;
@@ -270,49 +448,113 @@ __global__ void __launch_bounds__(NPB) step_kernel(const StepArgs a) {
         atomicAdd(a.counters + 2 + P.index, (unsigned long long)cnt);
     }
 
-    // 4. push delivery of the block's spikes, one flat (spike, link) range per connection
-    for (int c = P.out_first; c < P.out_first + P.n_out; ++c) {
-        const ConnDev C = a.push[c];
-        int deg = 0;
-        if (tid < cnt) {
-            const int s = s_spk[tid];
-            const int r0 = __ldg(C.ptr + s);
-            deg = __ldg(C.ptr + s + 1) - r0;
-            s_row[tid] = r0;
-        }
-        const int incl = warp_incl_scan(deg);
-        if (lane == 31) s_wsum[warp] = incl;
-        __syncthreads();
-        if (warp == 0) {
-            int v = lane < NW ? s_wsum[lane] : 0;
-            v = warp_incl_scan(v);
-            if (lane < NW) s_wsum[lane] = v;
-        }
-        __syncthreads();
-        if (tid < cnt) s_off[tid] = incl - deg + (warp > 0 ? s_wsum[warp - 1] : 0);
-        if (tid == 0) s_off[cnt] = s_wsum[NW - 1];
-        __syncthreads();
-        const int total = s_off[cnt];
-        const size_t tn = (size_t)C.tgt_n;
-        for (int idx = tid; idx < total; idx += NPB) {
-            int lo = 0, hi = cnt;  // s_off[lo] <= idx < s_off[hi]
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (s_off[mid] <= idx) lo = mid; else hi = mid;
+    // 4. the spikes' outgoing rows
+#pragma unroll
+    for (int c = 0; c < PREFETCH_OUT; ++c)
+        if (c < n_out)
+            deliver_spikes<NPB>(a, push_at<INL>(a, P.out_first + c), P.out_first + c, rows[c], fire, pos, cnt, n,
+                                s_row, s_off, s_wsum);
+    for (int c = PREFETCH_OUT; c < n_out; ++c) {
+        const ConnDev &C = push_at<INL>(a, P.out_first + c);
+        const Row r = fire ? row_of(C, j) : Row{0, 0, 0};
+        deliver_spikes<NPB>(a, C, P.out_first + c, r, fire, pos, cnt, n, s_row, s_off, s_wsum);
+    }
+}
+
+// 5. the far links of step n - 1: items of NPB links, one link per thread, two items at a time
+template <int NPB, bool INL>
+__device__ __forceinline__ void far_phase(const StepArgs &a, const long long n) {
+    const long long m = n - 1;
+    const int lst = (int)(((m % 3) + 3) % 3);
+    const int count = min(__ldcg(a.item_count + lst), a.item_cap);
+    const int4 *list = a.items + (size_t)lst * (size_t)a.item_cap;
+    const int G = gridDim.x;
+    for (int i = G - 1 - (int)blockIdx.x; i < count; i += 2 * G) {
+        const int4 it0 = __ldcg(list + i);
+        const bool two = i + G < count;
+        const int4 it1 = two ? __ldcg(list + i + G) : make_int4(0, 0, 0, 0);
+        const int l0 = it0.y + (int)threadIdx.x, l1 = it1.y + (int)threadIdx.x;
+        const ConnDev &C0 = push_at<INL>(a, it0.x);
+        const ConnDev &C1 = push_at<INL>(a, it1.x);
+        const bool h0 = l0 < it0.z, h1 = two && l1 < it1.z;
+        const uint32_t rec0 = h0 ? __ldg(C0.link + l0) : 0u;
+        const uint32_t rec1 = h1 ? __ldg(C1.link + l1) : 0u;
+        if (h0) deliver_rec(a, C0, rec0, l0, m, 2);
+        if (h1) deliver_rec(a, C1, rec1, l1, m, 2);
+    }
+}
+
+template <int NPB, bool INL>
+__device__ __forceinline__ void step_body(const StepArgs &a, const long long n) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.item_count + (int)((n + 1) % 3), 0);  // step n + 1's list
+    for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) tile_phase<NPB, INL>(a, n, tile_at<INL, NPB>(a, t));
+    far_phase<NPB, INL>(a, n);
+}
+
+// One step per launch: the launch boundary is the step's barrier.
+template <int NPB, bool INL>
+__global__ void __launch_bounds__(NPB) step_kernel(const __grid_constant__ StepArgs a) {
+    step_body<NPB, INL>(a, *a.step + a.offset);
+}
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid-wide barrier of a cooperative launch: the blocks arrive on counters of BAR_GROUP blocks, the last
+// of each group on the top counter, the last of all bumps the generation the others wait on. Every wait is
+// bounded (BAR_LIMIT_NS): a timeout sets error word 4 and the abort word, and the kernel winds down instead
+// of hanging. Returns false once aborted.
+__device__ __forceinline__ bool grid_sync(const StepArgs &a) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned *bar = a.barrier;
+        volatile unsigned *gen = bar + BAR_GEN;
+        volatile unsigned *abort = bar + BAR_ABORT;
+        const unsigned g = *gen;
+        __threadfence();  // this block's writes before its arrival
+        const unsigned grp = blockIdx.x / BAR_GROUP;
+        const unsigned n_groups = (gridDim.x + BAR_GROUP - 1) / BAR_GROUP;
+        const unsigned members = min((unsigned)BAR_GROUP, gridDim.x - grp * BAR_GROUP);
+        int ok = 1;
+        if (atomicAdd(bar + grp * BAR_STRIDE, 1u) == members - 1) {
+            atomicExch(bar + grp * BAR_STRIDE, 0u);  // every member has arrived: ready for the next barrier
+            __threadfence();
+            if (atomicAdd(bar + BAR_TOP, 1u) == n_groups - 1) {
+                atomicExch(bar + BAR_TOP, 0u);
+                __threadfence();
+                atomicAdd(bar + BAR_GEN, 1u);
             }
-            const int l = s_row[lo] + (idx - s_off[lo]);
-            const uint32_t rec = __ldg(C.link + l);
-            const int d = (int)(rec >> 24), t = (int)(rec & 0xFFFFFFu);
-            const long long wfx = C.homogeneous ? C.wfx : weight_fx(__ldg(C.w + l), C.wscale);
-            if (d >= 1 && d <= C.tgt_acc_mask && t < C.tgt_n) {
-                atomicAdd(reinterpret_cast<unsigned long long *>(C.tgt_acc + (size_t)((n + d) & C.tgt_acc_mask) * tn + t),
-                          (unsigned long long)wfx);
-            } else {
-                atomicAdd(a.err + 0, 1);
-            }
         }
-        if (tid == 0) atomicAdd(a.counters + 0, (unsigned long long)total);
-        __syncthreads();
+        const unsigned long long t0 = globaltimer();
+        while (*gen == g) {
+            if (*abort) { ok = 0; break; }
+            if (globaltimer() - t0 > BAR_LIMIT_NS) {
+                atomicExch(bar + BAR_ABORT, 1u);
+                atomicAdd(a.err + 4, 1);
+                ok = 0;
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();  // the other blocks' writes before this block's next reads
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// A window of n_steps steps in one cooperative launch (every block resident), steps separated by grid_sync.
+template <int NPB, bool INL>
+__global__ void __launch_bounds__(NPB) persistent_kernel(const __grid_constant__ StepArgs a, const int n_steps) {
+    if (*(volatile unsigned *)(a.barrier + BAR_ABORT)) return;  // an earlier window gave up: nothing runs
+    const long long n0 = *a.step;
+    for (int k = 0; k < n_steps; ++k) {
+        step_body<NPB, INL>(a, n0 + k);
+        if (!grid_sync(a)) return;
     }
 }
 
@@ -321,6 +563,10 @@ __global__ void set_kernel(long long *p, long long value) { *p = value; }
 __global__ void zero_kernel(int32_t *err, int n_err, unsigned long long *counters, int n_counters) {
     for (int k = threadIdx.x; k < n_err; k += blockDim.x) err[k] = 0;
     for (int k = threadIdx.x; k < n_counters; k += blockDim.x) counters[k] = 0;
+}
+__global__ void set_step_kernel(long long *step, long long value, int32_t *item_count) {
+    *step = value;
+    item_count[0] = item_count[1] = item_count[2] = 0;
 }
 
 }  // namespace n2b

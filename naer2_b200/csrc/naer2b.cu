@@ -41,8 +41,8 @@ bool pow2(int32_t x) { return x > 0 && (x & (x - 1)) == 0; }
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 struct Layout {
-    size_t pops, push, pull, tiles, step, rec0, err, counters, total;
-    int32_t n_push, n_pull, n_tiles;
+    size_t pops, push, pull, tiles, step, rec0, err, counters, items, item_count, barrier, total;
+    int32_t n_push, n_pull, n_tiles, item_cap;
 };
 
 int32_t block_of(const n2b_options *opt) {
@@ -53,7 +53,14 @@ int32_t block_of(const n2b_options *opt) {
 Layout layout(const n2b_population *pops, int32_t n_pops, const n2b_connection *conns, int32_t n_conns,
               int32_t block) {
     Layout L{};
-    for (int32_t c = 0; c < n_conns; ++c) (conns[c].mode == N2B_PULL ? L.n_pull : L.n_push) += 1;
+    // work items of one step at most: every row's deferred links in items of `block` links, every source firing
+    int64_t cap = 1;
+    for (int32_t c = 0; c < n_conns; ++c) {
+        (conns[c].mode == N2B_PULL ? L.n_pull : L.n_push) += 1;
+        if (conns[c].mode == N2B_PUSH && conns[c].split)
+            cap += (int64_t)conns[c].n_links / block + pops[conns[c].src].n + 1;
+    }
+    L.item_cap = (int32_t)std::min<int64_t>(cap, (int64_t)1 << 30);
     for (int32_t p = 0; p < n_pops; ++p) L.n_tiles += (pops[p].n + block - 1) / block;
     size_t o = 0;
     L.pops = o; o = align256(o + sizeof(n2b::PopDev) * std::max(n_pops, 1));
@@ -64,6 +71,9 @@ Layout layout(const n2b_population *pops, int32_t n_pops, const n2b_connection *
     L.rec0 = o; o = align256(o + sizeof(long long));
     L.err = o; o = align256(o + sizeof(int32_t) * N2B_ERR_WORDS);
     L.counters = o; o = align256(o + sizeof(unsigned long long) * (2 + std::max(n_pops, 1)));
+    L.item_count = o; o = align256(o + sizeof(int32_t) * 3);
+    L.items = o; o = align256(o + sizeof(int4) * 3 * (size_t)L.item_cap);
+    L.barrier = o; o = align256(o + sizeof(unsigned) * n2b::BAR_WORDS);
     L.total = o;
     return L;
 }
@@ -109,6 +119,8 @@ int validate(const n2b_population *pops, int32_t n_pops, const n2b_connection *c
         if (T.n > 0 && (!T.acc || !pow2(T.acc_depth))) return fail(N2B_EINVAL, at + "target has no arrival slots");
         if (C.mode == N2B_PULL && S.n > 0 && (!S.bits || !pow2(S.bit_depth)))
             return fail(N2B_EINVAL, at + "a pull connection needs the source's spike-bit ring");
+        if (C.mode == N2B_PULL && C.split) return fail(N2B_EINVAL, at + "split is for push connections");
+        if (S.n > 0 && (int64_t)C.n_links > ((int64_t)1 << 31) - 1) return fail(N2B_EINVAL, at + "more than 2^31 links");
     }
     return N2B_OK;
 }
@@ -118,6 +130,9 @@ int validate(const n2b_population *pops, int32_t n_pops, const n2b_connection *c
 struct n2b_net {
     int device = 0;
     int32_t block = 128;
+    int32_t grid = 0;
+    int32_t persistent = 0;
+    int32_t inl = 0;  // tables in the kernel parameters
     int32_t n_pops = 0;
     Layout L{};
     char *ws = nullptr;
@@ -129,20 +144,59 @@ struct n2b_net {
 
 namespace {
 
+template <int NPB, bool INL>
+cudaError_t launch_one(n2b_net *net, int64_t n_steps, cudaStream_t s) {
+    if (net->persistent) {
+        int32_t k = (int32_t)n_steps;
+        void *args[] = {(void *)&net->args, (void *)&k};
+        return cudaLaunchCooperativeKernel((const void *)n2b::persistent_kernel<NPB, INL>, dim3(net->grid), dim3(NPB),
+                                           args, 0, s);
+    }
+    n2b::StepArgs &a = net->args;
+    for (int64_t k = 0; k < n_steps; ++k) {
+        a.offset = (int32_t)k;
+        n2b::step_kernel<NPB, INL><<<net->grid, NPB, 0, s>>>(a);
+    }
+    a.offset = 0;
+    return cudaGetLastError();
+}
+
+template <bool INL>
+cudaError_t launch_block(n2b_net *net, int64_t n_steps, cudaStream_t s) {
+    switch (net->block) {
+        case 64: return launch_one<64, INL>(net, n_steps, s);
+        case 256: return launch_one<256, INL>(net, n_steps, s);
+        default: return launch_one<128, INL>(net, n_steps, s);
+    }
+}
+
 cudaError_t launch_steps(n2b_net *net, int64_t n_steps, cudaStream_t s) {
-    if (net->L.n_tiles > 0) {
-        n2b::StepArgs a = net->args;
-        for (int64_t k = 0; k < n_steps; ++k) {
-            a.offset = (int32_t)k;
-            switch (net->block) {
-                case 64: n2b::step_kernel<64><<<net->L.n_tiles, 64, 0, s>>>(a); break;
-                case 256: n2b::step_kernel<256><<<net->L.n_tiles, 256, 0, s>>>(a); break;
-                default: n2b::step_kernel<128><<<net->L.n_tiles, 128, 0, s>>>(a); break;
-            }
-        }
+    if (net->L.n_tiles > 0 && n_steps > 0) {
+        cudaError_t e = net->inl ? launch_block<true>(net, n_steps, s) : launch_block<false>(net, n_steps, s);
+        if (e != cudaSuccess) return e;
     }
     n2b::advance_kernel<<<1, 1, 0, s>>>(reinterpret_cast<long long *>(net->ws + net->L.step), n_steps);
     return cudaGetLastError();
+}
+
+template <int NPB, bool INL>
+cudaError_t occupancy(int *per_sm) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, n2b::persistent_kernel<NPB, INL>, NPB, 0);
+}
+
+int coresident_blocks(int32_t block, bool inl, int device, int *out) {
+    int per_sm = 0, sms = 0;
+    cudaError_t e = cudaSuccess;
+    switch (block) {
+        case 64: e = inl ? occupancy<64, true>(&per_sm) : occupancy<64, false>(&per_sm); break;
+        case 256: e = inl ? occupancy<256, true>(&per_sm) : occupancy<256, false>(&per_sm); break;
+        default: e = inl ? occupancy<128, true>(&per_sm) : occupancy<128, false>(&per_sm); break;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+    *out = per_sm * sms;
+    return N2B_OK;
 }
 
 void drop_graph(n2b_net *net) {
@@ -234,6 +288,8 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
         D.w = C.w;
         D.tgt_acc = reinterpret_cast<long long *>(T.acc);
         D.src_bits = S.bits;
+        D.has_split = C.mode == N2B_PUSH && C.split != nullptr;
+        D.split = C.mode == N2B_PUSH ? C.split : nullptr;
         return D;
     };
     for (int32_t p = 0; p < n_pops; ++p) {
@@ -255,6 +311,13 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
 
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     char *ws = static_cast<char *>(workspace);
+    // the first entries of every Poisson table, inline (read back once)
+    for (int32_t p = 0; p < n_pops; ++p) {
+        const int32_t k = std::min(pops[p].ext_len, n2b::EXT_INLINE);
+        if (pops[p].n > 0 && k > 0)
+            N2B_CUDA(cudaMemcpyAsync(pd[p].ext_tab, pops[p].ext_table, sizeof(uint32_t) * k, cudaMemcpyDeviceToHost, s));
+    }
+    N2B_CUDA(cudaStreamSynchronize(s));
     if (n_pops) N2B_CUDA(cudaMemcpyAsync(ws + L.pops, pd.data(), sizeof(n2b::PopDev) * n_pops, cudaMemcpyHostToDevice, s));
     if (!push.empty())
         N2B_CUDA(cudaMemcpyAsync(ws + L.push, push.data(), sizeof(n2b::ConnDev) * push.size(), cudaMemcpyHostToDevice, s));
@@ -262,17 +325,37 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
         N2B_CUDA(cudaMemcpyAsync(ws + L.pull, pull.data(), sizeof(n2b::ConnDev) * pull.size(), cudaMemcpyHostToDevice, s));
     if (!tiles.empty())
         N2B_CUDA(cudaMemcpyAsync(ws + L.tiles, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, s));
-    n2b::set_kernel<<<1, 1, 0, s>>>(reinterpret_cast<long long *>(ws + L.step), 0);
+    n2b::set_step_kernel<<<1, 1, 0, s>>>(reinterpret_cast<long long *>(ws + L.step), 0,
+                                         reinterpret_cast<int32_t *>(ws + L.item_count));
     n2b::set_kernel<<<1, 1, 0, s>>>(reinterpret_cast<long long *>(ws + L.rec0), 0);
     n2b::zero_kernel<<<1, 64, 0, s>>>(reinterpret_cast<int32_t *>(ws + L.err), N2B_ERR_WORDS,
                                       reinterpret_cast<unsigned long long *>(ws + L.counters), 2 + n_pops);
+    N2B_CUDA(cudaMemsetAsync(ws + L.barrier, 0, sizeof(unsigned) * n2b::BAR_WORDS, s));
     N2B_CUDA(cudaGetLastError());
     // the host images are read by the copies above: wait for them before they go
     N2B_CUDA(cudaStreamSynchronize(s));
 
+    int sms = 0;
+    N2B_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int persistent = opt && opt->persistent;
+    const bool inl = n_pops <= n2b::INLINE_POPS && (int32_t)push.size() <= n2b::INLINE_PUSH &&
+                     (int32_t)pull.size() <= n2b::INLINE_PULL;
+    int want = (opt && opt->grid > 0) ? opt->grid : 2 * sms;
+    int grid = std::max(L.n_tiles, want);
+    if (persistent) {
+        int most = 0;
+        int rc2 = coresident_blocks(block, inl, device, &most);
+        if (rc2) return rc2;
+        if (most < 1) return fail(N2B_ECUDA, "the persistent kernel cannot be resident");
+        grid = std::min(std::min(want, most), n2b::BAR_MAX_GROUPS * n2b::BAR_GROUP);
+        grid = std::max(grid, 1);
+    }
     n2b_net *net = new n2b_net();
     net->device = device;
     net->block = block;
+    net->persistent = persistent;
+    net->inl = inl;
+    net->grid = grid;
     net->n_pops = n_pops;
     net->L = L;
     net->ws = ws;
@@ -285,7 +368,25 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     a.rec0 = reinterpret_cast<const long long *>(ws + L.rec0);
     a.err = reinterpret_cast<int32_t *>(ws + L.err);
     a.counters = reinterpret_cast<unsigned long long *>(ws + L.counters);
+    a.items = reinterpret_cast<int4 *>(ws + L.items);
+    a.item_count = reinterpret_cast<int32_t *>(ws + L.item_count);
+    a.item_cap = L.item_cap;
+    a.n_tiles = L.n_tiles;
     a.offset = 0;
+    a.barrier = reinterpret_cast<unsigned *>(ws + L.barrier);
+    a.n_pops = n_pops;
+    if (inl) {
+        // inline: tiles in population order (the global table lists the largest populations first)
+        int32_t t = 0;
+        for (int32_t p = 0; p < n_pops; ++p) {
+            a.tile_first[p] = t;
+            t += (pops[p].n + block - 1) / block;
+            a.pops_i[p] = pd[p];
+        }
+        a.tile_first[n_pops] = t;
+        for (size_t c = 0; c < push.size(); ++c) a.push_i[c] = push[c];
+        for (size_t c = 0; c < pull.size(); ++c) a.pull_i[c] = pull[c];
+    }
     *out = net;
     return N2B_OK;
 }
@@ -340,8 +441,8 @@ int n2b_set_step(n2b_net *net, int64_t step, void *stream) {
     if (!net) return fail(N2B_EINVAL, "net is NULL");
     if (step < 0) return fail(N2B_EINVAL, "step < 0");
     N2B_CUDA(cudaSetDevice(net->device));
-    n2b::set_kernel<<<1, 1, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-        reinterpret_cast<long long *>(net->ws + net->L.step), step);
+    n2b::set_step_kernel<<<1, 1, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<long long *>(net->ws + net->L.step), step, reinterpret_cast<int32_t *>(net->ws + net->L.item_count));
     N2B_CUDA(cudaGetLastError());
     return N2B_OK;
 }
@@ -384,6 +485,8 @@ int n2b_reset_counters(n2b_net *net, void *stream) {
     n2b::zero_kernel<<<1, 64, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         reinterpret_cast<int32_t *>(net->ws + net->L.err), N2B_ERR_WORDS,
         reinterpret_cast<unsigned long long *>(net->ws + net->L.counters), 2 + net->n_pops);
+    N2B_CUDA(cudaMemsetAsync(net->ws + net->L.barrier, 0, sizeof(unsigned) * n2b::BAR_WORDS,
+                             reinterpret_cast<cudaStream_t>(stream)));
     N2B_CUDA(cudaGetLastError());
     return N2B_OK;
 }

@@ -25,6 +25,10 @@ class Network:
         self.resolution: float = 0.1  # the step dt (ms)
         self.window: int = 100  # steps per captured graph
         self.block: int | None = None  # neurons per block (None: the smallest population group_size)
+        self.grid: int | None = None  # blocks per launch (None: two per SM)
+        # a window of steps as one persistent cooperative launch (steps separated by a grid barrier), or one
+        # launch per step
+        self.persistent: bool = True
         self.device = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else None
         self.record_steps: int = 0  # raster rows kept per population (Network.record)
         self.tuned: dict = {}  # per connection id: the push/pull choice the tuner measured (runtime.tune)

@@ -32,7 +32,7 @@ import torch
 
 from . import _lib
 from .models import params_of
-from .topology import delay_steps, pull_form, push_form
+from .topology import delay_steps, pack_links, pull_form, push_form
 
 MAX_SHIFT = 40
 
@@ -98,7 +98,8 @@ class ConnDesc:
     link: np.ndarray      # uint32: delay << 24 | index
     weight: float         # when w is None
     w: np.ndarray | None  # fp32 per link, in the form's order
-    push_ptr: np.ndarray = field(default=None)   # the canonical (push) form, for checks
+    split: np.ndarray | None = field(default=None)  # push: per row its first link of delay >= 2
+    push_ptr: np.ndarray = field(default=None)   # the canonical order, rows per source (for checks)
     push_link: np.ndarray = field(default=None)
     push_w: np.ndarray | None = field(default=None)
 
@@ -168,17 +169,19 @@ def describe(net, modes: dict | None = None) -> NetDesc:
     cdesc = []
     for s, t, topo, steps, wscalar, warr, mode in cinfo:
         n_tgt = len(pops[t].shape)
-        push_ptr, push_link = push_form(topo, steps, n_tgt)
+        canon_ptr = topo.source_offsets.numpy().astype(np.int32)
+        canon_link = pack_links(topo.target_indices.numpy(), steps)
+        split = None
         if mode == "pull":
             ptr, link, perm = pull_form(topo, steps, n_tgt)
-            w = warr[perm] if warr is not None else None
         elif mode == "push":
-            ptr, link, w = push_ptr, push_link, warr
+            ptr, link, perm, split = push_form(topo, steps, n_tgt)
         else:
             raise ValueError(f"unknown connection mode {mode!r}")
+        w = warr[perm] if warr is not None else None
         cdesc.append(ConnDesc(src=s, tgt=t, mode=mode, n_links=len(topo), ptr=ptr, link=link,
-                              weight=wscalar if wscalar is not None else 0.0, w=w,
-                              push_ptr=push_ptr, push_link=push_link, push_w=warr))
+                              weight=wscalar if wscalar is not None else 0.0, w=w, split=split,
+                              push_ptr=canon_ptr, push_link=canon_link, push_w=warr))
     return NetDesc(dt=dt, pops=pdesc, conns=cdesc, n_links=sum(c.n_links for c in cdesc))
 
 
@@ -244,12 +247,15 @@ class NetworkRuntime:
             cc.link = dev_tensor(torch.from_numpy(link.view(np.int32).copy())).data_ptr()
             cc.weight = c.weight
             cc.w = dev_tensor(torch.from_numpy(c.w)).data_ptr() if c.w is not None else None
+            cc.split = dev_tensor(torch.from_numpy(c.split)).data_ptr() if c.split is not None and len(c.split) \
+                else None
         self.modes = [c.mode for c in desc.conns]
         self.n_links = desc.n_links
 
         block = net.block or min([p.group_size for p in pops] + [256])
         block = 64 if block <= 64 else 128 if block <= 128 else 256
-        self.opt = _lib.Options(block=block, device=dev.index if dev.index is not None else 0)
+        self.opt = _lib.Options(block=block, device=dev.index if dev.index is not None else 0, grid=int(net.grid or 0),
+                                persistent=int(bool(net.persistent)))
         nbytes = ctypes.c_size_t()
         _lib.check(lib.n2b_workspace_bytes(self.cpop, len(pops), self.cconn, len(desc.conns), ctypes.byref(self.opt),
                                            ctypes.byref(nbytes)), "n2b_workspace_bytes")

@@ -152,11 +152,24 @@ def pack_links(index: np.ndarray, steps: np.ndarray) -> np.ndarray:
 
 
 def push_form(topo: Topology, steps: np.ndarray, n_tgt: int):
-    """(ptr int32 [n_src + 1], link uint32 [n_links]) in canonical order."""
+    """(ptr int32 [n_src + 1], link uint32 [n_links], perm int64 [n_links], split int32 [n_src]): rows per source,
+    each row's delay-1 links first (stable: canonical order otherwise); perm[k] is the canonical link at position
+    k; split[s] is row s's first link of delay >= 2 (the rest of the row is delivered one launch later)."""
     tgt = topo.target_indices.numpy()
     if len(tgt) and (tgt.min() < 0 or tgt.max() >= n_tgt):
         raise ValueError("a link targets a neuron outside the target population")
-    return topo.source_offsets.numpy().astype(np.int32), pack_links(tgt, steps)
+    off = topo.source_offsets.numpy()
+    n_src = len(off) - 1
+    far = steps >= 2
+    near_per_row = np.bincount(np.repeat(np.arange(n_src), np.diff(off)), weights=~far, minlength=n_src) \
+        if len(tgt) else np.zeros(n_src)
+    if far.all() or not len(tgt):
+        perm = np.arange(len(tgt), dtype=np.int64)
+    else:
+        row = np.repeat(np.arange(n_src, dtype=np.int64), np.diff(off))
+        perm = np.argsort(row * 2 + far, kind="stable")
+    split = (off[:-1] + near_per_row.astype(np.int64)).astype(np.int32)
+    return off.astype(np.int32), pack_links(tgt[perm], steps[perm]), perm, split
 
 
 def pull_form(topo: Topology, steps: np.ndarray, n_tgt: int):

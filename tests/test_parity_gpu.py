@@ -23,9 +23,10 @@ from test_oracle import GOLDEN, brunel_golden_desc
 pytestmark = pytest.mark.gpu
 
 
-def run_both(net, steps, chunk=None, modes=None):
+def run_both(net, steps, chunk=None, modes=None, persistent=True):
     """Run `net` on the GPU and the oracle from the same initial state; return (gpu rasters, oracle rasters,
     gpu states, oracle states, gpu counters, oracle events)."""
+    net.persistent = persistent
     desc = describe(net, modes)
     st = oracle.states_of(net, desc)
     net.record(steps)
@@ -58,18 +59,20 @@ def assert_identical(gpu_r, ora_r, gpu_s, ora_s):
                                   want.view(np.uint32) if want.dtype == np.float32 else want), (k, slot)
 
 
-def test_config0_dsl_matches_oracle(cuda):
+@pytest.mark.parametrize("persistent", [True, False], ids=["persistent", "per-step"])
+def test_config0_dsl_matches_oracle(cuda, persistent):
     net, pops = brunel.build(**brunel.CONFIG0, seed=1)
-    gr, orr, gs, os_, cnt, ev = run_both(net, 1000)
+    gr, orr, gs, os_, cnt, ev = run_both(net, 1000, persistent=persistent)
     assert sum(r.sum() for r in gr) > 1000
     assert_identical(gr, orr, gs, os_)
     assert cnt["events"] == ev
     assert cnt["spikes"] == sum(int(r.sum()) for r in gr)
 
 
-def test_config1_first_1000_steps_match_oracle(cuda):
+@pytest.mark.parametrize("persistent", [True, False], ids=["persistent", "per-step"])
+def test_config1_first_1000_steps_match_oracle(cuda, persistent):
     net, pops = brunel.build(**brunel.CONFIG1, seed=2)
-    gr, orr, gs, os_, cnt, ev = run_both(net, 1000, chunk=300)
+    gr, orr, gs, os_, cnt, ev = run_both(net, 1000, chunk=300, persistent=persistent)
     assert sum(r.sum() for r in gr) > 10000
     assert_identical(gr, orr, gs, os_)
     assert cnt["events"] == ev
@@ -143,9 +146,11 @@ def test_pull_matches_push_and_oracle(cuda, mode):
     assert_identical(gr, orr, gs, os_)
 
 
-def test_graph_windows_match_single_steps(cuda):
+@pytest.mark.parametrize("persistent", [True, False], ids=["persistent", "per-step"])
+def test_graph_windows_match_single_steps(cuda, persistent):
     a, _ = brunel.build(**brunel.CONFIG0, seed=4)
     b, _ = brunel.build(**brunel.CONFIG0, seed=4)
+    a.persistent = b.persistent = persistent
     a.window, b.window = 50, 10_000
     a.record(730)
     b.record(730)
@@ -188,9 +193,10 @@ def pd14_small(seed=5, per_link=True):
     return net, pops
 
 
-def test_pd14_small_matches_oracle(cuda):
+@pytest.mark.parametrize("persistent", [True, False], ids=["persistent", "per-step"])
+def test_pd14_small_matches_oracle(cuda, persistent):
     net, pops = pd14_small()
-    gr, orr, gs, os_, cnt, ev = run_both(net, 800, chunk=250)
+    gr, orr, gs, os_, cnt, ev = run_both(net, 800, chunk=250, persistent=persistent)
     assert sum(r.sum() for r in gr) > 100
     assert_identical(gr, orr, gs, os_)
     assert cnt["events"] == ev
@@ -233,6 +239,13 @@ def test_silent_and_saturated_networks(cuda):
     assert cnt["events"] == ev
 
 
+def test_barrier_status_is_clean_after_persistent_windows(cuda):
+    net, pops = brunel.build(**brunel.CONFIG0, seed=12)
+    net.persistent = True
+    net.run_steps(2345)
+    assert net.runtime.status() == [0] * _lib.ERR_WORDS
+
+
 def test_counters_count_events(cuda):
     net, pops = brunel.build(**brunel.CONFIG0, seed=6)
     net.run_steps(300)
@@ -241,3 +254,25 @@ def test_counters_count_events(cuda):
     assert c["events"] > 0
     net.runtime.reset_counters()
     assert net.counters()["events"] == 0
+
+
+@pytest.mark.parametrize("persistent", [True, False], ids=["persistent", "per-step"])
+@pytest.mark.parametrize("grid", [1, 7, 1000])
+def test_grid_size_does_not_change_results(cuda, grid, persistent):
+    """Far links are shared by however many blocks the launch has (a persistent block looping over several
+    tiles when there are fewer blocks than tiles): the same sums for any grid."""
+    kw = dict(brunel.CONFIG0, delay="uniform", max_delay_steps=9, seed=8)
+    a, _ = brunel.build(**kw)
+    b, _ = brunel.build(**kw)
+    a.grid = grid
+    a.persistent = persistent
+    b.persistent = False
+    a.record(500)
+    b.record(500)
+    a.run_steps(500)
+    b.run_steps(500)
+    assert a.runtime.raster(a.populations[0]).sum() > 0
+    for pa, pb in zip(a.populations, b.populations):
+        assert np.array_equal(a.runtime.raster(pa), b.runtime.raster(pb))
+        assert torch.equal(pa.V, pb.V)
+    assert a.counters()["events"] == b.counters()["events"]
