@@ -304,7 +304,7 @@ def main() -> int:
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": ("n2b::persistent_kernel<128>" if MODE == "persistent" else "n2b::step_kernel<128>"),
+                         "kernel": ("n2b::persistent_kernel<256>" if MODE == "persistent" else "n2b::step_kernel<256>"),
                          "bytes_per_launch": alg_bytes, "us_per_launch": ms_per_launch * 1e3,
                          "note": "per simulation step: timed device time / steps (launch gaps and grid barriers "
                                  "included)"},

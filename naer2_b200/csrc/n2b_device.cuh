@@ -90,7 +90,9 @@ struct StepArgs {
     unsigned long long *counters;
     int4 *items;           // 3 work lists of item_cap entries: (push connection, first link, end link, 0)
     int32_t *item_count;   // their lengths; step n appends to list n mod 3, reads n - 1's
-    unsigned *barrier;     // persistent kernel: group counters (one per 128-byte line), then top, generation, abort
+    unsigned *barrier;     // persistent kernel: the arrival counter, the abort word
+    unsigned long long *trace;  // N2B_TRACE builds: per step and block, %globaltimer at each phase (else unused)
+    int32_t trace_steps;
     int32_t item_cap;
     int32_t n_tiles;
     int32_t offset;        // this launch's step = *step + offset (per-step launches)
@@ -100,6 +102,24 @@ struct StepArgs {
     ConnDev push_i[INLINE_PUSH];
     ConnDev pull_i[INLINE_PULL];
 };
+
+// Phase stamps of N2B_TRACE builds (the reference's TRACE levels, naer2/trace.py): step k's block b writes
+// %globaltimer at phase p into trace[(k * gridDim.x + b) * TRACE_PHASES + p].
+constexpr int TRACE_PHASES = 6;
+#ifdef N2B_TRACE
+#define N2B_STAMP(a, k, p)                                                                                   \
+    do {                                                                                                     \
+        if (threadIdx.x == 0 && (a).trace && (k) < (a).trace_steps) {                                        \
+            unsigned long long _t;                                                                           \
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(_t));                                           \
+            (a).trace[((size_t)(k) * gridDim.x + blockIdx.x) * TRACE_PHASES + (p)] = _t;                      \
+        }                                                                                                    \
+    } while (0)
+#else
+#define N2B_STAMP(a, k, p) \
+    do {                   \
+    } while (0)
+#endif
 
 template <bool INL>
 __device__ __forceinline__ const PopDev &pop_at(const StepArgs &a, int k) {
@@ -124,11 +144,10 @@ __device__ __forceinline__ int4 tile_at(const StepArgs &a, int t) {
     return make_int4(p, first, min(NPB, a.pops_i[p].n - first), 0);
 }
 
-constexpr int BAR_GROUP = 16;     // blocks per first-level barrier counter
-constexpr int BAR_STRIDE = 32;    // words between counters (a 128-byte line each)
-constexpr int BAR_MAX_GROUPS = 256;
-constexpr int BAR_TOP = BAR_MAX_GROUPS * BAR_STRIDE, BAR_GEN = BAR_TOP + BAR_STRIDE, BAR_ABORT = BAR_GEN + BAR_STRIDE;
-constexpr int BAR_WORDS = BAR_ABORT + BAR_STRIDE;
+constexpr int BAR_COUNT = 0;      // persistent launches: arrivals of this launch's barriers
+constexpr int BAR_ABORT = 32;     // set when a barrier wait gave up (a line of its own)
+constexpr int BAR_WORDS = 64;
+constexpr int BAR_MAX_BLOCKS = 1 << 16;
 constexpr unsigned long long BAR_LIMIT_NS = 2000000000ull;  // a barrier wait gives up after 2 s
 
 // ------------------------------------------------------------------ Philox
@@ -320,20 +339,90 @@ __device__ __forceinline__ Row row_of(const ConnDev &C, int j) {
     return r;
 }
 
-// The block's spikes of one outgoing push connection: the spiking threads append their far items (their
-// atomic's latency hidden under the near walk), the block walks the near links as one flat range.
-template <int NPB>
-__device__ __forceinline__ void deliver_spikes(const StepArgs &a, const ConnDev &C, int c, const Row &row, bool fire,
-                                               int pos, int cnt, long long n, int *s_row, int *s_off, int *s_wsum) {
+// The block's spikes, every outgoing push connection at once. Each spiking thread counts its links (the
+// events, counted when they are emitted) and appends its far items (the atomics' latency hidden under the
+// near walk); the block walks the near links of all (spike, connection) entries as one flat range.
+template <int NPB, bool INL>
+__device__ __forceinline__ void deliver_spikes(const StepArgs &a, const PopDev &P, const Row *rows, bool fire,
+                                               int pos, int cnt, long long n, int *s_row, int *s_off,
+                                               int *s_wsum) {
     const int tid = threadIdx.x, lane = tid & 31;
-    // events are counted when they are emitted (here), near and far alike
+    const int n_out = min(P.n_out, PREFETCH_OUT);
+    int links = 0;
+    int n_items[PREFETCH_OUT] = {}, at[PREFETCH_OUT] = {};
+#pragma unroll
+    for (int c = 0; c < PREFETCH_OUT; ++c) {
+        if (c < n_out && fire) {
+            const Row &r = rows[c];
+            links += r.r1 - r.r0;
+            s_row[pos * PREFETCH_OUT + c] = r.r0;
+            s_off[pos * PREFETCH_OUT + c] = r.sp - r.r0;  // near links, scanned below
+            n_items[c] = (r.r1 - r.sp + NPB - 1) / NPB;
+            if (n_items[c] > 0) at[c] = atomicAdd(a.item_count + (int)(n % 3), n_items[c]);
+        }
+    }
+    const int warp_links = __reduce_add_sync(FULL, links);
+    if (lane == 0 && warp_links) atomicAdd(a.counters + 0, (unsigned long long)warp_links);
+    __syncthreads();
+    // entries (spike, connection) = pos * PREFETCH_OUT + c, those of absent connections empty; each thread
+    // scans PREFETCH_OUT consecutive entries (NPB * PREFETCH_OUT >= n_ent)
+    const int n_ent = cnt * PREFETCH_OUT;
+    int v[PREFETCH_OUT];
+    int mine = 0;
+#pragma unroll
+    for (int c = 0; c < PREFETCH_OUT; ++c) {
+        const int e = tid * PREFETCH_OUT + c;
+        v[c] = (e < n_ent && c < n_out) ? s_off[e] : 0;
+        mine += v[c];
+    }
+    int total = 0;
+    int off = block_excl_scan<NPB>(mine, s_wsum, &total);
+#pragma unroll
+    for (int c = 0; c < PREFETCH_OUT; ++c) {
+        const int e = tid * PREFETCH_OUT + c;
+        if (e < n_ent) s_off[e] = off;
+        off += v[c];
+    }
+    if (tid == 0) s_off[n_ent] = total;
+    __syncthreads();
+    for (int idx = tid; idx < total; idx += NPB) {
+        int lo = 0, hi = n_ent;  // s_off[lo] <= idx < s_off[hi]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_off[mid] <= idx) lo = mid; else hi = mid;
+        }
+        const ConnDev &C = push_at<INL>(a, P.out_first + lo % PREFETCH_OUT);
+        const int l = s_row[lo] + (idx - s_off[lo]);
+        deliver_rec(a, C, __ldg(C.link + l), l, n, 1);
+    }
+    int4 *list = a.items + (size_t)(n % 3) * (size_t)a.item_cap;
+#pragma unroll
+    for (int c = 0; c < PREFETCH_OUT; ++c) {
+        for (int k = 0; k < n_items[c]; ++k) {
+            if (at[c] + k < a.item_cap) {
+                const int l0 = rows[c].sp + k * NPB;
+                list[at[c] + k] = make_int4(P.out_first + c, l0, min(l0 + NPB, rows[c].r1), 0);
+            } else {
+                atomicAdd(a.err + 3, 1);
+            }
+        }
+    }
+    __syncthreads();  // s_row / s_off free again
+}
+
+// Connections past the first PREFETCH_OUT: one at a time, their rows loaded on demand.
+template <int NPB, bool INL>
+__device__ __forceinline__ void deliver_spikes_one(const StepArgs &a, const ConnDev &C, int c, const Row &row,
+                                                   bool fire, int pos, int cnt, long long n, int *s_row, int *s_off,
+                                                   int *s_wsum) {
+    const int tid = threadIdx.x, lane = tid & 31;
     const int row_len = fire ? row.r1 - row.r0 : 0;
     const int warp_links = __reduce_add_sync(FULL, row_len);
     if (lane == 0 && warp_links) atomicAdd(a.counters + 0, (unsigned long long)warp_links);
     int n_items = 0, at = 0;
     if (fire) {
         s_row[pos] = row.r0;
-        s_off[pos] = row.sp - row.r0;  // near links, scanned below
+        s_off[pos] = row.sp - row.r0;
         n_items = (row.r1 - row.sp + NPB - 1) / NPB;
         if (n_items > 0) at = atomicAdd(a.item_count + (int)(n % 3), n_items);
     }
@@ -345,7 +434,7 @@ __device__ __forceinline__ void deliver_spikes(const StepArgs &a, const ConnDev 
     if (tid == 0) s_off[cnt] = total;
     __syncthreads();
     for (int idx = tid; idx < total; idx += NPB) {
-        int lo = 0, hi = cnt;  // s_off[lo] <= idx < s_off[hi]
+        int lo = 0, hi = cnt;
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
             if (s_off[mid] <= idx) lo = mid; else hi = mid;
@@ -364,16 +453,51 @@ __device__ __forceinline__ void deliver_spikes(const StepArgs &a, const ConnDev 
             }
         }
     }
-    __syncthreads();  // s_row / s_off free for the next connection
+    __syncthreads();
 }
 
 // ------------------------------------------------------------------ one tile of one step
 
-template <int NPB, bool INL>
-__device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n, const int4 tile) {
+// A neuron's state as its thread holds it through a step: membrane, current, refractory count, and its
+// outgoing row bounds. A persistent launch keeps its block's first tile here for the whole window.
+struct Neuron {
+    float v, cur;
+    int ref;
+    Row rows[PREFETCH_OUT];
+};
+
+template <bool INL>
+__device__ __forceinline__ void load_neuron(const StepArgs &a, const PopDev &P, int j, bool live, Neuron &nr) {
+    nr.v = 0.f;
+    nr.cur = 0.f;
+    nr.ref = 0;
+#pragma unroll
+    for (int c = 0; c < PREFETCH_OUT; ++c) nr.rows[c] = Row{0, 0, 0};
+    if (!live) return;
+    if (P.model != 3) {
+        nr.v = P.v[j];
+        nr.ref = P.ref[j];
+        if (P.model == 2) nr.cur = P.i[j];
+    }
+#pragma unroll
+    for (int c = 0; c < PREFETCH_OUT; ++c)
+        if (c < P.n_out) nr.rows[c] = row_of(push_at<INL>(a, P.out_first + c), j);
+}
+
+__device__ __forceinline__ void store_neuron(const PopDev &P, int j, bool live, const Neuron &nr) {
+    if (!live || P.model == 3) return;
+    P.v[j] = nr.v;
+    P.ref[j] = nr.ref;
+    if (P.model == 2) P.i[j] = nr.cur;
+}
+
+// One tile of one step. CACHED: the tile's Neuron is held in registers by the caller across steps (loaded
+// before the window, stored after it); otherwise it is loaded and stored here.
+template <int NPB, bool INL, bool CACHED>
+__device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n, const int4 tile, int k, Neuron &nr) {
     __shared__ int s_cnt;
-    __shared__ int s_row[NPB];
-    __shared__ int s_off[NPB + 1];
+    __shared__ int s_row[NPB * PREFETCH_OUT];
+    __shared__ int s_off[NPB * PREFETCH_OUT + 1];
     __shared__ int s_wsum[NPB / 32];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -383,26 +507,19 @@ __device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n,
     __syncthreads();  // a block's previous tile: every thread past its reads of the shared arrays
     if (tid == 0) s_cnt = 0;
 
-    // state and outgoing row bounds together: none of these loads waits for another
+    // the arrival slot (and, uncached, the state and row bounds: none of these loads waits for another)
     const int model = P.model;
-    float v = 0.f, cur = 0.f;
-    int ref = 0;
     long long acc = 0;
     long long *slot = nullptr;
-    Row rows[PREFETCH_OUT] = {};
-    const int n_out = P.n_out;
-    if (live) {
-        if (model != 3) {
-            slot = P.acc + (size_t)(n & P.acc_mask) * (size_t)P.n + j;
-            acc = __ldcg(slot);  // L2: other blocks' adds of this kernel are there, not in this SM's L1
-            v = P.v[j];
-            ref = P.ref[j];
-            if (model == 2) cur = P.i[j];
-        }
-#pragma unroll
-        for (int c = 0; c < PREFETCH_OUT; ++c)
-            if (c < n_out) rows[c] = row_of(push_at<INL>(a, P.out_first + c), j);
+    if (live && model != 3) {
+        slot = P.acc + (size_t)(n & P.acc_mask) * (size_t)P.n + j;
+        acc = __ldcg(slot);  // L2: other blocks' adds of this kernel are there, not in this SM's L1
     }
+    if (!CACHED) load_neuron<INL>(a, P, j, live, nr);
+    float &v = nr.v, &cur = nr.cur;
+    int &ref = nr.ref;
+    const Row *rows = nr.rows;
+    const int n_out = P.n_out;
 
     // 1-2. intake and update
     bool fire = false;
@@ -414,15 +531,9 @@ __device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n,
             *slot = 0;
             if (P.ext_len > 0) acc += (long long)poisson_count(P, draw(P, j, n, 0u)) * P.ext_wfx;
             const float in = __fmul_rn(__ll2float_rn(acc), P.inv_scale);
-            if (model == 1) {
-                fire = lif_delta(P, in, v, ref);
-            } else {
-                fire = pd14(P, in, v, cur, ref);
-                P.i[j] = cur;
-            }
-            P.v[j] = v;
-            P.ref[j] = ref;
+            fire = (model == 1) ? lif_delta(P, in, v, ref) : pd14(P, in, v, cur, ref);
         }
+        if (!CACHED) store_neuron(P, j, live, nr);
     }
 
     // 3. spike ring: a ballot word per warp, the spikes compacted into shared memory
@@ -441,6 +552,7 @@ __device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n,
     base = __shfl_sync(FULL, base, 0);
     const int pos = base + __popc(b & ((1u << lane) - 1u));
     __syncthreads();
+    N2B_STAMP(a, k, 1);
     const int cnt = s_cnt;
     if (cnt == 0) return;
     if (tid == 0) {
@@ -449,15 +561,11 @@ __device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n,
     }
 
     // 4. the spikes' outgoing rows
-#pragma unroll
-    for (int c = 0; c < PREFETCH_OUT; ++c)
-        if (c < n_out)
-            deliver_spikes<NPB>(a, push_at<INL>(a, P.out_first + c), P.out_first + c, rows[c], fire, pos, cnt, n,
-                                s_row, s_off, s_wsum);
+    if (n_out > 0) deliver_spikes<NPB, INL>(a, P, rows, fire, pos, cnt, n, s_row, s_off, s_wsum);
     for (int c = PREFETCH_OUT; c < n_out; ++c) {
         const ConnDev &C = push_at<INL>(a, P.out_first + c);
         const Row r = fire ? row_of(C, j) : Row{0, 0, 0};
-        deliver_spikes<NPB>(a, C, P.out_first + c, r, fire, pos, cnt, n, s_row, s_off, s_wsum);
+        deliver_spikes_one<NPB, INL>(a, C, P.out_first + c, r, fire, pos, cnt, n, s_row, s_off, s_wsum);
     }
 }
 
@@ -466,13 +574,27 @@ template <int NPB, bool INL>
 __device__ __forceinline__ void far_phase(const StepArgs &a, const long long n) {
     const long long m = n - 1;
     const int lst = (int)(((m % 3) + 3) % 3);
-    const int count = min(__ldcg(a.item_count + lst), a.item_cap);
     const int4 *list = a.items + (size_t)lst * (size_t)a.item_cap;
-    const int G = gridDim.x;
-    for (int i = G - 1 - (int)blockIdx.x; i < count; i += 2 * G) {
-        const int4 it0 = __ldcg(list + i);
+    // the items go to the blocks without a tile when there are enough of them (a quarter of the grid), else to
+    // every block, the tile-free ones first
+    const int free_blocks = (int)gridDim.x - a.n_tiles;
+    const bool split = free_blocks >= (int)gridDim.x / 4 && free_blocks > 0;
+    if (split && (int)blockIdx.x < a.n_tiles) return;
+    const int G = split ? free_blocks : (int)gridDim.x;
+    const int me = split ? (int)blockIdx.x - a.n_tiles : (int)blockIdx.x;
+    // the first two items loaded with the count, not after it (an item past the count is read, then ignored)
+    int i = G - 1 - me;
+    int4 pre0 = i < a.item_cap ? __ldcg(list + i) : make_int4(0, 0, 0, 0);
+    int4 pre1 = i + G < a.item_cap ? __ldcg(list + i + G) : make_int4(0, 0, 0, 0);
+    const int count = min(__ldcg(a.item_count + lst), a.item_cap);
+    for (; i < count; i += 2 * G) {
+        const int4 it0 = pre0;
         const bool two = i + G < count;
-        const int4 it1 = two ? __ldcg(list + i + G) : make_int4(0, 0, 0, 0);
+        const int4 it1 = two ? pre1 : make_int4(0, 0, 0, 0);
+        if (i + 2 * G < count) {
+            pre0 = __ldcg(list + i + 2 * G);
+            pre1 = i + 3 * G < count ? __ldcg(list + i + 3 * G) : make_int4(0, 0, 0, 0);
+        }
         const int l0 = it0.y + (int)threadIdx.x, l1 = it1.y + (int)threadIdx.x;
         const ConnDev &C0 = push_at<INL>(a, it0.x);
         const ConnDev &C1 = push_at<INL>(a, it1.x);
@@ -485,16 +607,25 @@ __device__ __forceinline__ void far_phase(const StepArgs &a, const long long n) 
 }
 
 template <int NPB, bool INL>
-__device__ __forceinline__ void step_body(const StepArgs &a, const long long n) {
+__device__ __forceinline__ void step_body(const StepArgs &a, const long long n, int k, Neuron *cached) {
+    N2B_STAMP(a, k, 0);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.item_count + (int)((n + 1) % 3), 0);  // step n + 1's list
-    for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) tile_phase<NPB, INL>(a, n, tile_at<INL, NPB>(a, t));
+    int t = blockIdx.x;
+    if (cached != nullptr && t < a.n_tiles) {
+        tile_phase<NPB, INL, true>(a, n, tile_at<INL, NPB>(a, t), k, *cached);
+        t += gridDim.x;
+    }
+    Neuron nr;
+    for (; t < a.n_tiles; t += gridDim.x) tile_phase<NPB, INL, false>(a, n, tile_at<INL, NPB>(a, t), k, nr);
+    N2B_STAMP(a, k, 2);
     far_phase<NPB, INL>(a, n);
+    N2B_STAMP(a, k, 3);
 }
 
 // One step per launch: the launch boundary is the step's barrier.
 template <int NPB, bool INL>
 __global__ void __launch_bounds__(NPB) step_kernel(const __grid_constant__ StepArgs a) {
-    step_body<NPB, INL>(a, *a.step + a.offset);
+    step_body<NPB, INL>(a, *a.step + a.offset, 0, nullptr);
 }
 
 __device__ __forceinline__ unsigned long long globaltimer() {
@@ -503,44 +634,42 @@ __device__ __forceinline__ unsigned long long globaltimer() {
     return t;
 }
 
-// Grid-wide barrier of a cooperative launch: the blocks arrive on counters of BAR_GROUP blocks, the last
-// of each group on the top counter, the last of all bumps the generation the others wait on. Every wait is
-// bounded (BAR_LIMIT_NS): a timeout sets error word 4 and the abort word, and the kernel winds down instead
-// of hanging. Returns false once aborted.
-__device__ __forceinline__ bool grid_sync(const StepArgs &a) {
+__device__ __forceinline__ void red_release_add(unsigned *p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide barrier k (0, 1, ...) of a cooperative launch: every block adds 1 to one counter with release
+// semantics (its writes before its arrival) and waits, with acquire loads, until the counter holds
+// (k + 1) * gridDim.x -- the counter starts each launch at 0 (advance_kernel clears it after every launch).
+// Every wait is bounded (BAR_LIMIT_NS): a timeout sets error word 4 and the abort word, and the kernel winds
+// down instead of hanging. Returns false once aborted.
+__device__ __forceinline__ bool grid_sync(const StepArgs &a, unsigned k) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned *bar = a.barrier;
-        volatile unsigned *gen = bar + BAR_GEN;
-        volatile unsigned *abort = bar + BAR_ABORT;
-        const unsigned g = *gen;
-        __threadfence();  // this block's writes before its arrival
-        const unsigned grp = blockIdx.x / BAR_GROUP;
-        const unsigned n_groups = (gridDim.x + BAR_GROUP - 1) / BAR_GROUP;
-        const unsigned members = min((unsigned)BAR_GROUP, gridDim.x - grp * BAR_GROUP);
+        const unsigned target = (k + 1) * gridDim.x;
+        red_release_add(bar + BAR_COUNT, 1u);
         int ok = 1;
-        if (atomicAdd(bar + grp * BAR_STRIDE, 1u) == members - 1) {
-            atomicExch(bar + grp * BAR_STRIDE, 0u);  // every member has arrived: ready for the next barrier
-            __threadfence();
-            if (atomicAdd(bar + BAR_TOP, 1u) == n_groups - 1) {
-                atomicExch(bar + BAR_TOP, 0u);
-                __threadfence();
-                atomicAdd(bar + BAR_GEN, 1u);
-            }
-        }
-        const unsigned long long t0 = globaltimer();
-        while (*gen == g) {
-            if (*abort) { ok = 0; break; }
-            if (globaltimer() - t0 > BAR_LIMIT_NS) {
+        unsigned long long t0 = 0;
+        for (int spin = 0;; ++spin) {
+            if ((int)(ld_acquire(bar + BAR_COUNT) - target) >= 0) break;
+            if (*(volatile unsigned *)(bar + BAR_ABORT)) { ok = 0; break; }
+            if (spin == 0) t0 = globaltimer();
+            else if (globaltimer() - t0 > BAR_LIMIT_NS) {
                 atomicExch(bar + BAR_ABORT, 1u);
                 atomicAdd(a.err + 4, 1);
                 ok = 0;
                 break;
             }
-            __nanosleep(32);
+            __nanosleep(20);
         }
-        __threadfence();  // the other blocks' writes before this block's next reads
         s_ok = ok;
     }
     __syncthreads();
@@ -552,13 +681,27 @@ template <int NPB, bool INL>
 __global__ void __launch_bounds__(NPB) persistent_kernel(const __grid_constant__ StepArgs a, const int n_steps) {
     if (*(volatile unsigned *)(a.barrier + BAR_ABORT)) return;  // an earlier window gave up: nothing runs
     const long long n0 = *a.step;
+    // the block's first tile stays in registers for the whole window
+    const bool has_tile = (int)blockIdx.x < a.n_tiles;
+    const int4 tile = has_tile ? tile_at<INL, NPB>(a, blockIdx.x) : make_int4(0, 0, 0, 0);
+    const PopDev &P = pop_at<INL>(a, tile.x);
+    const int j = tile.y + (int)threadIdx.x;
+    const bool live = has_tile && (int)threadIdx.x < tile.z;
+    Neuron mine;
+    load_neuron<INL>(a, P, j, live, mine);
     for (int k = 0; k < n_steps; ++k) {
-        step_body<NPB, INL>(a, n0 + k);
-        if (!grid_sync(a)) return;
+        step_body<NPB, INL>(a, n0 + k, k, &mine);
+        if (!grid_sync(a, (unsigned)k)) break;
+        N2B_STAMP(a, k, 4);
     }
+    store_neuron(P, j, live, mine);
 }
 
-__global__ void advance_kernel(long long *step, long long by) { *step += by; }
+// After every launch: the step counter advanced, the persistent barrier's arrivals cleared.
+__global__ void advance_kernel(long long *step, long long by, unsigned *barrier) {
+    *step += by;
+    barrier[BAR_COUNT] = 0;
+}
 __global__ void set_kernel(long long *p, long long value) { *p = value; }
 __global__ void zero_kernel(int32_t *err, int n_err, unsigned long long *counters, int n_counters) {
     for (int k = threadIdx.x; k < n_err; k += blockDim.x) err[k] = 0;

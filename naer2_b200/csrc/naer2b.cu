@@ -175,7 +175,8 @@ cudaError_t launch_steps(n2b_net *net, int64_t n_steps, cudaStream_t s) {
         cudaError_t e = net->inl ? launch_block<true>(net, n_steps, s) : launch_block<false>(net, n_steps, s);
         if (e != cudaSuccess) return e;
     }
-    n2b::advance_kernel<<<1, 1, 0, s>>>(reinterpret_cast<long long *>(net->ws + net->L.step), n_steps);
+    n2b::advance_kernel<<<1, 1, 0, s>>>(reinterpret_cast<long long *>(net->ws + net->L.step), n_steps,
+                                        reinterpret_cast<unsigned *>(net->ws + net->L.barrier));
     return cudaGetLastError();
 }
 
@@ -347,7 +348,7 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
         int rc2 = coresident_blocks(block, inl, device, &most);
         if (rc2) return rc2;
         if (most < 1) return fail(N2B_ECUDA, "the persistent kernel cannot be resident");
-        grid = std::min(std::min(want, most), n2b::BAR_MAX_GROUPS * n2b::BAR_GROUP);
+        grid = std::min(std::min(want, most), n2b::BAR_MAX_BLOCKS);
         grid = std::max(grid, 1);
     }
     n2b_net *net = new n2b_net();
@@ -490,6 +491,18 @@ int n2b_reset_counters(n2b_net *net, void *stream) {
     N2B_CUDA(cudaGetLastError());
     return N2B_OK;
 }
+
+#ifdef N2B_TRACE
+// Trace builds only (not part of the C ABI): phase stamps of the next persistent window's first `steps` steps
+// into trace[steps][grid][6] (device memory).
+int n2b_trace(n2b_net *net, unsigned long long *trace, int32_t steps, int32_t *grid) {
+    if (!net) return fail(N2B_EINVAL, "net is NULL");
+    net->args.trace = trace;
+    net->args.trace_steps = steps;
+    if (grid) *grid = net->grid;
+    return N2B_OK;
+}
+#endif
 
 int n2b_destroy(n2b_net *net) {
     if (!net) return N2B_OK;

@@ -26,7 +26,7 @@ CONFIG1 = dict(NE=10000, NI=2500, CE=1000, CI=250, delay="uniform", max_delay_st
 
 def build(NE: int = 800, NI: int = 200, CE: int = 80, CI: int = 20, J: float = 0.1, g: float = 5.0,
           eta: float = 2.0, delay="uniform", max_delay_steps: int = 20, tau: float = 20.0, theta: float = 20.0,
-          V_r: float = 10.0, t_ref: float = 2.0, dt: float = 0.1, seed: int = 0, group_size: int = 128):
+          V_r: float = 10.0, t_ref: float = 2.0, dt: float = 0.1, seed: int = 0, group_size: int = 256):
     """(network, {"E": E, "I": I}) of Brunel's model A at step dt."""
     nu_thr = theta / (J * CE * tau)
     ext_rate = CE * eta * nu_thr  # external events per ms into each neuron

@@ -22,7 +22,7 @@ _ORDER = itertools.count()  # creation order: the network lists its populations 
 
 
 class Population:
-    def __init__(self, instance, shape, group_size: int = 128, timestep: float | None = None,
+    def __init__(self, instance, shape, group_size: int = 256, timestep: float | None = None,
                  delay_resolution: float | None = None):
         object.__setattr__(self, "_state", {})
         object.__setattr__(self, "_net", None)
