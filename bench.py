@@ -118,7 +118,7 @@ def cpu_sample(desc, states, target_s: float = 12.0, threads: int = 0) -> dict:
     t0 = time.perf_counter()
     _, ev = oracle.run(desc, states, 0, probe, record=False)
     t_probe = time.perf_counter() - t0
-    steps = max(50, min(10_000, int(probe * target_s / max(t_probe, 1e-3))))
+    steps = max(50, min(400_000, int(probe * target_s / max(t_probe, 1e-3))))
     t0 = time.perf_counter()
     _, ev2 = oracle.run(desc, states, probe, steps, record=False)
     el = time.perf_counter() - t0
@@ -291,9 +291,10 @@ def main() -> int:
         achieved = alg_bytes / (ms_per_launch / 1e3) / 1e9
         peak, peak_kind = measured_peaks()
         traffic = None
-        prof = ROOT / "profiles" / "step_kernel_brunel_config1.json"
-        if prof.exists():
-            traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
+        prof = ROOT / "profiles" / "persistent_kernel_brunel_config1.json"
+        if prof.exists() and MODE == "persistent":  # one ncu capture, scaled to this run's events per step
+            pr = json.loads(prof.read_text())
+            traffic = pr["dram_bytes_per_step"] * ev_per_launch / pr["events_per_step"]
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
