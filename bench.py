@@ -109,6 +109,21 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def reduce_over_ranks(times, counts, world: int, device):
+    """Times: the max over ranks; counts: the sum (the whole job's work). One collective each, every rank."""
+    import torch
+
+    if world <= 1:
+        return [*map(float, times), *map(float, counts)]
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x) for x in times], dtype=torch.float64, device=device)
+    c = torch.tensor([float(x) for x in counts], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return [*t.tolist(), *c.tolist()]
+
+
 def cpu_sample(desc, states, target_s: float = 12.0, threads: int = 0) -> dict:
     """The oracle on the host cores: a bounded sample of the same network (first steps from the same state)."""
     import oracle
@@ -270,14 +285,7 @@ def main() -> int:
     e2e_events = rt.counters()["events"] - ev1
 
     # ---- max over ranks
-    stats = torch.tensor([dev_ms, e2e_s, float(events), float(e2e_events)], dtype=torch.float64, device=dev)
-    if world > 1:
-        t_max = stats[:2].clone()
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-        ev_sum = stats[2:].clone()
-        dist.all_reduce(ev_sum, op=dist.ReduceOp.SUM)
-        stats = torch.cat([t_max, ev_sum])
-    dev_ms, e2e_s, events_all, e2e_events_all = stats.tolist()
+    dev_ms, e2e_s, events_all, e2e_events_all = reduce_over_ranks([dev_ms, e2e_s], [events, e2e_events], world, dev)
 
     cpu = None
     if desc is not None:
