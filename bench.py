@@ -178,6 +178,83 @@ def run_reference(args) -> None:
     print(json.dumps(line))
 
 
+def run_pd14(args, dev) -> dict:
+    """Config 2: the full PD14 microcircuit (77,169 neurons, ~3e8 synapses) built on the GPU; events/s over the
+    timed steps, population rates and CV-ISI over them."""
+    import numpy as np
+    import torch
+
+    from naer2_b200.networks import pd14
+
+    t0 = time.perf_counter()
+    net, pops = pd14.build(scale=args.scale, seed=1, device=dev)
+    net.persistent = args.mode == "persistent"
+    net.record(args.steps * SIM_STEPS_PER_STEP)
+    for p in pops:
+        p.state_tensor("potential", dev)
+    rt_build = time.perf_counter()
+    net.run_steps(1)  # builds the runtime
+    rt = net.runtime
+    build_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        net.run_steps(SIM_STEPS_PER_STEP)
+    net.record(args.steps * SIM_STEPS_PER_STEP)
+    torch.cuda.synchronize(dev)
+    ev0 = rt.counters()["events"]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with Clocks(dev.index or 0) as clocks:
+        for k in range(args.steps):
+            flush.zero_()
+            rt._enter()
+            starts[k].record(rt.stream)
+            net.run_steps(SIM_STEPS_PER_STEP)
+            ends[k].record(rt.stream)
+        torch.cuda.synchronize(dev)
+    dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    events = rt.counters()["events"] - ev0
+    net.check()
+    steps = args.steps * SIM_STEPS_PER_STEP
+    rates, cvs = [], []
+    for p in pops:
+        r = torch.from_numpy(rt.raster(p))  # [steps, n]
+        n = r.shape[1]
+        rates.append(float(r.sum()) / n / (steps * 1e-4))
+        step_idx, nid = torch.nonzero(r, as_tuple=True)
+        order = torch.argsort(nid * (steps + 1) + step_idx)
+        nid, t = nid[order], step_idx[order].double()
+        same = nid[1:] == nid[:-1]
+        isi = (t[1:] - t[:-1])[same]
+        owner = nid[1:][same]
+        cnt = torch.bincount(owner, minlength=n).double()
+        s1 = torch.bincount(owner, weights=isi, minlength=n)
+        s2 = torch.bincount(owner, weights=isi * isi, minlength=n)
+        ok = cnt >= 3
+        mean = s1[ok] / cnt[ok]
+        var = (s2[ok] - cnt[ok] * mean * mean) / (cnt[ok] - 1)
+        cvs.append(float((var.clamp(min=0).sqrt() / mean).mean()) if int(ok.sum()) else float("nan"))
+    ev_step = events / steps
+    n_neurons = sum(len(p.shape) for p in pops)
+    alg = ev_step * BYTES_PER_EVENT + n_neurons * (BYTES_PER_NEURON_STEP + 16)
+    us = dev_ms * 1e3 / steps
+    peak, kind = measured_peaks()
+    return {"metric": METRIC, "value": events / (dev_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded draws on the GPU, PD14 microcircuit)",
+            "config": {"workload": "pd14_config2", "scale": args.scale, "neurons": n_neurons,
+                       "synapses": rt.n_links, "dt_ms": 0.1, "sim_steps_per_step": SIM_STEPS_PER_STEP,
+                       "launch": MODE, "l2": "flushed before every timed step (256 MiB write)"},
+            "realtime_factor": (dev_ms / 1e3) / (steps * 1e-4),
+            "roofline": {"bound": "hbm", "achieved": alg / (us * 1e-6) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (us * 1e-6) / 1e9 / peak, "traffic": None, "peak_kind": kind,
+                         "bytes_per_launch": alg, "us_per_launch": us},
+            "rates_hz": dict(zip(pd14.NAMES, [round(x, 3) for x in rates])),
+            "cv_isi": dict(zip(pd14.NAMES, [round(x, 3) for x in cvs])),
+            "events_per_sim_step": ev_step, "build_s": build_s, "clocks": clocks.summary()}
+
+
 def main() -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -185,6 +262,9 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="naer2_b200", choices=["naer2_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--config", type=int, default=1, choices=[1, 2],
+                    help="1: Brunel model A at config 1's size (the default workload); 2: the PD14 microcircuit")
+    ap.add_argument("--scale", type=float, default=1.0, help="config 2: population sizes times this")
     ap.add_argument("--mode", choices=["persistent", "per-step"], default="persistent",
                     help="a window of steps per cooperative launch, or one launch per step")
     ap.add_argument("--sim-steps", type=int, default=1000,
@@ -212,6 +292,11 @@ def main() -> int:
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.config == 2:
+        if world > 1:
+            raise SystemExit("config 2 runs on one GPU")
+        print(json.dumps(run_pd14(args, dev)))
+        return 0
     if world > 1:
         import datetime
 

@@ -38,11 +38,11 @@
 namespace n2b {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr int INLINE_POPS = 16;   // populations whose tables fit the kernel parameters
-constexpr int INLINE_PUSH = 32;
+constexpr int INLINE_POPS = 32;   // populations whose tables fit the kernel parameters
+constexpr int INLINE_PUSH = 64;
 constexpr int INLINE_PULL = 16;
 constexpr int EXT_INLINE = 32;    // Poisson table entries kept inline
-constexpr int PREFETCH_OUT = 4;   // outgoing push connections whose row bounds are prefetched
+constexpr int MERGE_OUT = 8;      // outgoing push connections walked together (more: one at a time)
 
 // ------------------------------------------------------------------ tables
 
@@ -97,6 +97,7 @@ struct StepArgs {
     int32_t n_tiles;
     int32_t offset;        // this launch's step = *step + offset (per-step launches)
     int32_t n_pops;
+    int32_t n_push;
     int32_t tile_first[INLINE_POPS + 1];  // inline tables: population p owns tiles [tile_first[p], tile_first[p+1])
     PopDev pops_i[INLINE_POPS];
     ConnDev push_i[INLINE_PUSH];
@@ -105,7 +106,7 @@ struct StepArgs {
 
 // Phase stamps of N2B_TRACE builds (the reference's TRACE levels, naer2/trace.py): step k's block b writes
 // %globaltimer at phase p into trace[(k * gridDim.x + b) * TRACE_PHASES + p].
-constexpr int TRACE_PHASES = 6;
+constexpr int TRACE_PHASES = 12;
 #ifdef N2B_TRACE
 #define N2B_STAMP(a, k, p)                                                                                   \
     do {                                                                                                     \
@@ -211,6 +212,34 @@ __device__ __forceinline__ long long warp_sum64(long long v) {
     return v;
 }
 
+__device__ __forceinline__ long long warp_incl_scan64(long long v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long u = __shfl_up_sync(FULL, v, o);
+        if (lane >= o) v += u;
+    }
+    return v;
+}
+
+// Block-wide exclusive scan of one int64 per thread (NPB threads); the total in *total.
+template <int NPB>
+__device__ __forceinline__ long long block_excl_scan64(long long v, long long *s_wsum, long long *total) {
+    constexpr int NW = NPB / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long incl = warp_incl_scan64(v);
+    if (lane == 31) s_wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        long long x = lane < NW ? s_wsum[lane] : 0;
+        x = warp_incl_scan64(x);
+        if (lane < NW) s_wsum[lane] = x;
+    }
+    __syncthreads();
+    *total = s_wsum[NW - 1];
+    return incl - v + (warp > 0 ? s_wsum[warp - 1] : 0);
+}
+
 // Block-wide exclusive scan of one int per thread (NPB threads); the total in *total.
 template <int NPB>
 __device__ __forceinline__ int block_excl_scan(int v, int *s_wsum, int *total) {
@@ -309,8 +338,55 @@ __device__ __forceinline__ long long pull_intake(const StepArgs &a, const PopDev
 
 // ------------------------------------------------------------------ delivery
 
-// One link word into the target's arrival slot (n + delay) mod D; out-of-range links counted, not written.
-__device__ __forceinline__ void deliver_rec(const StepArgs &a, const ConnDev &C, uint32_t rec, int l, long long n,
+// What delivering a push link needs of its connection, compact: the launch copies it into shared memory
+// (every lane of a walk may look up a different connection; shared memory serves that in one pass, the
+// parameter space's constant cache would serialize it).
+struct SConn {
+    long long *tgt_acc;
+    const uint32_t *link;
+    const float *w;
+    long long wfx;
+    float wscale;
+    int32_t tgt_n, tgt_acc_mask, homogeneous;
+};
+constexpr int SMEM_CONNS = 64;  // push connections whose SConn the launch keeps in shared memory
+
+__device__ __forceinline__ SConn sconn_of(const ConnDev &C) {
+    SConn s;
+    s.tgt_acc = C.tgt_acc;
+    s.link = C.link;
+    s.w = C.w;
+    s.wfx = C.wfx;
+    s.wscale = C.wscale;
+    s.tgt_n = C.tgt_n;
+    s.tgt_acc_mask = C.tgt_acc_mask;
+    s.homogeneous = C.homogeneous;
+    return s;
+}
+
+// Push connection c's SConn: from the launch's shared table, or (more connections than it holds) global memory.
+__device__ __forceinline__ SConn conn_view(const StepArgs &a, const SConn *s_conn, int c) {
+    return s_conn ? s_conn[c] : sconn_of(a.push[c]);
+}
+
+// Fill the shared table (every thread of the block, before a barrier).
+template <bool INL>
+__device__ __forceinline__ const SConn *fill_conns(const StepArgs &a, SConn *s_conn, int n_push) {
+    if (n_push > SMEM_CONNS) return nullptr;
+    for (int c = threadIdx.x; c < n_push; c += blockDim.x) s_conn[c] = sconn_of(push_at<INL>(a, c));
+    return s_conn;
+}
+
+// Link l's per-link weight (0 for a single-weight connection), loaded with its link word, not after it.
+template <class C_>
+__device__ __forceinline__ float link_weight(const C_ &C, int l) {
+    return C.homogeneous ? 0.f : __ldg(C.w + l);
+}
+
+// One link word (and its weight) into the target's arrival slot (n + delay) mod D; out-of-range links
+// counted, not written.
+template <class C_>
+__device__ __forceinline__ void deliver_rec(const StepArgs &a, const C_ &C, uint32_t rec, float w, long long n,
                                             int min_delay) {
     const int d = (int)(rec >> 24), t = (int)(rec & 0xFFFFFFu);
     if (d < min_delay) {
@@ -321,7 +397,7 @@ __device__ __forceinline__ void deliver_rec(const StepArgs &a, const ConnDev &C,
         atomicAdd(a.err + 0, 1);
         return;
     }
-    const long long wfx = C.homogeneous ? C.wfx : weight_fx(__ldg(C.w + l), C.wscale);
+    const long long wfx = C.homogeneous ? C.wfx : weight_fx(w, C.wscale);
     atomicAdd(reinterpret_cast<unsigned long long *>(C.tgt_acc + (size_t)((n + d) & C.tgt_acc_mask) * (size_t)C.tgt_n + t),
               (unsigned long long)wfx);
 }
@@ -339,78 +415,104 @@ __device__ __forceinline__ Row row_of(const ConnDev &C, int j) {
     return r;
 }
 
-// The block's spikes, every outgoing push connection at once. Each spiking thread counts its links (the
-// events, counted when they are emitted) and appends its far items (the atomics' latency hidden under the
-// near walk); the block walks the near links of all (spike, connection) entries as one flat range.
+// A block's shared scratch of one tile phase (declared once per kernel).
+template <int NPB>
+struct Scratch {
+    int cnt;
+    int spk[NPB];                      // the tile's spiking neurons (population indices), compacted
+    int row[NPB + 1];                  // connections past MERGE_OUT: per spike its row start
+    int off[NPB + 1];                  // ... and its near-link offsets
+    int wsum[NPB / 32];
+    int w_pref[NPB / 32][MERGE_OUT + 1];  // per warp: its spike's near links, prefix over connections
+    int w_r0[NPB / 32][MERGE_OUT];        // per warp: its spike's row start per connection
+};
+
+// The block's spikes, one warp per spike, its first MERGE_OUT outgoing push connections at once. Lane c holds
+// connection c's row bounds (from shared memory for a persistent block's own tile, else one round trip);
+// lane 0 claims the spike's far items with one atomic, issued before the walk and used after it; the warp
+// walks the spike's delay-1 links of every connection as one flat range, NEAR_BATCH loads per lane issued
+// before their reductions (an in-order issue would otherwise wait on each load before the next).
+constexpr int NEAR_BATCH = 4;
+
 template <int NPB, bool INL>
-__device__ __forceinline__ void deliver_spikes(const StepArgs &a, const PopDev &P, const Row *rows, bool fire,
-                                               int pos, int cnt, long long n, int *s_row, int *s_off,
-                                               int *s_wsum) {
-    const int tid = threadIdx.x, lane = tid & 31;
-    const int n_out = min(P.n_out, PREFETCH_OUT);
-    int links = 0;
-    int n_items[PREFETCH_OUT] = {}, at[PREFETCH_OUT] = {};
-#pragma unroll
-    for (int c = 0; c < PREFETCH_OUT; ++c) {
-        if (c < n_out && fire) {
-            const Row &r = rows[c];
-            links += r.r1 - r.r0;
-            s_row[pos * PREFETCH_OUT + c] = r.r0;
-            s_off[pos * PREFETCH_OUT + c] = r.sp - r.r0;  // near links, scanned below
-            n_items[c] = (r.r1 - r.sp + NPB - 1) / NPB;
-            if (n_items[c] > 0) at[c] = atomicAdd(a.item_count + (int)(n % 3), n_items[c]);
-        }
-    }
-    const int warp_links = __reduce_add_sync(FULL, links);
-    if (lane == 0 && warp_links) atomicAdd(a.counters + 0, (unsigned long long)warp_links);
-    __syncthreads();
-    // entries (spike, connection) = pos * PREFETCH_OUT + c, those of absent connections empty; each thread
-    // scans PREFETCH_OUT consecutive entries (NPB * PREFETCH_OUT >= n_ent)
-    const int n_ent = cnt * PREFETCH_OUT;
-    int v[PREFETCH_OUT];
-    int mine = 0;
-#pragma unroll
-    for (int c = 0; c < PREFETCH_OUT; ++c) {
-        const int e = tid * PREFETCH_OUT + c;
-        v[c] = (e < n_ent && c < n_out) ? s_off[e] : 0;
-        mine += v[c];
-    }
-    int total = 0;
-    int off = block_excl_scan<NPB>(mine, s_wsum, &total);
-#pragma unroll
-    for (int c = 0; c < PREFETCH_OUT; ++c) {
-        const int e = tid * PREFETCH_OUT + c;
-        if (e < n_ent) s_off[e] = off;
-        off += v[c];
-    }
-    if (tid == 0) s_off[n_ent] = total;
-    __syncthreads();
-    for (int idx = tid; idx < total; idx += NPB) {
-        int lo = 0, hi = n_ent;  // s_off[lo] <= idx < s_off[hi]
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (s_off[mid] <= idx) lo = mid; else hi = mid;
-        }
-        const ConnDev &C = push_at<INL>(a, P.out_first + lo % PREFETCH_OUT);
-        const int l = s_row[lo] + (idx - s_off[lo]);
-        deliver_rec(a, C, __ldg(C.link + l), l, n, 1);
-    }
-    int4 *list = a.items + (size_t)(n % 3) * (size_t)a.item_cap;
-#pragma unroll
-    for (int c = 0; c < PREFETCH_OUT; ++c) {
-        for (int k = 0; k < n_items[c]; ++k) {
-            if (at[c] + k < a.item_cap) {
-                const int l0 = rows[c].sp + k * NPB;
-                list[at[c] + k] = make_int4(P.out_first + c, l0, min(l0 + NPB, rows[c].r1), 0);
+__device__ __forceinline__ void deliver_spikes(const StepArgs &a, const PopDev &P, int tile_y, const int *s_cache,
+                                               int cnt, long long n, Scratch<NPB> &sc, const SConn *s_conn,
+                                               int k = 0) {
+    constexpr int NW = NPB / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int m = min(P.n_out, MERGE_OUT);
+    int *pref = sc.w_pref[warp], *r0s = sc.w_r0[warp];
+    // fewer spikes than warps: each spike's walk split over a group of g warps (g a power of two)
+    int g = 1;
+    while (2 * g * cnt <= NW) g *= 2;
+    const int sub = warp % g;
+    for (int p = warp / g; p < cnt; p += NW / g) {
+        const int jj = sc.spk[p];
+        Row r = Row{0, 0, 0};
+        if (lane < m) {
+            if (s_cache) {
+                const int t = jj - tile_y;
+                r = Row{s_cache[(3 * lane) * NPB + t], s_cache[(3 * lane + 1) * NPB + t], s_cache[(3 * lane + 2) * NPB + t]};
             } else {
-                atomicAdd(a.err + 3, 1);
+                r = row_of(push_at<INL>(a, P.out_first + lane), jj);
+            }
+        }
+        const int near_c = r.sp - r.r0;
+        const int items_c = (r.r1 - r.sp + NPB - 1) / NPB;
+        const int items_incl = warp_incl_scan(items_c);
+        const int near_incl = warp_incl_scan(near_c);
+        const int total_items = __shfl_sync(FULL, items_incl, 31);
+        const int total_near = __shfl_sync(FULL, near_incl, 31);
+        const int links = __reduce_add_sync(FULL, r.r1 - r.r0);
+        int base = 0;
+        if (lane == 0 && sub == 0) {  // the group's first warp claims the items and counts the events
+            if (total_items > 0) base = atomicAdd(a.item_count + (int)(n % 3), total_items);
+            if (links) atomicAdd(a.counters + 0, (unsigned long long)links);
+        }
+        if (lane < m) {
+            pref[lane] = near_incl - near_c;
+            r0s[lane] = r.r0;
+        }
+        if (lane == 0) pref[m] = total_near;
+        __syncwarp();
+        for (int b0 = sub * 32; b0 < total_near; b0 += 32 * g * NEAR_BATCH) {
+            uint32_t rec[NEAR_BATCH];
+            float w[NEAR_BATCH];
+            int cc[NEAR_BATCH];
+#pragma unroll
+            for (int b = 0; b < NEAR_BATCH; ++b) {
+                const int idx = b0 + b * 32 * g + lane;
+                cc[b] = -1;
+                if (idx < total_near) {
+                    int c = 0;
+                    while (c + 1 < m && pref[c + 1] <= idx) ++c;
+                    const SConn C = conn_view(a, s_conn, P.out_first + c);
+                    const int l = r0s[c] + (idx - pref[c]);
+                    rec[b] = __ldg(C.link + l);
+                    w[b] = link_weight(C, l);
+                    cc[b] = c;
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < NEAR_BATCH; ++b)
+                if (cc[b] >= 0) deliver_rec(a, conn_view(a, s_conn, P.out_first + cc[b]), rec[b], w[b], n, 1);
+        }
+        __syncwarp();
+        if (sub == 0) {
+            base = __shfl_sync(FULL, base, 0);
+            if (lane < m && items_c > 0) {
+                int at = base + items_incl - items_c;
+                int4 *list = a.items + (size_t)(n % 3) * (size_t)a.item_cap;
+                for (int q = r.sp; q < r.r1; q += NPB, ++at) {
+                    if (at < a.item_cap) list[at] = make_int4(P.out_first + lane, q, min(q + NPB, r.r1), 0);
+                    else atomicAdd(a.err + 3, 1);
+                }
             }
         }
     }
-    __syncthreads();  // s_row / s_off free again
 }
 
-// Connections past the first PREFETCH_OUT: one at a time, their rows loaded on demand.
+// Connections past the first MERGE_OUT: one at a time, their rows loaded on demand.
 template <int NPB, bool INL>
 __device__ __forceinline__ void deliver_spikes_one(const StepArgs &a, const ConnDev &C, int c, const Row &row,
                                                    bool fire, int pos, int cnt, long long n, int *s_row, int *s_off,
@@ -440,7 +542,7 @@ __device__ __forceinline__ void deliver_spikes_one(const StepArgs &a, const Conn
             if (s_off[mid] <= idx) lo = mid; else hi = mid;
         }
         const int l = s_row[lo] + (idx - s_off[lo]);
-        deliver_rec(a, C, __ldg(C.link + l), l, n, 1);
+        deliver_rec(a, C, __ldg(C.link + l), link_weight(C, l), n, 1);
     }
     if (n_items > 0) {
         int4 *list = a.items + (size_t)(n % 3) * (size_t)a.item_cap;
@@ -458,30 +560,22 @@ __device__ __forceinline__ void deliver_spikes_one(const StepArgs &a, const Conn
 
 // ------------------------------------------------------------------ one tile of one step
 
-// A neuron's state as its thread holds it through a step: membrane, current, refractory count, and its
-// outgoing row bounds. A persistent launch keeps its block's first tile here for the whole window.
+// A neuron's state as its thread holds it through a step: membrane, current, refractory count. A
+// persistent launch keeps its block's first tile here (and that tile's row bounds in shared memory) for the
+// whole window.
 struct Neuron {
     float v, cur;
     int ref;
-    Row rows[PREFETCH_OUT];
 };
 
-template <bool INL>
-__device__ __forceinline__ void load_neuron(const StepArgs &a, const PopDev &P, int j, bool live, Neuron &nr) {
+__device__ __forceinline__ void load_neuron(const PopDev &P, int j, bool live, Neuron &nr) {
     nr.v = 0.f;
     nr.cur = 0.f;
     nr.ref = 0;
-#pragma unroll
-    for (int c = 0; c < PREFETCH_OUT; ++c) nr.rows[c] = Row{0, 0, 0};
-    if (!live) return;
-    if (P.model != 3) {
-        nr.v = P.v[j];
-        nr.ref = P.ref[j];
-        if (P.model == 2) nr.cur = P.i[j];
-    }
-#pragma unroll
-    for (int c = 0; c < PREFETCH_OUT; ++c)
-        if (c < P.n_out) nr.rows[c] = row_of(push_at<INL>(a, P.out_first + c), j);
+    if (!live || P.model == 3) return;
+    nr.v = P.v[j];
+    nr.ref = P.ref[j];
+    if (P.model == 2) nr.cur = P.i[j];
 }
 
 __device__ __forceinline__ void store_neuron(const PopDev &P, int j, bool live, const Neuron &nr) {
@@ -491,14 +585,26 @@ __device__ __forceinline__ void store_neuron(const PopDev &P, int j, bool live, 
     if (P.model == 2) P.i[j] = nr.cur;
 }
 
+// The row bounds of a tile's neurons in its first MERGE_OUT outgoing connections, into shared memory:
+// s_cache[(3c + 0/1/2) * NPB + thread] = first link / split / end of connection c's row.
+template <int NPB, bool INL>
+__device__ __forceinline__ void cache_rows(const StepArgs &a, const PopDev &P, int j, bool live, int *s_cache) {
+    const int m = min(P.n_out, MERGE_OUT);
+    for (int c = 0; c < m; ++c) {
+        const Row r = live ? row_of(push_at<INL>(a, P.out_first + c), j) : Row{0, 0, 0};
+        s_cache[(3 * c) * NPB + threadIdx.x] = r.r0;
+        s_cache[(3 * c + 1) * NPB + threadIdx.x] = r.sp;
+        s_cache[(3 * c + 2) * NPB + threadIdx.x] = r.r1;
+    }
+}
+
 // One tile of one step. CACHED: the tile's Neuron is held in registers by the caller across steps (loaded
-// before the window, stored after it); otherwise it is loaded and stored here.
+// before the window, stored after it) and its row bounds are in s_cache; otherwise both come from memory.
 template <int NPB, bool INL, bool CACHED>
-__device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n, const int4 tile, int k, Neuron &nr) {
-    __shared__ int s_cnt;
-    __shared__ int s_row[NPB * PREFETCH_OUT];
-    __shared__ int s_off[NPB * PREFETCH_OUT + 1];
-    __shared__ int s_wsum[NPB / 32];
+__device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n, const int4 tile, int k, Neuron &nr,
+                                           const int *s_cache, Scratch<NPB> &sc, const SConn *s_conn) {
+    int &s_cnt = sc.cnt;
+    int *s_row = sc.row, *s_off = sc.off, *s_wsum = sc.wsum;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const PopDev &P = pop_at<INL>(a, tile.x);
@@ -507,7 +613,7 @@ __device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n,
     __syncthreads();  // a block's previous tile: every thread past its reads of the shared arrays
     if (tid == 0) s_cnt = 0;
 
-    // the arrival slot (and, uncached, the state and row bounds: none of these loads waits for another)
+    // the arrival slot (and, uncached, the state: the loads do not wait for each other)
     const int model = P.model;
     long long acc = 0;
     long long *slot = nullptr;
@@ -515,10 +621,9 @@ __device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n,
         slot = P.acc + (size_t)(n & P.acc_mask) * (size_t)P.n + j;
         acc = __ldcg(slot);  // L2: other blocks' adds of this kernel are there, not in this SM's L1
     }
-    if (!CACHED) load_neuron<INL>(a, P, j, live, nr);
+    if (!CACHED) load_neuron(P, j, live, nr);
     float &v = nr.v, &cur = nr.cur;
     int &ref = nr.ref;
-    const Row *rows = nr.rows;
     const int n_out = P.n_out;
 
     // 1-2. intake and update
@@ -551,6 +656,7 @@ __device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n,
     if (lane == 0 && b) base = atomicAdd(&s_cnt, __popc(b));
     base = __shfl_sync(FULL, base, 0);
     const int pos = base + __popc(b & ((1u << lane) - 1u));
+    if (fire) sc.spk[pos] = j;
     __syncthreads();
     N2B_STAMP(a, k, 1);
     const int cnt = s_cnt;
@@ -561,8 +667,8 @@ __device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n,
     }
 
     // 4. the spikes' outgoing rows
-    if (n_out > 0) deliver_spikes<NPB, INL>(a, P, rows, fire, pos, cnt, n, s_row, s_off, s_wsum);
-    for (int c = PREFETCH_OUT; c < n_out; ++c) {
+    if (n_out > 0) deliver_spikes<NPB, INL>(a, P, tile.y, CACHED ? s_cache : nullptr, cnt, n, sc, s_conn, k);
+    for (int c = MERGE_OUT; c < n_out; ++c) {
         const ConnDev &C = push_at<INL>(a, P.out_first + c);
         const Row r = fire ? row_of(C, j) : Row{0, 0, 0};
         deliver_spikes_one<NPB, INL>(a, C, P.out_first + c, r, fire, pos, cnt, n, s_row, s_off, s_wsum);
@@ -571,7 +677,7 @@ __device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n,
 
 // 5. the far links of step n - 1: items of NPB links, one link per thread, two items at a time
 template <int NPB, bool INL>
-__device__ __forceinline__ void far_phase(const StepArgs &a, const long long n) {
+__device__ __forceinline__ void far_phase(const StepArgs &a, const long long n, const SConn *s_conn) {
     const long long m = n - 1;
     const int lst = (int)(((m % 3) + 3) % 3);
     const int4 *list = a.items + (size_t)lst * (size_t)a.item_cap;
@@ -596,36 +702,44 @@ __device__ __forceinline__ void far_phase(const StepArgs &a, const long long n) 
             pre1 = i + 3 * G < count ? __ldcg(list + i + 3 * G) : make_int4(0, 0, 0, 0);
         }
         const int l0 = it0.y + (int)threadIdx.x, l1 = it1.y + (int)threadIdx.x;
-        const ConnDev &C0 = push_at<INL>(a, it0.x);
-        const ConnDev &C1 = push_at<INL>(a, it1.x);
+        const SConn C0 = conn_view(a, s_conn, it0.x);
+        const SConn C1 = conn_view(a, s_conn, it1.x);
         const bool h0 = l0 < it0.z, h1 = two && l1 < it1.z;
         const uint32_t rec0 = h0 ? __ldg(C0.link + l0) : 0u;
         const uint32_t rec1 = h1 ? __ldg(C1.link + l1) : 0u;
-        if (h0) deliver_rec(a, C0, rec0, l0, m, 2);
-        if (h1) deliver_rec(a, C1, rec1, l1, m, 2);
+        const float w0 = h0 ? link_weight(C0, l0) : 0.f;
+        const float w1 = h1 ? link_weight(C1, l1) : 0.f;
+        if (h0) deliver_rec(a, C0, rec0, w0, m, 2);
+        if (h1) deliver_rec(a, C1, rec1, w1, m, 2);
     }
 }
 
 template <int NPB, bool INL>
-__device__ __forceinline__ void step_body(const StepArgs &a, const long long n, int k, Neuron *cached) {
+__device__ __forceinline__ void step_body(const StepArgs &a, const long long n, int k, Neuron *cached,
+                                          const int *s_cache, const SConn *s_conn) {
+    __shared__ Scratch<NPB> sc;
     N2B_STAMP(a, k, 0);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.item_count + (int)((n + 1) % 3), 0);  // step n + 1's list
     int t = blockIdx.x;
     if (cached != nullptr && t < a.n_tiles) {
-        tile_phase<NPB, INL, true>(a, n, tile_at<INL, NPB>(a, t), k, *cached);
+        tile_phase<NPB, INL, true>(a, n, tile_at<INL, NPB>(a, t), k, *cached, s_cache, sc, s_conn);
         t += gridDim.x;
     }
     Neuron nr;
-    for (; t < a.n_tiles; t += gridDim.x) tile_phase<NPB, INL, false>(a, n, tile_at<INL, NPB>(a, t), k, nr);
+    for (; t < a.n_tiles; t += gridDim.x)
+        tile_phase<NPB, INL, false>(a, n, tile_at<INL, NPB>(a, t), k, nr, nullptr, sc, s_conn);
     N2B_STAMP(a, k, 2);
-    far_phase<NPB, INL>(a, n);
+    far_phase<NPB, INL>(a, n, s_conn);
     N2B_STAMP(a, k, 3);
 }
 
 // One step per launch: the launch boundary is the step's barrier.
 template <int NPB, bool INL>
 __global__ void __launch_bounds__(NPB) step_kernel(const __grid_constant__ StepArgs a) {
-    step_body<NPB, INL>(a, *a.step + a.offset, 0, nullptr);
+    __shared__ SConn s_tab[SMEM_CONNS];
+    const SConn *s_conn = fill_conns<INL>(a, s_tab, a.n_push);
+    __syncthreads();
+    step_body<NPB, INL>(a, *a.step + a.offset, 0, nullptr, nullptr, s_conn);
 }
 
 __device__ __forceinline__ unsigned long long globaltimer() {
@@ -678,7 +792,7 @@ __device__ __forceinline__ bool grid_sync(const StepArgs &a, unsigned k) {
 
 // A window of n_steps steps in one cooperative launch (every block resident), steps separated by grid_sync.
 template <int NPB, bool INL>
-__global__ void __launch_bounds__(NPB) persistent_kernel(const __grid_constant__ StepArgs a, const int n_steps) {
+__global__ void __launch_bounds__(NPB, 768 / NPB) persistent_kernel(const __grid_constant__ StepArgs a, const int n_steps) {
     if (*(volatile unsigned *)(a.barrier + BAR_ABORT)) return;  // an earlier window gave up: nothing runs
     const long long n0 = *a.step;
     // the block's first tile stays in registers for the whole window
@@ -688,9 +802,14 @@ __global__ void __launch_bounds__(NPB) persistent_kernel(const __grid_constant__
     const int j = tile.y + (int)threadIdx.x;
     const bool live = has_tile && (int)threadIdx.x < tile.z;
     Neuron mine;
-    load_neuron<INL>(a, P, j, live, mine);
+    load_neuron(P, j, live, mine);
+    __shared__ int s_cache[3 * MERGE_OUT * NPB];
+    cache_rows<NPB, INL>(a, P, j, live, s_cache);
+    __shared__ SConn s_tab[SMEM_CONNS];
+    const SConn *s_conn = fill_conns<INL>(a, s_tab, a.n_push);
+    __syncthreads();
     for (int k = 0; k < n_steps; ++k) {
-        step_body<NPB, INL>(a, n0 + k, k, &mine);
+        step_body<NPB, INL>(a, n0 + k, k, &mine, s_cache, s_conn);
         if (!grid_sync(a, (unsigned)k)) break;
         N2B_STAMP(a, k, 4);
     }

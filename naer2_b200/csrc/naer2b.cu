@@ -341,7 +341,9 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     const int persistent = opt && opt->persistent;
     const bool inl = n_pops <= n2b::INLINE_POPS && (int32_t)push.size() <= n2b::INLINE_PUSH &&
                      (int32_t)pull.size() <= n2b::INLINE_PULL;
-    int want = (opt && opt->grid > 0) ? opt->grid : 2 * sms;
+    // default: two blocks per SM, and for persistent windows at least one per tile plus half an SM's worth of
+    // tile-free blocks for the far links (capped by what can be resident)
+    int want = (opt && opt->grid > 0) ? opt->grid : std::max(2 * sms, persistent ? L.n_tiles + sms / 2 : 0);
     int grid = std::max(L.n_tiles, want);
     if (persistent) {
         int most = 0;
@@ -376,6 +378,7 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     a.offset = 0;
     a.barrier = reinterpret_cast<unsigned *>(ws + L.barrier);
     a.n_pops = n_pops;
+    a.n_push = L.n_push;
     if (inl) {
         // inline: tiles in population order (the global table lists the largest populations first)
         int32_t t = 0;

@@ -75,12 +75,14 @@ class fixed_outdegree(_Drawn):
     (test/networks/PD14/connection.py:8-35): given a connection probability p, the total
     Q = ln(1 - p) / ln(1 - 1/(N_src N_tgt)) split as k = round(Q / N_src) per source; or k given."""
 
-    def __init__(self, probability: float | None = None, k: int | None = None, seed: int | None = None):
+    def __init__(self, probability: float | None = None, k: int | None = None, seed: int | None = None,
+                 device=None):
         if (probability is None) == (k is None):
             raise ValueError("give one of probability or k")
         self.probability = probability
         self.k = k
         self.seed = next(_SEEDS) if seed is None else int(seed)
+        self.device = torch.device(device) if device is not None else None  # draw there (torch's Philox)
         self._cache = None
 
     def per_source(self, n_src: int, n_tgt: int) -> int:
@@ -93,6 +95,12 @@ class fixed_outdegree(_Drawn):
 
     def links(self, n_src: int, n_tgt: int, same: bool = False):
         k = self.per_source(n_src, n_tgt)
+        if self.device is not None and self.device.type == "cuda":
+            offsets = torch.arange(n_src + 1, dtype=torch.int64, device=self.device) * k
+            if k == 0:
+                return offsets, torch.zeros(0, dtype=torch.int64, device=self.device)
+            g = torch.Generator(device=self.device).manual_seed(self.seed)
+            return offsets, torch.randint(0, n_tgt, (n_src * k,), generator=g, device=self.device)
         offsets = np.arange(n_src + 1, dtype=np.int64) * k
         if k == 0:
             return offsets, np.zeros(0, dtype=np.int64)

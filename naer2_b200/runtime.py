@@ -52,26 +52,31 @@ def wfx(w: float, shift: int) -> int:
     return int(np.rint(np.ldexp(np.float32(w), shift)))
 
 
-def weights_of(conn, n_links: int):
-    """(scalar or None, per-link fp32 array or None): a connection's weights in canonical order."""
+def weights_of(conn, n_links: int, device=None):
+    """(scalar or None, per-link fp32 tensor or None): a connection's weights in canonical order (a tensor of
+    one value counts as a scalar)."""
     w = conn.fabric.value("weight")
     if w is None:
         raise ValueError(f"connection {conn._source!r} -> {conn._target!r} has no weight")
     if isinstance(w, torch.Tensor):
         if w.numel() == 1:
             return float(np.float32(float(w.reshape(())))), None
-        arr = w.detach().cpu().to(torch.float32).numpy().reshape(-1)
-        if len(arr) != n_links:
-            raise ValueError(f"weight has {len(arr)} values for {n_links} links")
-        if len(arr) and np.all(arr == arr[0]):
+        arr = w.detach().reshape(-1).to(torch.float32)
+        if device is not None:
+            arr = arr.to(device)
+        if arr.numel() != n_links:
+            raise ValueError(f"weight has {arr.numel()} values for {n_links} links")
+        if arr.numel() == 0:
+            return 0.0, None
+        if bool((arr == arr[0]).all()):
             return float(arr[0]), None
-        return None, np.ascontiguousarray(arr, dtype=np.float32)
+        return None, arr.contiguous()
     return float(np.float32(w)), None
 
 
 @dataclass
 class PopDesc:
-    """One population as the kernels see it (host arrays; the n2b_population fields)."""
+    """One population as the kernels see it (the n2b_population fields)."""
     model: int
     n: int
     acc_depth: int
@@ -89,19 +94,27 @@ class PopDesc:
 
 @dataclass
 class ConnDesc:
-    """One connection in its device form (push rows by source or pull rows by target)."""
+    """One connection in its device form (push rows by source or pull rows by target), torch tensors on the
+    device its topology was built on; `canonical()` gives the canonical rows (for the oracle)."""
     src: int
     tgt: int
     mode: str
     n_links: int
-    ptr: np.ndarray       # int32
-    link: np.ndarray      # uint32: delay << 24 | index
-    weight: float         # when w is None
-    w: np.ndarray | None  # fp32 per link, in the form's order
-    split: np.ndarray | None = field(default=None)  # push: per row its first link of delay >= 2
-    push_ptr: np.ndarray = field(default=None)   # the canonical order, rows per source (for checks)
-    push_link: np.ndarray = field(default=None)
-    push_w: np.ndarray | None = field(default=None)
+    ptr: torch.Tensor              # int32
+    link: torch.Tensor             # int32 bit pattern of uint32: delay << 24 | index
+    weight: float                  # when w is None
+    w: torch.Tensor | None         # fp32 per link, in the form's order
+    split: torch.Tensor | None     # push: per row its first link of delay >= 2
+    topo: object = None            # the canonical Topology
+    steps: torch.Tensor = None     # per-link delays in steps, canonical order
+    warr: torch.Tensor | None = None  # per-link weights, canonical order
+
+    def canonical(self):
+        """(ptr int32, link uint32, w fp32 or None) as numpy arrays, rows per source in canonical order."""
+        ptr = self.topo.source_offsets.cpu().numpy().astype(np.int32)
+        link = pack_links(self.topo.target_indices, self.steps.to(self.topo.target_indices.device))
+        w = self.warr.cpu().numpy() if self.warr is not None else None
+        return ptr, link.cpu().numpy().view(np.uint32), w
 
 
 @dataclass
@@ -114,8 +127,9 @@ class NetDesc:
 
 def describe(net, modes: dict | None = None) -> NetDesc:
     """The network as the kernels see it: per population its model constants, ring depths, fixed-point
-    shift and external-drive table; per connection its CSR form. modes: connection id -> "push" / "pull"
-    (default: the connection's own `mode`, else the network's tuned choice, else push)."""
+    shift and external-drive table; per connection its CSR form, built where its topology lives (a pattern
+    drawn on the GPU is restructured there). modes: connection id -> "push" / "pull" (default: the
+    connection's own `mode`, else the network's tuned choice, else push)."""
     dt = float(net.resolution)
     pops, conns = list(net.populations), list(net.connections)
     index = {id(p): k for k, p in enumerate(pops)}
@@ -126,7 +140,8 @@ def describe(net, modes: dict | None = None) -> NetDesc:
     kp = [params_of(p, dt) for p in pops]
     max_in_delay = [0] * len(pops)
     max_pull_delay = [0] * len(pops)
-    in_sum = [np.zeros(len(p.shape)) for p in pops]
+    in_max = [0.0] * len(pops)
+    in_sum: list = [None] * len(pops)
     cinfo = []
     for c in conns:
         s, t = index[id(c._source)], index[id(c._target)]
@@ -136,24 +151,30 @@ def describe(net, modes: dict | None = None) -> NetDesc:
         if port not in pops[t].ports:
             raise ValueError(f"{pops[t]!r} has no receive port {port!r}")
         topo = c.fabric.topology
+        dev = topo.target_indices.device
         n_links = len(topo)
-        steps = delay_steps(c.fabric.value("delay"), n_links, dt)
-        wscalar, warr = weights_of(c, n_links)
+        steps = delay_steps(c.fabric.value("delay"), n_links, dt, device=dev)
+        wscalar, warr = weights_of(c, n_links, device=dev)
         mode = (modes or {}).get(id(c)) or c.mode or net.tuned.get(id(c), "push")
         if n_links:
-            tgt = topo.target_indices.numpy()
-            absw = np.abs(warr.astype(np.float64)) if warr is not None else np.full(n_links, abs(wscalar))
-            in_sum[t] += np.bincount(tgt, weights=absw, minlength=len(pops[t].shape))
+            tgt = topo.target_indices
+            absw = warr.abs().to(torch.float64) if warr is not None else None
+            part = torch.bincount(tgt, weights=absw, minlength=len(pops[t].shape)).to(torch.float64)
+            if warr is None:
+                part = part * abs(wscalar)
+            in_sum[t] = part.cpu() if in_sum[t] is None else in_sum[t] + part.cpu()
             max_in_delay[t] = max(max_in_delay[t], int(steps.max()))
             if mode == "pull":
                 max_pull_delay[s] = max(max_pull_delay[s], int(steps.max()))
         cinfo.append((s, t, topo, steps, wscalar, warr, mode))
+    for k in range(len(pops)):
+        in_max[k] = float(in_sum[k].max()) if in_sum[k] is not None and len(in_sum[k]) else 0.0
 
     pdesc = []
     for k, (p, par) in enumerate(zip(pops, kp)):
         n = len(p.shape)
         table = par["ext_table"]
-        max_input = float(in_sum[k].max()) if n else 0.0
+        max_input = in_max[k]
         if len(table):
             max_input += abs(par["ext_weight"]) * (len(table) - 1)
         sh = fixed_shift(max_input)
@@ -169,8 +190,6 @@ def describe(net, modes: dict | None = None) -> NetDesc:
     cdesc = []
     for s, t, topo, steps, wscalar, warr, mode in cinfo:
         n_tgt = len(pops[t].shape)
-        canon_ptr = topo.source_offsets.numpy().astype(np.int32)
-        canon_link = pack_links(topo.target_indices.numpy(), steps)
         split = None
         if mode == "pull":
             ptr, link, perm = pull_form(topo, steps, n_tgt)
@@ -178,10 +197,10 @@ def describe(net, modes: dict | None = None) -> NetDesc:
             ptr, link, perm, split = push_form(topo, steps, n_tgt)
         else:
             raise ValueError(f"unknown connection mode {mode!r}")
-        w = warr[perm] if warr is not None else None
+        w = warr[perm].contiguous() if warr is not None else None
         cdesc.append(ConnDesc(src=s, tgt=t, mode=mode, n_links=len(topo), ptr=ptr, link=link,
                               weight=wscalar if wscalar is not None else 0.0, w=w, split=split,
-                              push_ptr=canon_ptr, push_link=canon_link, push_w=warr))
+                              topo=topo, steps=steps, warr=warr))
     return NetDesc(dt=dt, pops=pdesc, conns=cdesc, n_links=sum(c.n_links for c in cdesc))
 
 
@@ -242,13 +261,11 @@ class NetworkRuntime:
             cc = self.cconn[k]
             cc.src, cc.tgt, cc.n_links = c.src, c.tgt, c.n_links
             cc.mode = _lib.PULL if c.mode == "pull" else _lib.PUSH
-            cc.ptr = dev_tensor(torch.from_numpy(c.ptr)).data_ptr()
-            link = c.link if len(c.link) else np.zeros(1, dtype=np.uint32)
-            cc.link = dev_tensor(torch.from_numpy(link.view(np.int32).copy())).data_ptr()
+            cc.ptr = dev_tensor(c.ptr).data_ptr()
+            cc.link = dev_tensor(c.link if c.link.numel() else torch.zeros(1, dtype=torch.int32)).data_ptr()
             cc.weight = c.weight
-            cc.w = dev_tensor(torch.from_numpy(c.w)).data_ptr() if c.w is not None else None
-            cc.split = dev_tensor(torch.from_numpy(c.split)).data_ptr() if c.split is not None and len(c.split) \
-                else None
+            cc.w = dev_tensor(c.w).data_ptr() if c.w is not None else None
+            cc.split = dev_tensor(c.split).data_ptr() if c.split is not None and c.split.numel() else None
         self.modes = [c.mode for c in desc.conns]
         self.n_links = desc.n_links
 

@@ -97,6 +97,8 @@ class Topology:
             offsets, targets = pattern.links(n_src, n_tgt if n_tgt is not None else n_src,
                                              same=same or target_region is None)
             topo = Topology(torch.as_tensor(offsets, dtype=torch.int64), torch.as_tensor(targets, dtype=torch.int64))
+            if topo.source_offsets.device != topo.target_indices.device:
+                topo.source_offsets = topo.source_offsets.to(topo.target_indices.device)
             if target_region is None:
                 size = int(topo.target_indices.max()) + 1 if len(topo) else 0
                 return topo, Region(size)
@@ -126,60 +128,73 @@ class Topology:
         return (topo, inferred) if target_region is None else topo
 
 
-def delay_steps(delay, n_links: int, dt: float) -> np.ndarray:
-    """Per-link delays in whole steps of dt: round(delay / dt), at least 1 (a spike is delivered from the
-    next step on; the reference clamps delays to >= its 0.1 ms resolution, test/networks/PD14/net.py:102)."""
-    if delay is None:
-        return np.ones(n_links, dtype=np.int64)
+def delay_steps(delay, n_links: int, dt: float, device=None) -> torch.Tensor:
+    """Per-link delays in whole steps of dt (int64, on `device` or the delay tensor's): round(delay / dt) half
+    to even, at least 1 (a spike is delivered from the next step on; the reference clamps delays to >= its
+    0.1 ms resolution, test/networks/PD14/net.py:102)."""
     if isinstance(delay, torch.Tensor):
-        d = delay.detach().cpu().double().numpy().reshape(-1)
-        if len(d) != n_links:
-            raise ValueError(f"delay has {len(d)} values for {n_links} links")
+        d = delay.detach().reshape(-1)
+        if device is not None:
+            d = d.to(device)
+        if d.numel() != n_links:
+            raise ValueError(f"delay has {d.numel()} values for {n_links} links")
+        steps = torch.round(d.to(torch.float64) / dt).to(torch.int64)
     else:
-        d = np.full(n_links, float(delay))
-    steps = np.rint(d / dt).astype(np.int64)
-    steps = np.maximum(steps, 1)
-    if len(steps) and steps.max() > MAX_DELAY_STEPS:
+        value = 1 if delay is None else int(np.rint(float(delay) / dt))
+        steps = torch.full((n_links,), value, dtype=torch.int64, device=device)
+    steps = steps.clamp(min=1)
+    if n_links and int(steps.max()) > MAX_DELAY_STEPS:
         raise ValueError(f"a delay of {int(steps.max())} steps exceeds {MAX_DELAY_STEPS}")
     return steps
 
 
-def pack_links(index: np.ndarray, steps: np.ndarray) -> np.ndarray:
-    """(delay_steps << 24) | index as uint32."""
-    if len(index) and (index.min() < 0 or index.max() >= MAX_INDEX):
+def pack_links(index: torch.Tensor, steps: torch.Tensor) -> torch.Tensor:
+    """(delay_steps << 24) | index as int32 holding the uint32 bit pattern."""
+    if index.numel() and (int(index.min()) < 0 or int(index.max()) >= MAX_INDEX):
         raise ValueError("a link index outside [0, 2^24)")
-    return ((steps.astype(np.uint32) << np.uint32(24)) | index.astype(np.uint32)).astype(np.uint32)
+    word = (steps.to(torch.int64) << 24) | index.to(torch.int64)
+    return torch.where(word >= 2 ** 31, word - 2 ** 32, word).to(torch.int32)
 
 
-def push_form(topo: Topology, steps: np.ndarray, n_tgt: int):
-    """(ptr int32 [n_src + 1], link uint32 [n_links], perm int64 [n_links], split int32 [n_src]): rows per source,
-    each row's delay-1 links first (stable: canonical order otherwise); perm[k] is the canonical link at position
-    k; split[s] is row s's first link of delay >= 2 (the rest of the row is delivered one launch later)."""
-    tgt = topo.target_indices.numpy()
-    if len(tgt) and (tgt.min() < 0 or tgt.max() >= n_tgt):
+def _rows(off: torch.Tensor) -> torch.Tensor:
+    """The source row of every link of a CSR with offsets `off`."""
+    return torch.repeat_interleave(torch.arange(len(off) - 1, device=off.device), off.diff())
+
+
+def push_form(topo: Topology, steps: torch.Tensor, n_tgt: int):
+    """(ptr int32 [n_src + 1], link int32 [n_links], perm int64 [n_links], split int32 [n_src]): rows per
+    source, each row's delay-1 links first (stable: canonical order otherwise); perm[k] is the canonical link
+    at position k; split[s] is row s's first link of delay >= 2 (the rest of the row is delivered one launch
+    later). Computed on the topology's device."""
+    tgt = topo.target_indices
+    off = topo.source_offsets.to(tgt.device)
+    if tgt.numel() and (int(tgt.min()) < 0 or int(tgt.max()) >= n_tgt):
         raise ValueError("a link targets a neuron outside the target population")
-    off = topo.source_offsets.numpy()
-    n_src = len(off) - 1
+    steps = steps.to(tgt.device)
     far = steps >= 2
-    near_per_row = np.bincount(np.repeat(np.arange(n_src), np.diff(off)), weights=~far, minlength=n_src) \
-        if len(tgt) else np.zeros(n_src)
-    if far.all() or not len(tgt):
-        perm = np.arange(len(tgt), dtype=np.int64)
+    n_src = len(off) - 1
+    if not tgt.numel():
+        perm = torch.zeros(0, dtype=torch.int64, device=tgt.device)
+        split = off[:-1].to(torch.int32)
     else:
-        row = np.repeat(np.arange(n_src, dtype=np.int64), np.diff(off))
-        perm = np.argsort(row * 2 + far, kind="stable")
-    split = (off[:-1] + near_per_row.astype(np.int64)).astype(np.int32)
-    return off.astype(np.int32), pack_links(tgt[perm], steps[perm]), perm, split
+        row = _rows(off)
+        near_per_row = torch.bincount(row, weights=(~far).to(torch.float64), minlength=n_src).to(torch.int64)
+        split = (off[:-1] + near_per_row).to(torch.int32)
+        perm = torch.arange(tgt.numel(), device=tgt.device) if bool(far.all()) else \
+            torch.argsort(row * 2 + far.to(torch.int64), stable=True)
+    return off.to(torch.int32), pack_links(tgt[perm], steps[perm]), perm, split
 
 
-def pull_form(topo: Topology, steps: np.ndarray, n_tgt: int):
-    """(ptr int32 [n_tgt + 1], link uint32 [n_links], perm int64 [n_links]): the links sorted by target
-    (stable: canonical order within a target); perm[k] is the canonical link at pull position k."""
-    off = topo.source_offsets.numpy()
-    tgt = topo.target_indices.numpy()
-    src = np.repeat(np.arange(len(off) - 1, dtype=np.int64), np.diff(off))
-    perm = np.argsort(tgt, kind="stable")
-    counts = np.bincount(tgt, minlength=n_tgt) if len(tgt) else np.zeros(n_tgt, dtype=np.int64)
-    ptr = np.zeros(n_tgt + 1, dtype=np.int64)
-    ptr[1:] = np.cumsum(counts)
-    return ptr.astype(np.int32), pack_links(src[perm], steps[perm]), perm
+def pull_form(topo: Topology, steps: torch.Tensor, n_tgt: int):
+    """(ptr int32 [n_tgt + 1], link int32 [n_links], perm int64 [n_links]): the links sorted by target (stable:
+    canonical order within a target); perm[k] is the canonical link at pull position k."""
+    tgt = topo.target_indices
+    off = topo.source_offsets.to(tgt.device)
+    steps = steps.to(tgt.device)
+    src = _rows(off)
+    perm = torch.argsort(tgt, stable=True)
+    counts = torch.bincount(tgt, minlength=n_tgt) if tgt.numel() else torch.zeros(n_tgt, dtype=torch.int64,
+                                                                                  device=tgt.device)
+    ptr = torch.zeros(n_tgt + 1, dtype=torch.int64, device=tgt.device)
+    ptr[1:] = torch.cumsum(counts, 0)
+    return ptr.to(torch.int32), pack_links(src[perm], steps[perm]), perm

@@ -147,12 +147,13 @@ def run(desc, states: list, step0: int, n_steps: int, record: bool = True, ext_c
     conns = (OrConn * max(len(desc.conns), 1))()
     for k, c in enumerate(desc.conns):
         oc = conns[k]
-        ptr = np.ascontiguousarray(c.push_ptr, dtype=np.int32)
-        link = np.ascontiguousarray(c.push_link, dtype=np.uint32)
+        ptr, link, w = c.canonical()  # rows per source, canonical order
+        ptr = np.ascontiguousarray(ptr, dtype=np.int32)
+        link = np.ascontiguousarray(link, dtype=np.uint32)
         keep += [ptr, link]
         oc.src, oc.tgt, oc.ptr, oc.link = c.src, c.tgt, _ptr(ptr), _ptr(link)
-        if c.push_w is not None:
-            w = np.ascontiguousarray(c.push_w, dtype=np.float32)
+        if w is not None:
+            w = np.ascontiguousarray(w, dtype=np.float32)
             keep.append(w)
             oc.w = _ptr(w)
         oc.weight = c.weight

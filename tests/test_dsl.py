@@ -172,18 +172,19 @@ def test_region_types():
 def test_push_and_pull_forms():
     topo = Topology(torch.tensor([0, 3, 5, 5]), torch.tensor([2, 0, 1, 2, 0]))
     steps = np.array([3, 1, 2, 1, 4])
-    ptr, link, perm, split = push_form(topo, steps, 3)
+    ptr, link, perm, split = push_form(topo, torch.from_numpy(steps), 3)
     assert ptr.tolist() == [0, 3, 5, 5]
-    d, t = (link >> 24).tolist(), (link & 0xFFFFFF).tolist()
+    word = link.to(torch.int64) & 0xFFFFFFFF
+    d, t = (word >> 24).tolist(), (word & 0xFFFFFF).tolist()
     assert d == [1, 3, 2, 1, 4] and t == [0, 2, 1, 2, 0]  # delay-1 links first within each row
     assert split.tolist() == [1, 4, 5]
     assert perm.tolist() == [1, 0, 2, 3, 4]
-    pptr, plink, pperm = pull_form(topo, steps, 3)
+    pptr, plink, pperm = pull_form(topo, torch.from_numpy(steps), 3)
     assert pptr.tolist() == [0, 2, 3, 5]
     assert (plink & 0xFFFFFF).tolist() == [0, 1, 0, 0, 1]  # sources, target order, canonical order within
     assert pperm.tolist() == [1, 4, 2, 0, 3]
     with pytest.raises(ValueError):
-        push_form(topo, steps, 2)  # a target outside the population
+        push_form(topo, torch.from_numpy(steps), 2)  # a target outside the population
 
 
 def test_describe_brunel():
@@ -197,7 +198,7 @@ def test_describe_brunel():
     assert [c.mode for c in d.conns] == ["push"] * 4
     assert all(c.w is None for c in d.conns)  # single-weight connections carry no weight array
     assert d.n_links == 1000 * 100
-    assert all((c.split == c.ptr[:-1]).all() for c in d.conns)  # delay 15: no delay-1 link
+    assert all(torch.equal(c.split, c.ptr[:-1]) for c in d.conns)  # delay 15: no delay-1 link
 
 
 def test_describe_pd14_and_sources():
@@ -214,7 +215,7 @@ def test_describe_pd14_and_sources():
     assert pa.p[0] == float(np.float32(P_V)) and pa.p[3] == -65.0
     assert ps.fire_threshold == int(math.floor((1 - math.exp(-0.005)) * 2 ** 32))
     assert d.conns[0].w is not None and len(d.conns[0].w) == 500
-    w = c.fabric.value("weight").numpy()
+    w = c.fabric.value("weight").numpy()  # (describe's weights: the same values, as a tensor)
     tgt = c.fabric.topology.target_indices.numpy()
     max_in = np.bincount(tgt, weights=np.abs(w.astype(np.float64)), minlength=50).max()
     assert pa.shift == fixed_shift(max_in + 0.08781 * (len(pa.ext_table) - 1))

@@ -15,7 +15,9 @@ import oracle
 from naer2_b200 import philox as host_philox
 from naer2_b200.poisson import cdf_table, count
 from naer2_b200.runtime import ConnDesc, NetDesc, PopDesc, fixed_shift, wfx
-from naer2_b200.topology import pack_links
+import torch
+
+from naer2_b200.topology import Topology, pack_links
 
 GOLDEN = pathlib.Path(__file__).resolve().parent / "golden"
 
@@ -67,7 +69,8 @@ def test_fixed_point_weights():
 
 
 def brunel_golden_desc(g):
-    """The fixture's network as one population (the reference's own layout): LIF, one push connection."""
+    """The fixture's network as one population (the reference's own layout): LIF, one push connection with
+    per-link weights (J for excitatory sources, -gJ for inhibitory ones) and the fixture's one delay."""
     src = g["src"].astype(np.int64)
     N, K = src.shape
     NE = int(g["NE"])
@@ -78,15 +81,18 @@ def brunel_golden_desc(g):
     order = np.argsort(s, kind="stable")
     ptr = np.zeros(N + 1, np.int64)
     ptr[1:] = np.cumsum(np.bincount(s, minlength=N))
-    link = pack_links(tgt[order], np.full(len(s), int(g["delay_steps"])))
+    topo = Topology(torch.from_numpy(ptr), torch.from_numpy(tgt[order]))
+    steps = torch.full((len(s),), int(g["delay_steps"]), dtype=torch.int64)
+    warr = torch.from_numpy(w[order])
     table = g["table"]
     insum = np.bincount(tgt, weights=np.abs(w.astype(np.float64)), minlength=N).max()
     sh = fixed_shift(insum + J * (len(table) - 1))
     pop = PopDesc(model=1, n=N, acc_depth=16, bit_depth=0, shift=sh, ref_steps=20, fire_threshold=0,
                   seed=int(g["seed"]), p=[float(np.float32(math.exp(-0.1 / 20))), 20.0, 10.0] + [0.0] * 5,
                   ext_table=table, ext_weight=J, ext_wfx=wfx(J, sh), state={})
-    conn = ConnDesc(src=0, tgt=0, mode="push", n_links=len(s), ptr=ptr.astype(np.int32), link=link, weight=0.0,
-                    w=w[order], push_ptr=ptr.astype(np.int32), push_link=link, push_w=w[order])
+    conn = ConnDesc(src=0, tgt=0, mode="push", n_links=len(s), ptr=topo.source_offsets.to(torch.int32),
+                    link=pack_links(topo.target_indices, steps), weight=0.0, w=warr, split=None, topo=topo,
+                    steps=steps, warr=warr)
     return NetDesc(dt=0.1, pops=[pop], conns=[conn], n_links=len(s))
 
 

@@ -91,9 +91,9 @@ def test_reference_brunel_fixture_through_c_abi(cuda):
     words = (N + 31) // 32
     raster = torch.zeros(steps * words, dtype=torch.int32, device=dev)
     table = torch.from_numpy(d.ext_table.view(np.int32).copy()).to(dev)
-    ptr = torch.from_numpy(c.ptr).to(dev)
-    link = torch.from_numpy(c.link.view(np.int32).copy()).to(dev)
-    w = torch.from_numpy(c.w).to(dev)
+    ptr = c.ptr.to(dev)
+    link = c.link.to(dev)
+    w = c.w.to(dev)
     P = (_lib.Population * 1)()
     p = P[0]
     p.model, p.n, p.acc_depth, p.shift, p.ref_steps = _lib.MODEL_LIF_DELTA, N, d.acc_depth, d.shift, d.ref_steps
@@ -276,3 +276,25 @@ def test_grid_size_does_not_change_results(cuda, grid, persistent):
         assert np.array_equal(a.runtime.raster(pa), b.runtime.raster(pb))
         assert torch.equal(pa.V, pb.V)
     assert a.counters()["events"] == b.counters()["events"]
+
+
+def test_pd14_builder_scaled_matches_oracle(cuda):
+    """The config-2 builder (explicit Poisson background, per-link normal weights and delays) at 2% size."""
+    from naer2_b200.networks import pd14
+
+    net, pops = pd14.build(scale=0.02, seed=3)
+    gr, orr, gs, os_, cnt, ev = run_both(net, 600, chunk=250)
+    assert sum(r.sum() for r in gr) > 1000
+    assert_identical(gr, orr, gs, os_)
+    assert cnt["events"] == ev
+
+
+def test_pd14_drawn_on_the_gpu_matches_oracle(cuda):
+    """Connectivity, weights and delays drawn on the device (the full-size path), checked at 2% size."""
+    from naer2_b200.networks import pd14
+
+    net, pops = pd14.build(scale=0.02, seed=4, device=cuda)
+    assert net.connections[0].fabric.topology.target_indices.is_cuda
+    gr, orr, gs, os_, cnt, ev = run_both(net, 400)
+    assert_identical(gr, orr, gs, os_)
+    assert cnt["events"] == ev
