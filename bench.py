@@ -255,6 +255,88 @@ def run_pd14(args, dev) -> dict:
             "events_per_sim_step": ev_step, "build_s": build_s, "clocks": clocks.summary()}
 
 
+def run_batched(args, dev) -> dict:
+    """Config 3: B uneven Brunel instances in one network (one persistent launch per window), tuned by the
+    autotuner, against the same instances stepped one network at a time on the same GPU (same seeds: the same
+    spikes). Aggregate synaptic events/s of both, and per-instance rates."""
+    import torch
+
+    from naer2_b200.networks import batched
+    from naer2_b200.tune import autotune
+
+    B = args.instances
+    sim = SIM_STEPS_PER_STEP
+
+    def timed(net, n_steps):
+        rt = net.runtime
+        c0 = rt.counters()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        rt._enter()
+        e0.record(rt.stream)
+        net.run_steps(n_steps)
+        e1.record(rt.stream)
+        e1.synchronize()
+        c1 = rt.counters()
+        net.check()
+        return e0.elapsed_time(e1), c1["events"] - c0["events"], [b - a for a, b in zip(c0["per_population"],
+                                                                                      c1["per_population"])]
+
+    t0 = time.perf_counter()
+    net, parts = batched.build(B, seed=1, device=dev)
+    build_s = time.perf_counter() - t0
+    report = autotune(net, steps=200, warmup=50) if args.tune else None
+    net.run_steps(args.warmup * sim)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    ms_b, ev_b, spk_b = 0.0, 0, None
+    for _ in range(args.steps):
+        flush.zero_()
+        ms, ev, spk = timed(net, sim)
+        ms_b, ev_b = ms_b + ms, ev_b + ev
+        spk_b = spk if spk_b is None else [x + y for x, y in zip(spk_b, spk)]
+    n_links = net.runtime.n_links
+    neurons = sum(len(p.shape) for p in net.populations)
+    chosen = dict(block=net.block, grid=net.grid, persistent=net.persistent, tuned=dict(net.tuned))
+    net.close()
+    del net, parts
+    torch.cuda.empty_cache()
+    # the same instances, one network at a time, the tuned configuration
+    ms_p, ev_p, spk_p = 0.0, 0, []
+    for b in range(B):
+        inst, _ = batched.build_instance(b, seed=1, device=dev)
+        inst.block, inst.grid, inst.persistent = chosen["block"], None, chosen["persistent"]
+        inst.run_steps(args.warmup * sim)
+        for _ in range(args.steps):
+            flush.zero_()
+            ms, ev, spk = timed(inst, sim)
+            ms_p, ev_p = ms_p + ms, ev_p + ev
+            if len(spk_p) < 2 * (b + 1):
+                spk_p += spk
+            else:
+                spk_p[-2:] = [x + y for x, y in zip(spk_p[-2:], spk)]
+        inst.close()
+    steps = args.steps * sim
+    rates_b, rates_p = [], []
+    for b in range(B):
+        n_e = batched.instance_params(b, 1)["NE"]
+        n_i = batched.instance_params(b, 1)["NI"]
+        rates_b.append([spk_b[2 * b] / n_e / (steps * 1e-4), spk_b[2 * b + 1] / n_i / (steps * 1e-4)])
+        rates_p.append([spk_p[2 * b] / n_e / (steps * 1e-4), spk_p[2 * b + 1] / n_i / (steps * 1e-4)])
+    value = ev_b / (ms_b / 1e3)
+    plain = ev_p / (ms_p / 1e3)
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_b / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded draws on the GPU, 64 uneven Brunel instances)",
+            "config": {"workload": "batched_config3", "instances": B, "neurons": neurons, "synapses": n_links,
+                       "dt_ms": 0.1, "sim_steps_per_step": sim, "tuned": {k: v for k, v in chosen.items()
+                                                                             if k != "tuned"}},
+            "plain_one_at_a_time": {"value": plain, "ms_per_step": ms_p / args.steps},
+            "batched_over_plain": value / plain,
+            "identical_spike_counts": spk_b == spk_p,
+            "rates_hz_first4": [[round(x, 2) for x in r] for r in rates_b[:4]],
+            "max_rate_difference_hz": max(abs(x - y) for rb, rp in zip(rates_b, rates_p) for x, y in zip(rb, rp)),
+            "tune": report["trials"] if report else None, "build_s": build_s}
+
+
 def main() -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -262,8 +344,11 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="naer2_b200", choices=["naer2_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", type=int, default=1, choices=[1, 2],
-                    help="1: Brunel model A at config 1's size (the default workload); 2: the PD14 microcircuit")
+    ap.add_argument("--config", type=int, default=1, choices=[1, 2, 3],
+                    help="1: Brunel model A at config 1's size (the default workload); 2: the PD14 microcircuit; "
+                         "3: 64 uneven Brunel instances batched against one at a time")
+    ap.add_argument("--instances", type=int, default=64, help="config 3: instances")
+    ap.add_argument("--tune", action="store_true", help="config 3: run the autotuner first")
     ap.add_argument("--scale", type=float, default=1.0, help="config 2: population sizes times this")
     ap.add_argument("--mode", choices=["persistent", "per-step"], default="persistent",
                     help="a window of steps per cooperative launch, or one launch per step")
@@ -292,10 +377,10 @@ def main() -> int:
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if args.config == 2:
+    if args.config in (2, 3):
         if world > 1:
-            raise SystemExit("config 2 runs on one GPU")
-        print(json.dumps(run_pd14(args, dev)))
+            raise SystemExit(f"config {args.config} runs on one GPU")
+        print(json.dumps(run_pd14(args, dev) if args.config == 2 else run_batched(args, dev)))
         return 0
     if world > 1:
         import datetime

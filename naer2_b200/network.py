@@ -31,7 +31,8 @@ class Network:
         self.persistent: bool = True
         self.device = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else None
         self.record_steps: int = 0  # raster rows kept per population (Network.record)
-        self.tuned: dict = {}  # per connection id: the push/pull choice the tuner measured (runtime.tune)
+        self.tuned: dict = {}  # per connection id: the push/pull choice the tuner measured (naer2_b200.tune)
+        self.tune_report: dict | None = None
         self._runtime = None
 
     # ------------------------------------------------------------------ structure

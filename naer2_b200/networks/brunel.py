@@ -26,8 +26,10 @@ CONFIG1 = dict(NE=10000, NI=2500, CE=1000, CI=250, delay="uniform", max_delay_st
 
 def build(NE: int = 800, NI: int = 200, CE: int = 80, CI: int = 20, J: float = 0.1, g: float = 5.0,
           eta: float = 2.0, delay="uniform", max_delay_steps: int = 20, tau: float = 20.0, theta: float = 20.0,
-          V_r: float = 10.0, t_ref: float = 2.0, dt: float = 0.1, seed: int = 0, group_size: int = 256):
-    """(network, {"E": E, "I": I}) of Brunel's model A at step dt."""
+          V_r: float = 10.0, t_ref: float = 2.0, dt: float = 0.1, seed: int = 0, group_size: int = 256,
+          device=None):
+    """(network, {"E": E, "I": I}) of Brunel's model A at step dt. device: draw the connectivity and delays there
+    (CUDA: torch's generator, fast at large sizes; default: numpy's Philox on the host)."""
     nu_thr = theta / (J * CE * tau)
     ext_rate = CE * eta * nu_thr  # external events per ms into each neuron
     E = LIF(tau=tau, theta=theta, V_r=V_r, t_ref=t_ref, ext_rate=ext_rate, ext_weight=J) * NE
@@ -40,11 +42,16 @@ def build(NE: int = 800, NI: int = 200, CE: int = 80, CI: int = 20, J: float = 0
     for tgt in (E, I):
         for src, C, w in ((E, CE, J), (I, CI, -g * J)):
             k += 1
-            conn = src >> fixed_indegree(C, autapses=False, seed=(seed << 8) | (16 + k)) >> tgt
+            conn = src >> fixed_indegree(C, autapses=False, seed=(seed << 8) | (16 + k), device=device) >> tgt
             conn.weight = w
             if delay == "uniform":
-                steps = philox.generator((seed << 8) | (32 + k)).integers(1, max_delay_steps + 1, conn.shape[0])
-                conn.delay = torch.from_numpy((steps * dt).astype(np.float32))
+                if device is not None and torch.device(device).type == "cuda":
+                    gen = torch.Generator(device=device).manual_seed((seed << 8) | (32 + k))
+                    steps_t = torch.randint(1, max_delay_steps + 1, (conn.shape[0],), generator=gen, device=device)
+                    conn.delay = (steps_t * dt).to(torch.float32)
+                else:
+                    steps = philox.generator((seed << 8) | (32 + k)).integers(1, max_delay_steps + 1, conn.shape[0])
+                    conn.delay = torch.from_numpy((steps * dt).astype(np.float32))
             else:
                 conn.delay = float(delay)
     net = E.network

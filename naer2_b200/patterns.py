@@ -50,10 +50,11 @@ class fixed_indegree(_Drawn):
     neuron drawing itself where source and target are one population (the reference's Brunel_indegree,
     test/networks/Brunel/connection.py:8-33, keeps autapses). Rows ordered by target."""
 
-    def __init__(self, K: int, autapses: bool = True, seed: int | None = None):
+    def __init__(self, K: int, autapses: bool = True, seed: int | None = None, device=None):
         self.K = int(K)
         self.autapses = autapses
         self.seed = next(_SEEDS) if seed is None else int(seed)
+        self.device = torch.device(device) if device is not None else None  # draw there (torch's Philox)
         self._cache = None
 
     def links(self, n_src: int, n_tgt: int, same: bool = False):
@@ -62,6 +63,17 @@ class fixed_indegree(_Drawn):
             return np.zeros(n_src + 1, dtype=np.int64), np.zeros(0, dtype=np.int64)
         if n_src - exclude <= 0:
             raise ValueError("no source to draw from")
+        if self.device is not None and self.device.type == "cuda":
+            dev = self.device
+            g = torch.Generator(device=dev).manual_seed(self.seed)
+            tgt_t = torch.arange(n_tgt, dtype=torch.int64, device=dev).repeat_interleave(self.K)
+            src_t = torch.randint(0, n_src - (1 if exclude else 0), (n_tgt * self.K,), generator=g, device=dev)
+            if exclude:
+                src_t += (src_t >= tgt_t).to(torch.int64)
+            order = torch.argsort(src_t, stable=True)
+            off = torch.zeros(n_src + 1, dtype=torch.int64, device=dev)
+            off[1:] = torch.cumsum(torch.bincount(src_t, minlength=n_src), 0)
+            return off, tgt_t[order]
         tgt = np.repeat(np.arange(n_tgt, dtype=np.int64), self.K)
         src = philox.generator(self.seed).integers(0, n_src - (1 if exclude else 0), n_tgt * self.K, dtype=np.int64)
         if exclude:
