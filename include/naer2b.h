@@ -6,7 +6,8 @@
  * Plain C: pointers, sizes and integers only. PyTorch (or any caller) owns
  * every device buffer; the library borrows the pointers for the lifetime of
  * a handle and allocates no device memory of its own (its tables live in the
- * caller's workspace, n2b_workspace_bytes). One handle = one network on one
+ * caller's workspace, n2b_workspace_bytes; n2b_run_static uses a fixed array
+ * inside the library instead). One handle = one network on one
  * device; calls on one handle are not thread-safe and must be serialised by
  * the caller; the work runs on the stream passed to each call.
  *
@@ -175,6 +176,36 @@ int n2b_reset_counters(n2b_net *net, void *stream);
 
 /* Release the handle (its graph; the caller's buffers stay the caller's). */
 int n2b_destroy(n2b_net *net);
+
+/* Size of the library's own device scratch used by n2b_run_static. */
+#define N2B_STATIC_SCRATCH_BYTES ((size_t)32 << 20)
+
+/* No counterpart in the reference: an addition of this library for callers
+ * that cannot allocate device memory -- a host engine that reserves all of a
+ * GPU's memory for its own pool up front (a cudaMalloc would fail or escape
+ * its accounting), or code that must not call cudaMalloc / cudaFree because
+ * they synchronise the whole device. It runs n_steps steps of the network
+ * from step step0 (the step index the Poisson draws use), exactly as
+ * n2b_create + n2b_set_step + n2b_record(step0) + n2b_step would on a
+ * workspace, but with the workspace held in a file-scope device array of
+ * N2B_STATIC_SCRATCH_BYTES bytes inside this library; it allocates no device
+ * memory. The caller passes every input and output buffer, as for
+ * n2b_create. The far links of the call's last step are delivered into the
+ * arrival slots before the call's work ends, so a later call from step
+ * step0 + n_steps continues the run exactly. If `status` is not NULL, the call
+ * waits for its work on `stream` and copies the N2B_ERR_WORDS error words
+ * there.
+ *
+ * Limits: a network whose workspace (n2b_workspace_bytes) exceeds
+ * N2B_STATIC_SCRATCH_BYTES is rejected with N2B_ESPACE. Every device that
+ * loads this library holds the array until the process exits. The first call
+ * on a device looks the array's address up (with that device current); make
+ * that first call before any stream capture. Every call on a device shares
+ * the one array, and each call starts by resetting the counts, error words
+ * and barrier in it: two calls whose work overlaps on the GPU (different
+ * streams, or threads) race and corrupt each other. */
+int n2b_run_static(const n2b_population *pops, int32_t n_pops, const n2b_connection *conns, int32_t n_conns,
+                   const n2b_options *opt, int64_t step0, int64_t n_steps, int32_t *status, void *stream);
 
 #ifdef __cplusplus
 }

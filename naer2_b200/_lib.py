@@ -13,6 +13,7 @@ ABI_VERSION = 1
 MODEL_LIF_DELTA, MODEL_PD14, MODEL_POISSON_SOURCE = 1, 2, 3
 PUSH, PULL = 0, 1
 ERR_PUSH_LINK, ERR_PULL_LINK, ERR_SPLIT, ERR_ITEMS, ERR_BARRIER, ERR_WORDS = 0, 1, 2, 3, 4, 8
+STATIC_SCRATCH_BYTES = 32 << 20  # N2B_STATIC_SCRATCH_BYTES: the workspace limit of n2b_run_static
 
 
 class Population(ctypes.Structure):
@@ -59,6 +60,9 @@ SIGNATURES = {
     "n2b_counters": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int32, _P]),
     "n2b_reset_counters": (ctypes.c_int, [_P, _P]),
     "n2b_destroy": (ctypes.c_int, [_P]),
+    "n2b_run_static": (ctypes.c_int, [ctypes.POINTER(Population), ctypes.c_int32, ctypes.POINTER(Connection),
+                                      ctypes.c_int32, ctypes.POINTER(Options), ctypes.c_int64, ctypes.c_int64,
+                                      ctypes.POINTER(ctypes.c_int32), _P]),
 }
 
 _lib = None

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -516,3 +517,97 @@ int n2b_destroy(n2b_net *net) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------------------------
+// n2b_run_static: the same step kernels with their workspace in a fixed device array of this library, for callers
+// that cannot allocate device memory (an engine whose own pool holds the GPU's memory, code that must not take
+// the device-wide synchronisation of cudaMalloc / cudaFree). The array is the one workspace of every such call on
+// a device; each call resets what must start at zero (item counts, error words, counters, barrier) through
+// n2b_create's initialisation, so calls whose work overlaps on the GPU race.
+
+static __device__ __align__(256) unsigned char g_static_scratch[N2B_STATIC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int STATIC_MAX_DEVICES = 64;
+std::mutex g_static_mu;
+void *g_static_ptr[STATIC_MAX_DEVICES] = {};
+
+// The array's device address on `device` (which must be current): looked up once per device, on its first call.
+int static_scratch(int device, void **out) {
+    if (device < 0 || device >= STATIC_MAX_DEVICES) return fail(N2B_EINVAL, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_ptr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_static_scratch)");
+        if (!p || (reinterpret_cast<uintptr_t>(p) & 255) != 0) return fail(N2B_ECUDA, "static scratch misaligned");
+        g_static_ptr[device] = p;
+    }
+    *out = g_static_ptr[device];
+    return N2B_OK;
+}
+
+// The far links of step n - 1 (the work list the step kernel of step n would deliver), with no neuron update:
+// what is left of a run that stops after step n - 1.
+template <int NPB, bool INL>
+__global__ void __launch_bounds__(NPB) drain_kernel(const __grid_constant__ n2b::StepArgs a) {
+    __shared__ n2b::SConn s_tab[n2b::SMEM_CONNS];
+    const n2b::SConn *s_conn = n2b::fill_conns<INL>(a, s_tab, a.n_push);
+    __syncthreads();
+    n2b::far_phase<NPB, INL>(a, *a.step, s_conn);
+}
+
+template <bool INL>
+cudaError_t launch_drain(n2b_net *net, cudaStream_t s) {
+    const int grid = std::max(net->grid, 1);
+    switch (net->block) {
+        case 64: drain_kernel<64, INL><<<grid, 64, 0, s>>>(net->args); break;
+        case 256: drain_kernel<256, INL><<<grid, 256, 0, s>>>(net->args); break;
+        default: drain_kernel<128, INL><<<grid, 128, 0, s>>>(net->args); break;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" int n2b_run_static(const n2b_population *pops, int32_t n_pops, const n2b_connection *conns,
+                              int32_t n_conns, const n2b_options *opt, int64_t step0, int64_t n_steps,
+                              int32_t *status, void *stream) {
+    if (step0 < 0) return fail(N2B_EINVAL, "step0 < 0");
+    if (n_steps < 0 || n_steps > (int64_t)1 << 30) return fail(N2B_EINVAL, "n_steps out of range");
+    size_t need = 0;
+    int rc = n2b_workspace_bytes(pops, n_pops, conns, n_conns, opt, &need);
+    if (rc) return rc;
+    if (need > N2B_STATIC_SCRATCH_BYTES)
+        return fail(N2B_ESPACE, "n2b_run_static: the network needs " + std::to_string(need) +
+                                    " bytes of workspace, the static scratch holds " +
+                                    std::to_string((size_t)N2B_STATIC_SCRATCH_BYTES) +
+                                    " (use n2b_create with a workspace of the caller's)");
+    const int device = opt ? opt->device : 0;
+    N2B_CUDA(cudaSetDevice(device));
+    void *ws = nullptr;
+    rc = static_scratch(device, &ws);
+    if (rc) return rc;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    n2b_net *net = nullptr;
+    rc = n2b_create(pops, n_pops, conns, n_conns, opt, ws, N2B_STATIC_SCRATCH_BYTES, stream, &net);
+    if (rc) return rc;
+    rc = n2b_set_step(net, step0, stream);
+    if (!rc) rc = n2b_record(net, step0, stream);
+    if (!rc) rc = n2b_step(net, n_steps, stream);
+    if (!rc && n_steps > 0 && net->L.n_tiles > 0) {
+        cudaError_t e = net->inl ? launch_drain<true>(net, s) : launch_drain<false>(net, s);
+        if (e != cudaSuccess) rc = cuda_fail(e, "drain launch");
+    }
+    if (!rc && status) {
+        int32_t host[N2B_ERR_WORDS];
+        cudaError_t e = cudaMemcpyAsync(host, net->ws + net->L.err, sizeof(host), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = cuda_fail(e, "status copy");
+        else
+            for (int k = 0; k < N2B_ERR_WORDS; ++k) status[k] = host[k];
+    }
+    n2b_destroy(net);
+    return rc;
+}
