@@ -51,6 +51,60 @@ def measured_peaks() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
+_RED_PEAK = {}
+
+
+def l2_atomic_peak(dev) -> dict | None:
+    """Reductions/s of the L2 atomic units for the delivery's own instruction (red.global.add.u64 at random
+    slots of a 64 MiB array that stays in L2), measured here by naer2_b200/libn2b_peak.so: the best of 5 runs of
+    148 x 8 blocks x 256 threads x 256 reductions. Measured once per process."""
+    import ctypes
+
+    import torch
+
+    key = dev.index or 0
+    if key in _RED_PEAK:
+        return _RED_PEAK[key]
+    path = ROOT / "naer2_b200" / "libn2b_peak.so"
+    if not path.exists():
+        return None
+    lib = ctypes.CDLL(str(path))
+    lib.n2b_red_peak.restype = ctypes.c_int
+    lib.n2b_red_peak.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                 ctypes.c_void_p]
+    n_slots = 1 << 23
+    slots = torch.zeros(n_slots, dtype=torch.int64, device=dev)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    grid, block, ops = sms * 8, 256, 256
+    stream = torch.cuda.current_stream(dev)
+    best = None
+    for k in range(7):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        if lib.n2b_red_peak(ctypes.c_void_p(slots.data_ptr()), n_slots, grid, block, ops,
+                            ctypes.c_void_p(stream.cuda_stream)) != 0:
+            return None
+        e1.record(stream)
+        e1.synchronize()
+        if k >= 2:
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+    total = grid * block * ops
+    assert int(slots.sum()) == 7 * total  # every reduction landed
+    _RED_PEAK[key] = {"peak": total / (best / 1e3), "unit": "reductions/s",
+                      "probe": f"red.global.add.u64, {grid}x{block} threads x {ops}, 64 MiB L2-resident array"}
+    return _RED_PEAK[key]
+
+
+def l2_atomics(events_per_s: float, dev) -> dict | None:
+    """The step kernel's reduction rate (one red.global.add.u64 per synaptic event) against the measured peak."""
+    pk = l2_atomic_peak(dev)
+    if pk is None:
+        return None
+    return {"achieved": events_per_s, "peak": pk["peak"], "unit": pk["unit"], "frac": events_per_s / pk["peak"],
+            "peak_probe": pk["probe"]}
+
+
 def config(n_gpus: int) -> dict:
     return {"workload": WORKLOAD, "neurons": 12500, "synapses": 15_625_000, "delays_steps": "U{1..20}", "dt_ms": 0.1,
             "sim_steps_per_step": SIM_STEPS_PER_STEP, "l2": "flushed before every timed step (256 MiB write)",
@@ -250,6 +304,7 @@ def run_pd14(args, dev) -> dict:
             "roofline": {"bound": "hbm", "achieved": alg / (us * 1e-6) / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": alg / (us * 1e-6) / 1e9 / peak, "traffic": None, "peak_kind": kind,
                          "bytes_per_launch": alg, "us_per_launch": us},
+            "l2_atomics": l2_atomics(events / (dev_ms / 1e3), dev),
             "rates_hz": dict(zip(pd14.NAMES, [round(x, 3) for x in rates])),
             "cv_isi": dict(zip(pd14.NAMES, [round(x, 3) for x in cvs])),
             "events_per_sim_step": ev_step, "build_s": build_s, "clocks": clocks.summary()}
@@ -329,6 +384,7 @@ def run_batched(args, dev) -> dict:
             "config": {"workload": "batched_config3", "instances": B, "neurons": neurons, "synapses": n_links,
                        "dt_ms": 0.1, "sim_steps_per_step": sim, "tuned": {k: v for k, v in chosen.items()
                                                                              if k != "tuned"}},
+            "l2_atomics": l2_atomics(value, dev),
             "plain_one_at_a_time": {"value": plain, "ms_per_step": ms_p / args.steps},
             "batched_over_plain": value / plain,
             "identical_spike_counts": spk_b == spk_p,
@@ -487,6 +543,7 @@ def main() -> int:
                          "bytes_per_launch": alg_bytes, "us_per_launch": ms_per_launch * 1e3,
                          "note": "per simulation step: timed device time / steps (launch gaps and grid barriers "
                                  "included)"},
+            "l2_atomics": l2_atomics(events / (dev_ms / 1e3), dev),
             "gpu_launches": launches_all,
             "clocks": clocks.summary(),
             "events_per_sim_step": ev_per_launch,

@@ -90,6 +90,7 @@ struct StepArgs {
     unsigned long long *counters;
     int4 *items;           // 3 work lists of item_cap entries: (push connection, first link, end link, 0)
     int32_t *item_count;   // their lengths; step n appends to list n mod 3, reads n - 1's
+    int32_t *tile_claim;   // per step n mod 3: tiles past the first gridDim.x claimed so far
     unsigned *barrier;     // persistent kernel: the arrival counter, the abort word
     unsigned long long *trace;  // N2B_TRACE builds: per step and block, %globaltimer at each phase (else unused)
     int32_t trace_steps;
@@ -383,8 +384,16 @@ __device__ __forceinline__ float link_weight(const C_ &C, int l) {
     return C.homogeneous ? 0.f : __ldg(C.w + l);
 }
 
+// One synaptic event: a 64-bit reduction into an arrival slot, issued as a reduction (no value comes back).
+// No memory clobber: nothing in the step reads an arrival slot after adding to it before the step's barrier
+// (a grid barrier or the launch boundary), which orders the slot's reads.
+__device__ __forceinline__ void red_add_u64(long long *p, long long v) {
+    asm volatile("red.global.add.u64 [%0], %1;" ::"l"(p), "l"(v));
+}
+
 // One link word (and its weight) into the target's arrival slot (n + delay) mod D; out-of-range links
 // counted, not written.
+
 template <class C_>
 __device__ __forceinline__ void deliver_rec(const StepArgs &a, const C_ &C, uint32_t rec, float w, long long n,
                                             int min_delay) {
@@ -398,8 +407,7 @@ __device__ __forceinline__ void deliver_rec(const StepArgs &a, const C_ &C, uint
         return;
     }
     const long long wfx = C.homogeneous ? C.wfx : weight_fx(w, C.wscale);
-    atomicAdd(reinterpret_cast<unsigned long long *>(C.tgt_acc + (size_t)((n + d) & C.tgt_acc_mask) * (size_t)C.tgt_n + t),
-              (unsigned long long)wfx);
+    red_add_u64(C.tgt_acc + (size_t)((n + d) & C.tgt_acc_mask) * (size_t)C.tgt_n + t, wfx);
 }
 
 // Row bounds of neuron j in an outgoing push connection: first link, split, end.
@@ -675,7 +683,27 @@ __device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n,
     }
 }
 
-// 5. the far links of step n - 1: items of NPB links, one link per thread, two items at a time
+// Two items of step m's work list, one link of each per thread: both link loads in flight before the reductions.
+// it0 is a listed item; it1 is one only if `two` (otherwise it may be anything past the list's end, never
+// dereferenced: it is replaced by an empty item of connection 0 before its connection is looked up).
+template <bool INL>
+__device__ __forceinline__ void far_pair(const StepArgs &a, const SConn *s_conn, const int4 it0, const int4 it1_in,
+                                         const bool two, const long long m) {
+    const int4 it1 = two ? it1_in : make_int4(0, 0, 0, 0);
+    const int l0 = it0.y + (int)threadIdx.x, l1 = it1.y + (int)threadIdx.x;
+    const SConn C0 = conn_view(a, s_conn, it0.x);
+    const SConn C1 = conn_view(a, s_conn, it1.x);
+    const bool h0 = l0 < it0.z, h1 = two && l1 < it1.z;
+    const uint32_t rec0 = h0 ? __ldg(C0.link + l0) : 0u;
+    const uint32_t rec1 = h1 ? __ldg(C1.link + l1) : 0u;
+    const float w0 = h0 ? link_weight(C0, l0) : 0.f;
+    const float w1 = h1 ? link_weight(C1, l1) : 0.f;
+    if (h0) deliver_rec(a, C0, rec0, w0, m, 2);
+    if (h1) deliver_rec(a, C1, rec1, w1, m, 2);
+}
+
+// 5. the far links of step n - 1: items of NPB links, one link per thread, two items at a time, in a static
+// share per block (the next pair's items loaded under this pair's links)
 template <int NPB, bool INL>
 __device__ __forceinline__ void far_phase(const StepArgs &a, const long long n, const SConn *s_conn) {
     const long long m = n - 1;
@@ -692,25 +720,15 @@ __device__ __forceinline__ void far_phase(const StepArgs &a, const long long n, 
     int i = G - 1 - me;
     int4 pre0 = i < a.item_cap ? __ldcg(list + i) : make_int4(0, 0, 0, 0);
     int4 pre1 = i + G < a.item_cap ? __ldcg(list + i + G) : make_int4(0, 0, 0, 0);
-    const int count = min(__ldcg(a.item_count + lst), a.item_cap);
+    const int count = min(__ldcg(a.item_count + lst), a.item_cap);  // final: appended before the last barrier
     for (; i < count; i += 2 * G) {
-        const int4 it0 = pre0;
+        const int4 it0 = pre0, it1 = pre1;
         const bool two = i + G < count;
-        const int4 it1 = two ? pre1 : make_int4(0, 0, 0, 0);
         if (i + 2 * G < count) {
             pre0 = __ldcg(list + i + 2 * G);
             pre1 = i + 3 * G < count ? __ldcg(list + i + 3 * G) : make_int4(0, 0, 0, 0);
         }
-        const int l0 = it0.y + (int)threadIdx.x, l1 = it1.y + (int)threadIdx.x;
-        const SConn C0 = conn_view(a, s_conn, it0.x);
-        const SConn C1 = conn_view(a, s_conn, it1.x);
-        const bool h0 = l0 < it0.z, h1 = two && l1 < it1.z;
-        const uint32_t rec0 = h0 ? __ldg(C0.link + l0) : 0u;
-        const uint32_t rec1 = h1 ? __ldg(C1.link + l1) : 0u;
-        const float w0 = h0 ? link_weight(C0, l0) : 0.f;
-        const float w1 = h1 ? link_weight(C1, l1) : 0.f;
-        if (h0) deliver_rec(a, C0, rec0, w0, m, 2);
-        if (h1) deliver_rec(a, C1, rec1, w1, m, 2);
+        far_pair<INL>(a, s_conn, it0, it1, two, m);
     }
 }
 
@@ -719,15 +737,36 @@ __device__ __forceinline__ void step_body(const StepArgs &a, const long long n, 
                                           const int *s_cache, const SConn *s_conn) {
     __shared__ Scratch<NPB> sc;
     N2B_STAMP(a, k, 0);
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.item_count + (int)((n + 1) % 3), 0);  // step n + 1's list
-    int t = blockIdx.x;
-    if (cached != nullptr && t < a.n_tiles) {
-        tile_phase<NPB, INL, true>(a, n, tile_at<INL, NPB>(a, t), k, *cached, s_cache, sc, s_conn);
-        t += gridDim.x;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {  // step n + 1's list and tile counter
+        atomicExch(a.item_count + (int)((n + 1) % 3), 0);
+        atomicExch(a.tile_claim + (int)((n + 1) % 3), 0);
     }
+    // tile blockIdx.x first (a persistent launch holds it in registers); with fewer blocks than tiles, the
+    // tiles past the first gridDim.x are claimed one at a time from the step's counter, so that blocks whose
+    // tiles take longer (more spikes) take fewer of them. Thread 0's next claim is in flight under each tile.
+    const bool dyn = (int)gridDim.x < a.n_tiles;
+    int *claim = a.tile_claim + (int)(n % 3);
+    int next = 0;
+    if (dyn && threadIdx.x == 0) next = atomicAdd(claim, 1);
     Neuron nr;
-    for (; t < a.n_tiles; t += gridDim.x)
-        tile_phase<NPB, INL, false>(a, n, tile_at<INL, NPB>(a, t), k, nr, nullptr, sc, s_conn);
+    const int t = blockIdx.x;
+    if (t < a.n_tiles) {
+        if (cached != nullptr)
+            tile_phase<NPB, INL, true>(a, n, tile_at<INL, NPB>(a, t), k, *cached, s_cache, sc, s_conn);
+        else
+            tile_phase<NPB, INL, false>(a, n, tile_at<INL, NPB>(a, t), k, nr, nullptr, sc, s_conn);
+    }
+    if (dyn) {
+        __shared__ int s_tile;
+        for (;;) {
+            if (threadIdx.x == 0) s_tile = next;
+            __syncthreads();
+            const int u = (int)gridDim.x + s_tile;  // every thread reads it before the tile's first barrier
+            if (u >= a.n_tiles) break;
+            if (threadIdx.x == 0) next = atomicAdd(claim, 1);
+            tile_phase<NPB, INL, false>(a, n, tile_at<INL, NPB>(a, u), k, nr, nullptr, sc, s_conn);
+        }
+    }
     N2B_STAMP(a, k, 2);
     far_phase<NPB, INL>(a, n, s_conn);
     N2B_STAMP(a, k, 3);
@@ -828,7 +867,7 @@ __global__ void zero_kernel(int32_t *err, int n_err, unsigned long long *counter
 }
 __global__ void set_step_kernel(long long *step, long long value, int32_t *item_count) {
     *step = value;
-    item_count[0] = item_count[1] = item_count[2] = 0;
+    for (int k = 0; k < 6; ++k) item_count[k] = 0;  // the three list lengths and the three tile counters
 }
 
 }  // namespace n2b

@@ -72,7 +72,7 @@ Layout layout(const n2b_population *pops, int32_t n_pops, const n2b_connection *
     L.rec0 = o; o = align256(o + sizeof(long long));
     L.err = o; o = align256(o + sizeof(int32_t) * N2B_ERR_WORDS);
     L.counters = o; o = align256(o + sizeof(unsigned long long) * (2 + std::max(n_pops, 1)));
-    L.item_count = o; o = align256(o + sizeof(int32_t) * 3);
+    L.item_count = o; o = align256(o + sizeof(int32_t) * 6);  // three list lengths, three tile counters
     L.items = o; o = align256(o + sizeof(int4) * 3 * (size_t)L.item_cap);
     L.barrier = o; o = align256(o + sizeof(unsigned) * n2b::BAR_WORDS);
     L.total = o;
@@ -374,6 +374,7 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     a.counters = reinterpret_cast<unsigned long long *>(ws + L.counters);
     a.items = reinterpret_cast<int4 *>(ws + L.items);
     a.item_count = reinterpret_cast<int32_t *>(ws + L.item_count);
+    a.tile_claim = a.item_count + 3;
     a.item_cap = L.item_cap;
     a.n_tiles = L.n_tiles;
     a.offset = 0;
