@@ -177,6 +177,66 @@ int n2b_reset_counters(n2b_net *net, void *stream);
 /* Release the handle (its graph; the caller's buffers stay the caller's). */
 int n2b_destroy(n2b_net *net);
 
+/* ---- Surrogate-gradient BPTT of a recurrent LIF layer --------------------
+ * No counterpart in the reference (naer2 has no differentiable path): the
+ * layer of the BPTT workload, hand-written forward and adjoint kernels.
+ * Per sample and step t (dt = one step), hidden neuron i:
+ *   Vpre = alpha V + U[t] + sum_in(i) w_k s[t - d_k][pre_k]   (d_k 1..5 steps)
+ *   s    = Vpre >= theta (or, smooth, f(Vpre - theta), f(x) = x / (1 + slope |x|))
+ *   V    = Vpre - theta s;   O[t] = beta O[t-1] + s W_out;   m = max over t of O
+ * The backward uses g = 1 / (1 + slope |Vpre - theta|)^2 for ds/dVpre (the
+ * fast-sigmoid surrogate; the exact derivative of the smooth f), the reset
+ * included. The forward keeps the spikes of every step (one bit per neuron,
+ * sample and step) and the membrane every `checkpoint` steps; the backward
+ * recomputes each segment from its checkpoint, then runs it backwards over
+ * the transposed (outgoing) rows. */
+
+/* error words: 0 links with a bad code (skipped); 1 recomputed spikes that
+ * differ from the forward's; 2 in_cta_max / out_cta_max below the rows' counts */
+#define N2B_BPTT_ERR_WORDS 4
+
+typedef struct n2b_bptt_desc {
+    int32_t batch;       /* B, a multiple of 8 (8 samples per cluster of 8 CTAs) */
+    int32_t steps;       /* T */
+    int32_t hidden;      /* H, a multiple of 8, at most 2048 */
+    int32_t readouts;    /* R, at most 32 */
+    int32_t checkpoint;  /* K: membrane checkpoint every K steps */
+    int32_t smooth;      /* 1: the smooth forward (hidden <= 256), for gradient checks */
+    int32_t nnz;         /* recurrent links */
+    int32_t in_cta_max;  /* most incoming links of any eighth of the hidden neurons */
+    int32_t out_cta_max; /* most outgoing links of any eighth of the hidden neurons */
+    float alpha, beta, theta, slope;
+    const int32_t *in_ptr;    /* [H+1] incoming rows; the links' order is the weights' order */
+    const uint16_t *in_code;  /* [nnz] source | delay << 11 */
+    const int32_t *out_grp;   /* [H][6] outgoing rows: start of the delay-1..5 links, then the row end */
+    const uint16_t *out_code; /* [nnz] target | delay << 11, outgoing order */
+    const int32_t *out_perm;  /* [nnz] incoming-order index of each outgoing link */
+} n2b_bptt_desc;
+
+/* Device workspace bytes of the layer (spike tape, checkpoints, one segment's
+ * surrogate derivatives, per-cluster gradient partials). */
+int n2b_bptt_workspace_bytes(const n2b_bptt_desc *d, size_t *bytes);
+
+/* Forward over all steps: u [T][B][H] input current, w_rec [nnz] (incoming
+ * order), w_out [H][R]; writes m [B][R] (max over time of the readouts) and
+ * tstar [B][R] (its first step). tape = 1 keeps what the backward needs in
+ * the workspace; 0 is the plain forward. */
+int n2b_bptt_forward(const n2b_bptt_desc *d, const float *u, const float *w_rec, const float *w_out, int32_t tape,
+                     float *m, int32_t *tstar, void *workspace, size_t workspace_bytes, void *stream);
+
+/* Backward of the last taped forward: dm [B][R] = dL/dm, tstar as the forward
+ * wrote it; writes du [T][B][H] = dL/du, dw_rec [nnz], dw_out [H][R]. */
+int n2b_bptt_backward(const n2b_bptt_desc *d, const float *u, const float *w_rec, const float *w_out,
+                      const float *dm, const int32_t *tstar, float *du, float *dw_rec, float *dw_out,
+                      void *workspace, size_t workspace_bytes, void *stream);
+
+/* The N2B_BPTT_ERR_WORDS error words after the work on `stream` (a synchronisation). */
+int n2b_bptt_status(const n2b_bptt_desc *d, void *workspace, size_t workspace_bytes, int32_t *words, void *stream);
+
+/* Copy the taped spikes into out (device): [T][B/8][H] bytes, bit j = sample
+ * 8c + j of cluster c; smooth: [T][B/8][H][8] floats. */
+int n2b_bptt_spikes(const n2b_bptt_desc *d, void *workspace, size_t workspace_bytes, void *out, void *stream);
+
 /* Size of the library's own device scratch used by n2b_run_static. */
 #define N2B_STATIC_SCRATCH_BYTES ((size_t)32 << 20)
 

@@ -41,6 +41,20 @@ class Options(ctypes.Structure):
                 ("persistent", ctypes.c_int32)]
 
 
+BPTT_ERR_WORDS = 4  # N2B_BPTT_ERR_WORDS
+
+
+class BpttDesc(ctypes.Structure):
+    _fields_ = [
+        ("batch", ctypes.c_int32), ("steps", ctypes.c_int32), ("hidden", ctypes.c_int32),
+        ("readouts", ctypes.c_int32), ("checkpoint", ctypes.c_int32), ("smooth", ctypes.c_int32),
+        ("nnz", ctypes.c_int32), ("in_cta_max", ctypes.c_int32), ("out_cta_max", ctypes.c_int32),
+        ("alpha", ctypes.c_float), ("beta", ctypes.c_float), ("theta", ctypes.c_float), ("slope", ctypes.c_float),
+        ("in_ptr", ctypes.c_void_p), ("in_code", ctypes.c_void_p), ("out_grp", ctypes.c_void_p),
+        ("out_code", ctypes.c_void_p), ("out_perm", ctypes.c_void_p),
+    ]
+
+
 # every entry point include/naer2b.h declares: (name, restype, argtypes)
 _P = ctypes.c_void_p
 SIGNATURES = {
@@ -60,6 +74,14 @@ SIGNATURES = {
     "n2b_counters": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int32, _P]),
     "n2b_reset_counters": (ctypes.c_int, [_P, _P]),
     "n2b_destroy": (ctypes.c_int, [_P]),
+    "n2b_bptt_workspace_bytes": (ctypes.c_int, [ctypes.POINTER(BpttDesc), ctypes.POINTER(ctypes.c_size_t)]),
+    "n2b_bptt_forward": (ctypes.c_int, [ctypes.POINTER(BpttDesc), _P, _P, _P, ctypes.c_int32, _P, _P, _P,
+                                        ctypes.c_size_t, _P]),
+    "n2b_bptt_backward": (ctypes.c_int, [ctypes.POINTER(BpttDesc), _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                                         ctypes.c_size_t, _P]),
+    "n2b_bptt_status": (ctypes.c_int, [ctypes.POINTER(BpttDesc), _P, ctypes.c_size_t,
+                                       ctypes.POINTER(ctypes.c_int32), _P]),
+    "n2b_bptt_spikes": (ctypes.c_int, [ctypes.POINTER(BpttDesc), _P, ctypes.c_size_t, _P, _P]),
     "n2b_run_static": (ctypes.c_int, [ctypes.POINTER(Population), ctypes.c_int32, ctypes.POINTER(Connection),
                                       ctypes.c_int32, ctypes.POINTER(Options), ctypes.c_int64, ctypes.c_int64,
                                       ctypes.POINTER(ctypes.c_int32), _P]),

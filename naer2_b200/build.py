@@ -21,7 +21,7 @@ HERE = pathlib.Path(__file__).resolve().parent
 ROOT = HERE.parent
 CSRC = HERE / "csrc"
 LIB = HERE / "libnaer2b.so"
-SOURCES = [CSRC / "naer2b.cu"]
+SOURCES = [CSRC / "naer2b.cu", CSRC / "bptt.cu"]
 HEADERS = [CSRC / "n2b_device.cuh", ROOT / "include" / "naer2b.h"]
 PEAK_LIB = HERE / "libn2b_peak.so"
 PEAK_SOURCES = [CSRC / "l2_peak.cu"]

@@ -1,0 +1,782 @@
+// Surrogate-gradient BPTT of a recurrent LIF layer with delayed sparse recurrence (include/naer2b.h,
+// n2b_bptt_*). No counterpart in the reference: naer2 has no differentiable path.
+//
+// Model, per sample b, hidden neuron i, step t (dt = 1 step):
+//   R[t][i]     = sum over incoming links k of i: w_k * s[t - d_k][pre_k]          (d_k in 1..5 steps)
+//   Vpre[t][i]  = alpha * V[t-1][i] + U[t][i] + R[t][i]                             (U: input current)
+//   s[t][i]     = Vpre >= theta  (spiking)   |   f(Vpre - theta), f(x) = x / (1 + slope |x|)  (smooth)
+//   V[t][i]     = Vpre - theta * s[t][i]                                            (subtractive reset)
+//   O[t][r]     = beta * O[t-1][r] + sum_i w_out[i][r] * s[t][i];   m[r] = max_t O[t][r] at t*[r]
+// Backward (q = dL/dVpre, g = f'(Vpre - theta) = 1 / (1 + slope |Vpre - theta|)^2, the fast-sigmoid
+// surrogate in the spiking model, the true derivative in the smooth one; the reset is differentiated):
+//   o[t][r]  = dm[r] * [t == t*[r]] + beta * o[t+1][r]
+//   q[t][i]  = alpha q[t+1][i] + g[t][i] * (sum_{k out of i} w_k q[t + d_k][post_k]
+//                                           + sum_r w_out[i][r] o[t][r] - theta alpha q[t+1][i])
+//   dU[t][i] = q[t][i];  dw_k = sum_t,b s[t - d_k][pre_k] q[t][post_k];  dw_out[i][r] = sum_t,b s[t][i] o[t][r]
+//
+// Layout: a cluster of 8 CTAs runs 8 samples; CTA `rank` owns hidden neurons [rank*HC, rank*HC + HC), HC = H/8,
+// two threads per neuron (one per 4 samples; the link loops split a row between the two, interleaved).
+// Forward: every CTA keeps the spikes of the last 6 steps of all H neurons for its 8 samples (one byte of 8
+// sample bits per neuron, or 8 floats in the smooth model) in shared memory; each step a neuron's new entry
+// is written into all 8 CTAs' rings (distributed shared memory) before one cluster barrier. Backward: each
+// K-step segment is first recomputed from its membrane checkpoint and the stored spikes of every step
+// (same arithmetic, same order: the same Vpre bit for bit), then run backwards; q of all neurons is exchanged
+// the same way, and each neuron pushes its outgoing rows' q sums into a 6-slot ring of its own partials.
+// Every sum has a fixed order (no float atomics), so results are bit-for-bit reproducible.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <string>
+
+#include "../../include/naer2b.h"
+
+namespace cg = cooperative_groups;
+
+namespace n2b_bptt {
+
+constexpr int NS = 8;    // samples per cluster
+constexpr int CL = 8;    // CTAs per cluster
+constexpr int RING = 6;  // spike / partial ring slots (delays 1..5)
+constexpr int MAXD = 5;
+constexpr unsigned FULL = 0xffffffffu;
+
+struct Args {
+    int B, T, H, R, K, HC, NC, nseg, nnz;
+    float alpha, beta, theta, slope;
+    int tape, csr_smem;
+    const int32_t *in_ptr;
+    const uint16_t *in_code;
+    const float *in_w;
+    const int32_t *out_grp;  // [H][MAXD + 1]: row start of each delay 1..5, then the row end
+    const uint16_t *out_code;
+    const float *out_w;
+    const float *U;     // [T][B][H]
+    uint8_t *s_bits;    // [T][NC][H]      (spiking)
+    float *s_f;         // [T][NC][H][8]   (smooth)
+    float *v_ckpt;      // [nseg][B][H]
+    float *g_seg;       // [K][B][H]
+    float *dU;          // [T][B][H]
+    const float *w_out; // [H][R]
+    float *m;           // [B][R]
+    int32_t *tstar;     // [B][R]
+    const float *dm;    // [B][R]
+    const int32_t *tstar_in;
+    float *dwp;         // [NC][nnz] per-cluster dw, out order
+    float *dwo_p;       // [NC][H][R]
+    int32_t *err;       // [N2B_BPTT_ERR_WORDS]
+};
+
+__device__ __forceinline__ float surrogate(float x, float slope) {
+    const float a = __fadd_rn(1.f, __fmul_rn(slope, fabsf(x)));
+    return __fdiv_rn(1.f, __fmul_rn(a, a));
+}
+
+__device__ __forceinline__ float smooth_spike(float x, float slope) {
+    return __fdiv_rn(x, __fadd_rn(1.f, __fmul_rn(slope, fabsf(x))));
+}
+
+// Shared-memory layout of the forward kernel (identical in every CTA, so that remote addresses match).
+struct FwdSmem {
+    size_t ring, xbuf, wout, ptr, code, w, total;
+};
+__host__ __device__ inline FwdSmem fwd_smem(int H, int HC, int R, bool smooth, bool csr_smem, int in_cta_max) {
+    FwdSmem L{};
+    size_t o = 0;
+    auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };
+    L.ring = o; o = a16(o + (smooth ? sizeof(float) * RING * H * NS : (size_t)RING * H));
+    L.xbuf = o; o = a16(o + sizeof(float) * 2 * CL * NS * R);
+    L.wout = o; o = a16(o + sizeof(float) * HC * R);
+    L.ptr = o; o = a16(o + sizeof(int32_t) * (HC + 1));
+    L.code = o; o = a16(o + (csr_smem ? sizeof(uint16_t) * in_cta_max : 0));
+    L.w = o; o = a16(o + (csr_smem ? sizeof(float) * in_cta_max : 0));
+    L.total = o;
+    return L;
+}
+
+struct BwdSmem {
+    size_t pnew, part, ring, wout, dwo, obuf, grp, code, dw, total;
+};
+__host__ __device__ inline BwdSmem bwd_smem(int H, int HC, int R, bool smooth, int out_cta_max) {
+    BwdSmem L{};
+    size_t o = 0;
+    auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };
+    L.pnew = o; o = a16(o + sizeof(float) * 2 * H * NS);
+    L.part = o; o = a16(o + sizeof(float) * RING * HC * NS);
+    L.ring = o; o = a16(o + (smooth ? sizeof(float) * RING * H * NS : (size_t)RING * H));
+    L.wout = o; o = a16(o + sizeof(float) * HC * R);
+    L.dwo = o; o = a16(o + sizeof(float) * HC * R);
+    L.obuf = o; o = a16(o + sizeof(float) * NS * R);
+    L.grp = o; o = a16(o + sizeof(int32_t) * HC * (MAXD + 1));
+    L.code = o; o = a16(o + sizeof(uint16_t) * out_cta_max);
+    L.dw = o; o = a16(o + sizeof(float) * out_cta_max);
+    L.total = o;
+    return L;
+}
+
+// The spikes of neuron j at ring slot `slot`: 8 samples (bits, or floats in the smooth model).
+template <bool SMOOTH>
+__device__ __forceinline__ void load_spikes(const unsigned char *ring, int H, int slot, int j, float s[NS],
+                                            uint32_t &byte) {
+    if constexpr (SMOOTH) {
+        const float4 *p = reinterpret_cast<const float4 *>(ring) + ((size_t)slot * H + j) * 2;
+        const float4 a = p[0], b = p[1];
+        s[0] = a.x; s[1] = a.y; s[2] = a.z; s[3] = a.w;
+        s[4] = b.x; s[5] = b.y; s[6] = b.z; s[7] = b.w;
+        byte = 0xffu;  // every sample may contribute
+    } else {
+        (void)s;
+        byte = ring[(size_t)slot * H + j];
+    }
+}
+
+// R for the 8 samples of post `post`: this thread's half of its incoming row (links rs + half, rs + half + 2,
+// ...), then the two halves added (a + b in both lanes: the same value in each).
+template <bool SMOOTH>
+__device__ __forceinline__ void gather_in(const Args &a, const unsigned char *ring, const uint16_t *code,
+                                          const float *w, int rs, int re, int half, int t, float acc[NS]) {
+#pragma unroll
+    for (int b = 0; b < NS; ++b) acc[b] = 0.f;
+    for (int l = rs + half; l < re; l += 2) {
+        const uint32_t c = code[l];
+        const int pre = (int)(c & 0x7FFu), d = (int)(c >> 11);
+        if (d < 1 || d > MAXD || pre >= a.H) {
+            atomicAdd(a.err + 0, 1);
+            continue;
+        }
+        if (t - d < 0) continue;
+        float s[NS];
+        uint32_t byte;
+        load_spikes<SMOOTH>(ring, a.H, (t - d) % RING, pre, s, byte);
+        if (!byte) continue;
+        const float wl = w[l];
+        if constexpr (SMOOTH) {
+#pragma unroll
+            for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __fmul_rn(wl, s[b]));
+        } else {
+#pragma unroll
+            for (int b = 0; b < NS; ++b)
+                if ((byte >> b) & 1u) acc[b] = __fadd_rn(acc[b], wl);
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __shfl_xor_sync(FULL, acc[b], 1));
+}
+
+// One membrane step of one sample: returns the spike value, updates V (and gives Vpre).
+template <bool SMOOTH>
+__device__ __forceinline__ float lif_step(const Args &a, float &V, float u, float r, float &vpre) {
+    const float vp = __fadd_rn(__fadd_rn(__fmul_rn(a.alpha, V), u), r);
+    float s;
+    if constexpr (SMOOTH) s = smooth_spike(__fadd_rn(vp, -a.theta), a.slope);
+    else s = vp >= a.theta ? 1.f : 0.f;
+    V = __fadd_rn(vp, -__fmul_rn(a.theta, s));
+    vpre = vp;
+    return s;
+}
+
+// ------------------------------------------------------------------------------------------------ forward
+
+template <bool SMOOTH>
+__global__ void __launch_bounds__(512) fwd_kernel(const __grid_constant__ Args a, int in_cta_max) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    const int q = (int)blockIdx.x / CL;
+    const int H = a.H, HC = a.HC, R = a.R, B = a.B;
+    const int h0 = rank * HC;
+    const FwdSmem L = fwd_smem(H, HC, R, SMOOTH, a.csr_smem != 0, in_cta_max);
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned char *ring = smem + L.ring;
+    float *xbuf = reinterpret_cast<float *>(smem + L.xbuf);
+    float *wout = reinterpret_cast<float *>(smem + L.wout);
+    int32_t *lptr = reinterpret_cast<int32_t *>(smem + L.ptr);
+    const int tid = threadIdx.x, nthr = blockDim.x;
+
+    for (size_t k = tid; k < (L.xbuf - L.ring) / 4; k += nthr) reinterpret_cast<uint32_t *>(ring)[k] = 0u;
+    for (int k = tid; k < HC * R; k += nthr) wout[k] = a.w_out[(size_t)h0 * R + k];
+    const int base = a.in_ptr[h0];
+    for (int k = tid; k <= HC; k += nthr) lptr[k] = a.in_ptr[h0 + k] - base;
+    const uint16_t *code = a.in_code + base;
+    const float *wl = a.in_w + base;
+    const int n_in = a.in_ptr[h0 + HC] - base;
+    if (a.csr_smem && n_in > in_cta_max && tid == 0) atomicAdd(a.err + 2, 1);  // a wrong in_cta_max: rows stay global
+    if (a.csr_smem && n_in <= in_cta_max) {
+        uint16_t *sc = reinterpret_cast<uint16_t *>(smem + L.code);
+        float *sw = reinterpret_cast<float *>(smem + L.w);
+        for (int k = tid; k < n_in; k += nthr) {
+            sc[k] = code[k];
+            sw[k] = wl[k];
+        }
+        code = sc;
+        wl = sw;
+    }
+    __syncthreads();
+    cl.sync();  // every CTA's shared memory is initialised before any remote write reaches it
+
+    const bool nt = tid < 2 * HC;
+    const int pl = nt ? tid >> 1 : 0, half = tid & 1;
+    const int post = h0 + pl;
+    const int rs = nt ? lptr[pl] : 0, re = nt ? lptr[pl + 1] : 0;
+    float V[4] = {0.f, 0.f, 0.f, 0.f};
+    const bool ro = tid < NS * R;
+    const int rb = ro ? tid / R : 0, rr = ro ? tid % R : 0;
+    float O = 0.f, mx = -INFINITY;
+    int ts = -1;
+
+    for (int t = 0; t < a.T; ++t) {
+        if (a.tape && t % a.K == 0 && nt) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                a.v_ckpt[((size_t)(t / a.K) * B + q * NS + 4 * half + j) * H + post] = V[j];
+        }
+        float acc[NS];
+        gather_in<SMOOTH>(a, ring, code, wl, rs, re, half, t, acc);
+        float s4[4] = {0.f, 0.f, 0.f, 0.f};
+        uint32_t bits = 0;
+        if (nt) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int b = 4 * half + j;
+                const float u = __ldg(a.U + ((size_t)t * B + q * NS + b) * H + post);
+                float vp;
+                s4[j] = lif_step<SMOOTH>(a, V[j], u, half ? acc[4 + j] : acc[j], vp);
+                if (s4[j] != 0.f) bits |= 1u << j;
+            }
+        }
+        const uint32_t other = __shfl_xor_sync(FULL, bits, 1);
+        const int slot = t % RING;
+        if (nt) {
+            if constexpr (SMOOTH) {
+                const float4 v = make_float4(s4[0], s4[1], s4[2], s4[3]);
+                float4 *dst = reinterpret_cast<float4 *>(ring) + ((size_t)slot * H + post) * 2 + half;
+                for (int k = 0; k < CL; ++k) *cl.map_shared_rank(dst, k) = v;
+                if (a.tape)
+                    reinterpret_cast<float4 *>(a.s_f)[(((size_t)t * a.NC + q) * H + post) * 2 + half] = v;
+            } else {
+                const uint32_t byte = half ? (other | (bits << 4)) : (bits | (other << 4));
+                unsigned char *dst = ring + (size_t)slot * H + post;
+                for (int k = half; k < CL; k += 2) *cl.map_shared_rank(dst, k) = (unsigned char)byte;
+                if (a.tape && half == 0) a.s_bits[((size_t)t * a.NC + q) * H + post] = (uint8_t)byte;
+            }
+        }
+        __syncthreads();  // this CTA's own neurons' entries are in its ring
+        if (ro) {
+            float sum = 0.f;
+            for (int p = 0; p < HC; ++p) {
+                float s[NS];
+                uint32_t byte;
+                load_spikes<SMOOTH>(ring, H, slot, h0 + p, s, byte);
+                if constexpr (SMOOTH) sum = __fadd_rn(sum, __fmul_rn(s[rb], wout[p * R + rr]));
+                else if ((byte >> rb) & 1u) sum = __fadd_rn(sum, wout[p * R + rr]);
+            }
+            float *dst = xbuf + (((size_t)(t & 1) * CL + rank) * NS + rb) * R + rr;
+            *cl.map_shared_rank(dst, 0) = sum;
+        }
+        cl.sync();  // step t's spikes in every ring, its readout partials in rank 0
+        if (rank == 0 && ro) {
+            float tot = 0.f;
+            for (int k = 0; k < CL; ++k) tot = __fadd_rn(tot, xbuf[(((size_t)(t & 1) * CL + k) * NS + rb) * R + rr]);
+            O = __fadd_rn(__fmul_rn(a.beta, O), tot);
+            if (O > mx) {
+                mx = O;
+                ts = t;
+            }
+        }
+    }
+    if (rank == 0 && ro) {
+        a.m[(size_t)(q * NS + rb) * R + rr] = mx;
+        a.tstar[(size_t)(q * NS + rb) * R + rr] = ts;
+    }
+    cl.sync();  // no CTA leaves while another may still address its shared memory
+}
+
+// ------------------------------------------------------------------------------------------------ backward
+
+template <bool SMOOTH>
+__global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a, int out_cta_max) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    const int q = (int)blockIdx.x / CL;
+    const int H = a.H, HC = a.HC, R = a.R, B = a.B, T = a.T, K = a.K;
+    const int h0 = rank * HC;
+    const BwdSmem L = bwd_smem(H, HC, R, SMOOTH, out_cta_max);
+    extern __shared__ __align__(16) unsigned char smem[];
+    float *pnew = reinterpret_cast<float *>(smem + L.pnew);
+    float *part = reinterpret_cast<float *>(smem + L.part);
+    unsigned char *ring = smem + L.ring;
+    float *wout = reinterpret_cast<float *>(smem + L.wout);
+    float *dwo = reinterpret_cast<float *>(smem + L.dwo);
+    float *obuf = reinterpret_cast<float *>(smem + L.obuf);
+    int32_t *grp = reinterpret_cast<int32_t *>(smem + L.grp);
+    uint16_t *ocode = reinterpret_cast<uint16_t *>(smem + L.code);
+    float *dw = reinterpret_cast<float *>(smem + L.dw);
+    const int tid = threadIdx.x, nthr = blockDim.x;
+
+    const int obase = a.out_grp[(size_t)h0 * (MAXD + 1)];
+    const int on_all = a.out_grp[(size_t)(h0 + HC - 1) * (MAXD + 1) + MAXD] - obase;
+    const int on = min(on_all, out_cta_max);  // a wrong out_cta_max: the links past it are skipped, counted
+    for (size_t k = tid; k < L.total / 4; k += nthr) reinterpret_cast<uint32_t *>(smem)[k] = 0u;
+    __syncthreads();
+    for (int k = tid; k < HC * R; k += nthr) wout[k] = a.w_out[(size_t)h0 * R + k];
+    for (int k = tid; k < HC * (MAXD + 1); k += nthr) grp[k] = a.out_grp[(size_t)h0 * (MAXD + 1) + k] - obase;
+    for (int k = tid; k < on; k += nthr) ocode[k] = a.out_code[obase + k];
+    const float *ow = a.out_w + obase;
+    __syncthreads();
+    cl.sync();
+
+    const bool nt = tid < 2 * HC;
+    const int pl = nt ? tid >> 1 : 0, half = tid & 1;
+    const int me = h0 + pl;  // this thread's neuron (post of its incoming row, pre of its outgoing row)
+    const int irs = nt ? a.in_ptr[me] : 0, ire = nt ? a.in_ptr[me + 1] : 0;
+    const bool ro = tid < NS * R;
+    const int rb = ro ? tid / R : 0, rr = ro ? tid % R : 0;
+    const float dmv = ro ? a.dm[(size_t)(q * NS + rb) * R + rr] : 0.f;
+    const int tsv = ro ? a.tstar_in[(size_t)(q * NS + rb) * R + rr] : -1;
+    float o = 0.f;
+    float pprev[4] = {0.f, 0.f, 0.f, 0.f};
+    const int R2 = (R + 1) / 2;
+
+    // this neuron's 8 samples' spikes at step tt (0 before step 0): a byte of bits, or floats in the smooth model
+    auto spikes_at = [&](int tt, float out[NS], uint32_t &byte) {
+        byte = 0;
+        if constexpr (SMOOTH) {
+#pragma unroll
+            for (int b = 0; b < NS; ++b) out[b] = 0.f;
+            if (tt < 0 || !nt) return;
+            const float4 *src = reinterpret_cast<const float4 *>(a.s_f) + (((size_t)tt * a.NC + q) * H + me) * 2;
+            const float4 x = src[0], y = src[1];
+            out[0] = x.x; out[1] = x.y; out[2] = x.z; out[3] = x.w;
+            out[4] = y.x; out[5] = y.y; out[6] = y.z; out[7] = y.w;
+            byte = 0xffu;
+        } else {
+            (void)out;
+            if (tt < 0 || !nt) return;
+            byte = a.s_bits[((size_t)tt * a.NC + q) * H + me];
+        }
+    };
+
+    for (int seg = a.nseg - 1; seg >= 0; --seg) {
+        const int t0 = seg * K, t1 = min(T, t0 + K);
+        // ---- recompute the segment from its checkpoint (no cluster barrier: every spike is stored)
+        float V[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            V[j] = nt ? a.v_ckpt[((size_t)seg * B + q * NS + 4 * half + j) * H + me] : 0.f;
+        __syncthreads();  // the previous use of the ring is over
+        for (int d = 1; d <= MAXD; ++d) {
+            const int tt = t0 - d, slot = ((tt % RING) + RING) % RING;
+            for (int j = tid; j < H; j += nthr) {
+                if constexpr (SMOOTH) {
+                    float4 *dst = reinterpret_cast<float4 *>(ring) + ((size_t)slot * H + j) * 2;
+                    if (tt >= 0) {
+                        const float4 *src = reinterpret_cast<const float4 *>(a.s_f) + (((size_t)tt * a.NC + q) * H + j) * 2;
+                        dst[0] = src[0];
+                        dst[1] = src[1];
+                    } else {
+                        dst[0] = dst[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
+                } else {
+                    ring[(size_t)slot * H + j] = tt >= 0 ? a.s_bits[((size_t)tt * a.NC + q) * H + j] : 0;
+                }
+            }
+        }
+        __syncthreads();
+        for (int t = t0; t < t1; ++t) {
+            if (t > t0) {  // S[t - 1] into its slot (it replaces S[t - 7], no longer read)
+                const int tt = t - 1, slot = tt % RING;
+                for (int j = tid; j < H; j += nthr) {
+                    if constexpr (SMOOTH) {
+                        const float4 *src = reinterpret_cast<const float4 *>(a.s_f) + (((size_t)tt * a.NC + q) * H + j) * 2;
+                        float4 *dst = reinterpret_cast<float4 *>(ring) + ((size_t)slot * H + j) * 2;
+                        dst[0] = src[0];
+                        dst[1] = src[1];
+                    } else {
+                        ring[(size_t)slot * H + j] = a.s_bits[((size_t)tt * a.NC + q) * H + j];
+                    }
+                }
+                __syncthreads();
+            }
+            float acc[NS];
+            gather_in<SMOOTH>(a, ring, a.in_code, a.in_w, irs, ire, half, t, acc);
+            if (nt) {
+                float st[NS];
+                uint32_t byte;
+                spikes_at(t, st, byte);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int b = 4 * half + j;
+                    const float u = __ldg(a.U + ((size_t)t * B + q * NS + b) * H + me);
+                    float vp;
+                    const float s = lif_step<SMOOTH>(a, V[j], u, half ? acc[4 + j] : acc[j], vp);
+                    float stored;
+                    if constexpr (SMOOTH) stored = half ? st[4 + j] : st[j];
+                    else stored = ((byte >> b) & 1u) ? 1.f : 0.f;
+                    if (s != stored) atomicAdd(a.err + 1, 1);  // the replay differs from the forward
+                    a.g_seg[((size_t)(t - t0) * B + q * NS + b) * H + me] = surrogate(__fadd_rn(vp, -a.theta), a.slope);
+                }
+            }
+        }
+        // ---- the segment backwards
+        // this neuron's spikes at t - 1 .. t - 5 (for its outgoing links' dw), shifted in as t falls
+        uint64_t hist = 0;      // spiking: byte d - 1 = the 8 samples' spikes at t - d
+        float histf[MAXD][NS];  // smooth: histf[d - 1] = spikes at t - d
+        for (int d = 1; d <= MAXD; ++d) {
+            uint32_t byte;
+            spikes_at(t1 - 1 - d, histf[d - 1], byte);
+            if constexpr (!SMOOTH) hist |= (uint64_t)byte << (8 * (d - 1));
+        }
+        for (int t = t1 - 1; t >= t0; --t) {
+            if (ro) {
+                o = __fadd_rn(t == tsv ? dmv : 0.f, __fmul_rn(a.beta, o));
+                obuf[rb * R + rr] = o;
+            }
+            __syncthreads();  // obuf ready; the previous step's partial-ring writes done
+            if (nt) {
+                float qv[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int b = 4 * half + j;
+                    float *pp = part + ((size_t)(t % RING) * HC + pl) * NS + b;
+                    float sh = *pp;
+                    for (int r = 0; r < R; ++r) sh = __fadd_rn(sh, __fmul_rn(wout[pl * R + r], obuf[b * R + r]));
+                    *pp = 0.f;
+                    const float g = a.g_seg[((size_t)(t - t0) * B + q * NS + b) * H + me];
+                    const float ap = __fmul_rn(a.alpha, pprev[j]);
+                    qv[j] = __fadd_rn(ap, __fmul_rn(g, __fadd_rn(sh, -__fmul_rn(a.theta, ap))));
+                    pprev[j] = qv[j];
+                    a.dU[((size_t)t * B + q * NS + b) * H + me] = qv[j];
+                }
+                const float4 v = make_float4(qv[0], qv[1], qv[2], qv[3]);
+                float4 *dst = reinterpret_cast<float4 *>(pnew) + ((size_t)(t & 1) * H + me) * 2 + half;
+                for (int k = 0; k < CL; ++k) *cl.map_shared_rank(dst, k) = v;
+                // dw_out: this neuron's spikes at t times o[t]; each half takes half of the readouts
+                float st[NS];
+                uint32_t byte;
+                spikes_at(t, st, byte);
+                if (byte) {
+                    for (int r = half * R2; r < min(R, (half + 1) * R2); ++r) {
+                        float acc = dwo[pl * R + r];
+                        for (int b = 0; b < NS; ++b) {
+                            if constexpr (SMOOTH) acc = __fadd_rn(acc, __fmul_rn(st[b], obuf[b * R + r]));
+                            else if ((byte >> b) & 1u) acc = __fadd_rn(acc, obuf[b * R + r]);
+                        }
+                        dwo[pl * R + r] = acc;
+                    }
+                }
+            }
+            cl.sync();  // q[t] of every neuron in every CTA's pnew[t & 1]
+            // outgoing rows: partial[t - d] += w q[t][post]; dw += s[t - d][me] q[t][post]
+            const float *pn = pnew + (size_t)(t & 1) * H * NS;
+            for (int d = 1; d <= MAXD; ++d) {
+                float acc[NS];
+#pragma unroll
+                for (int b = 0; b < NS; ++b) acc[b] = 0.f;
+                const int gs = nt ? grp[pl * (MAXD + 1) + d - 1] : 0, ge = nt ? grp[pl * (MAXD + 1) + d] : 0;
+                const uint32_t sbyte = SMOOTH ? 0xffu : (uint32_t)((hist >> (8 * (d - 1))) & 0xffu);
+                for (int l = gs + half; l < ge; l += 2) {
+                    if (l >= on) {
+                        atomicAdd(a.err + 2, 1);
+                        continue;
+                    }
+                    const uint32_t c = ocode[l];
+                    const int post = (int)(c & 0x7FFu);
+                    if ((int)(c >> 11) != d || post >= H) {
+                        atomicAdd(a.err + 0, 1);
+                        continue;
+                    }
+                    const float wl = __ldg(ow + l);
+                    const float4 x0 = reinterpret_cast<const float4 *>(pn)[(size_t)post * 2];
+                    const float4 x1 = reinterpret_cast<const float4 *>(pn)[(size_t)post * 2 + 1];
+                    const float x[NS] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+#pragma unroll
+                    for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __fmul_rn(wl, x[b]));
+                    if (sbyte) {
+                        float dk = 0.f;
+#pragma unroll
+                        for (int b = 0; b < NS; ++b) {
+                            if constexpr (SMOOTH) dk = __fadd_rn(dk, __fmul_rn(histf[d - 1][b], x[b]));
+                            else if ((sbyte >> b) & 1u) dk = __fadd_rn(dk, x[b]);
+                        }
+                        dw[l] = __fadd_rn(dw[l], dk);
+                    }
+                }
+#pragma unroll
+                for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __shfl_xor_sync(FULL, acc[b], 1));
+                if (nt && t - d >= 0) {
+                    float *pp = part + ((size_t)((t - d) % RING) * HC + pl) * NS + 4 * half;
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) pp[j] = __fadd_rn(pp[j], half ? acc[4 + j] : acc[j]);
+                }
+            }
+            // the spike history of step t - 1: delays 1..5 reach t - 2 .. t - 6
+            if constexpr (SMOOTH) {
+                for (int d = 1; d <= MAXD; ++d) {
+                    uint32_t byte;
+                    spikes_at(t - 1 - d, histf[d - 1], byte);
+                }
+            } else {
+                uint32_t byte;
+                spikes_at(t - 1 - MAXD, histf[0], byte);
+                hist = (hist >> 8) | ((uint64_t)byte << (8 * (MAXD - 1)));
+            }
+        }
+    }
+    __syncthreads();
+    if (nt && half == 0)
+        for (int r = 0; r < R; ++r) a.dwo_p[((size_t)q * H + me) * R + r] = dwo[pl * R + r];
+    for (int k = tid; k < on; k += nthr) a.dwp[(size_t)q * a.nnz + obase + k] = dw[k];
+    cl.sync();
+}
+
+// dw_rec in the caller's (incoming, canonical) order: the clusters' partials added in cluster order.
+__global__ void reduce_dw_kernel(const float *dwp, const int32_t *perm, int nnz, int NC, float *dw) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nnz) return;
+    float s = 0.f;
+    for (int c = 0; c < NC; ++c) s = __fadd_rn(s, dwp[(size_t)c * nnz + l]);
+    dw[perm[l]] = s;
+}
+
+__global__ void reduce_dwo_kernel(const float *dwo_p, int n, int NC, float *dwo) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    float s = 0.f;
+    for (int c = 0; c < NC; ++c) s = __fadd_rn(s, dwo_p[(size_t)c * n + k]);
+    dwo[k] = s;
+}
+
+__global__ void gather_kernel(const float *src, const int32_t *perm, int n, float *dst) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l < n) dst[l] = src[perm[l]];
+}
+
+}  // namespace n2b_bptt
+
+// ------------------------------------------------------------------------------------------------ host
+
+namespace n2b_host {
+int set_error(int code, const std::string &msg);
+}
+
+namespace {
+
+using namespace n2b_bptt;
+
+int bfail(int code, const std::string &msg) { return n2b_host::set_error(code, msg); }
+int bcuda(cudaError_t e, const char *what) {
+    return n2b_host::set_error(N2B_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define B_CUDA(call)                                    \
+    do {                                                \
+        cudaError_t _e = (call);                        \
+        if (_e != cudaSuccess) return bcuda(_e, #call); \
+    } while (0)
+
+struct WsLayout {
+    size_t spikes, vck, gseg, outw, dwp, dwo, err, total;
+};
+
+size_t a256(size_t x) { return (x + 255) & ~size_t(255); }
+
+int check_desc(const n2b_bptt_desc *d) {
+    if (!d) return bfail(N2B_EINVAL, "desc is NULL");
+    if (d->batch <= 0 || d->batch % NS) return bfail(N2B_EINVAL, "batch must be a positive multiple of 8");
+    if (d->hidden <= 0 || d->hidden % CL || d->hidden > 2048)
+        return bfail(N2B_EINVAL, "hidden must be a multiple of 8, at most 2048");
+    if (d->readouts <= 0 || d->readouts > 32) return bfail(N2B_EINVAL, "readouts must be in 1..32");
+    if (d->steps <= 0 || d->checkpoint <= 0) return bfail(N2B_EINVAL, "steps and checkpoint must be positive");
+    if (d->smooth && d->hidden > 256) return bfail(N2B_EINVAL, "the smooth model is for hidden <= 256");
+    if (d->nnz < 0 || (d->nnz > 0 && (!d->in_code || !d->out_code || !d->out_perm)))
+        return bfail(N2B_EINVAL, "missing link arrays");
+    if (!d->in_ptr || !d->out_grp) return bfail(N2B_EINVAL, "missing row arrays");
+    if (d->in_cta_max < 0 || d->out_cta_max < 0) return bfail(N2B_EINVAL, "negative link counts");
+    return N2B_OK;
+}
+
+WsLayout ws_layout(const n2b_bptt_desc *d) {
+    WsLayout L{};
+    const size_t T = d->steps, B = d->batch, H = d->hidden, R = d->readouts, NC = B / NS;
+    const size_t nseg = (T + d->checkpoint - 1) / d->checkpoint, K = std::min<size_t>(d->checkpoint, T);
+    size_t o = 0;
+    L.spikes = o; o = a256(o + (d->smooth ? sizeof(float) * T * NC * H * NS : T * NC * H));
+    L.vck = o; o = a256(o + sizeof(float) * nseg * B * H);
+    L.gseg = o; o = a256(o + sizeof(float) * K * B * H);
+    L.outw = o; o = a256(o + sizeof(float) * std::max<size_t>(d->nnz, 1));
+    L.dwp = o; o = a256(o + sizeof(float) * NC * std::max<size_t>(d->nnz, 1));
+    L.dwo = o; o = a256(o + sizeof(float) * NC * H * R);
+    L.err = o; o = a256(o + sizeof(int32_t) * N2B_BPTT_ERR_WORDS);
+    L.total = o;
+    return L;
+}
+
+int threads_of(const n2b_bptt_desc *d) {
+    const int n = std::max(2 * (d->hidden / CL), NS * d->readouts);
+    return (n + 31) / 32 * 32;
+}
+
+Args args_of(const n2b_bptt_desc *d, char *ws, const WsLayout &L) {
+    Args a{};
+    a.B = d->batch;
+    a.T = d->steps;
+    a.H = d->hidden;
+    a.R = d->readouts;
+    a.K = d->checkpoint;
+    a.HC = d->hidden / CL;
+    a.NC = d->batch / NS;
+    a.nseg = (d->steps + d->checkpoint - 1) / d->checkpoint;
+    a.nnz = d->nnz;
+    a.alpha = d->alpha;
+    a.beta = d->beta;
+    a.theta = d->theta;
+    a.slope = d->slope;
+    a.in_ptr = d->in_ptr;
+    a.in_code = d->in_code;
+    a.out_grp = d->out_grp;
+    a.out_code = d->out_code;
+    a.s_bits = reinterpret_cast<uint8_t *>(ws + L.spikes);
+    a.s_f = reinterpret_cast<float *>(ws + L.spikes);
+    a.v_ckpt = reinterpret_cast<float *>(ws + L.vck);
+    a.g_seg = reinterpret_cast<float *>(ws + L.gseg);
+    a.out_w = reinterpret_cast<float *>(ws + L.outw);
+    a.dwp = reinterpret_cast<float *>(ws + L.dwp);
+    a.dwo_p = reinterpret_cast<float *>(ws + L.dwo);
+    a.err = reinterpret_cast<int32_t *>(ws + L.err);
+    return a;
+}
+
+int check_ws(const n2b_bptt_desc *d, void *ws, size_t bytes, WsLayout &L) {
+    int rc = check_desc(d);
+    if (rc) return rc;
+    L = ws_layout(d);
+    if (!ws || (reinterpret_cast<uintptr_t>(ws) & 255)) return bfail(N2B_EINVAL, "workspace must be 256-byte aligned");
+    if (bytes < L.total) return bfail(N2B_ESPACE, "workspace too small: need " + std::to_string(L.total) + " bytes");
+    return N2B_OK;
+}
+
+template <class Kern>
+int launch_cluster(Kern kern, int grid, int threads, size_t smem, cudaStream_t s, const Args &a, int extra) {
+    if (smem > 227 * 1024) return bfail(N2B_EINVAL, "shared memory need " + std::to_string(smem) + " bytes > 227 KiB");
+    B_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    B_CUDA(cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg));
+    if (clusters < 1) return bfail(N2B_ECUDA, "a cluster of 8 CTAs of this size cannot be resident");
+    B_CUDA(cudaLaunchKernelEx(&cfg, kern, a, extra));
+    return N2B_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int n2b_bptt_workspace_bytes(const n2b_bptt_desc *d, size_t *bytes) {
+    if (!bytes) return bfail(N2B_EINVAL, "bytes is NULL");
+    int rc = check_desc(d);
+    if (rc) return rc;
+    *bytes = ws_layout(d).total;
+    return N2B_OK;
+}
+
+int n2b_bptt_forward(const n2b_bptt_desc *d, const float *u, const float *w_rec, const float *w_out, int32_t tape,
+                     float *m, int32_t *tstar, void *workspace, size_t workspace_bytes, void *stream) {
+    WsLayout L;
+    int rc = check_ws(d, workspace, workspace_bytes, L);
+    if (rc) return rc;
+    if (!u || !w_out || !m || !tstar || (d->nnz > 0 && !w_rec)) return bfail(N2B_EINVAL, "missing arguments");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    char *ws = static_cast<char *>(workspace);
+    Args a = args_of(d, ws, L);
+    a.tape = tape != 0;
+    a.U = u;
+    a.in_w = w_rec;
+    a.w_out = w_out;
+    a.m = m;
+    a.tstar = tstar;
+    B_CUDA(cudaMemsetAsync(ws + L.err, 0, sizeof(int32_t) * N2B_BPTT_ERR_WORDS, s));
+    const bool smooth = d->smooth != 0;
+    FwdSmem S = fwd_smem(d->hidden, d->hidden / CL, d->readouts, smooth, true, d->in_cta_max);
+    a.csr_smem = S.total <= 200 * 1024;
+    if (!a.csr_smem) S = fwd_smem(d->hidden, d->hidden / CL, d->readouts, smooth, false, 0);
+    const int grid = (d->batch / NS) * CL, threads = threads_of(d);
+    return smooth ? launch_cluster(fwd_kernel<true>, grid, threads, S.total, s, a, d->in_cta_max)
+                  : launch_cluster(fwd_kernel<false>, grid, threads, S.total, s, a, d->in_cta_max);
+}
+
+int n2b_bptt_backward(const n2b_bptt_desc *d, const float *u, const float *w_rec, const float *w_out,
+                      const float *dm, const int32_t *tstar, float *du, float *dw_rec, float *dw_out,
+                      void *workspace, size_t workspace_bytes, void *stream) {
+    WsLayout L;
+    int rc = check_ws(d, workspace, workspace_bytes, L);
+    if (rc) return rc;
+    if (!u || !w_out || !dm || !tstar || !du || !dw_out || (d->nnz > 0 && (!w_rec || !dw_rec)))
+        return bfail(N2B_EINVAL, "missing arguments");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    char *ws = static_cast<char *>(workspace);
+    Args a = args_of(d, ws, L);
+    a.U = u;
+    a.in_w = w_rec;
+    a.w_out = w_out;
+    a.dm = dm;
+    a.tstar_in = tstar;
+    a.dU = du;
+    if (d->nnz > 0) {  // the weights in outgoing order
+        gather_kernel<<<(d->nnz + 255) / 256, 256, 0, s>>>(w_rec, d->out_perm, d->nnz,
+                                                           reinterpret_cast<float *>(ws + L.outw));
+        B_CUDA(cudaGetLastError());
+    }
+    const bool smooth = d->smooth != 0;
+    const BwdSmem S = bwd_smem(d->hidden, d->hidden / CL, d->readouts, smooth, d->out_cta_max);
+    const int grid = (d->batch / NS) * CL, threads = threads_of(d);
+    rc = smooth ? launch_cluster(bwd_kernel<true>, grid, threads, S.total, s, a, d->out_cta_max)
+                : launch_cluster(bwd_kernel<false>, grid, threads, S.total, s, a, d->out_cta_max);
+    if (rc) return rc;
+    const int NC = d->batch / NS;
+    if (d->nnz > 0) {
+        reduce_dw_kernel<<<(d->nnz + 255) / 256, 256, 0, s>>>(a.dwp, d->out_perm, d->nnz, NC, dw_rec);
+        B_CUDA(cudaGetLastError());
+    }
+    const int n = d->hidden * d->readouts;
+    reduce_dwo_kernel<<<(n + 255) / 256, 256, 0, s>>>(a.dwo_p, n, NC, dw_out);
+    B_CUDA(cudaGetLastError());
+    return N2B_OK;
+}
+
+int n2b_bptt_status(const n2b_bptt_desc *d, void *workspace, size_t workspace_bytes, int32_t *words, void *stream) {
+    WsLayout L;
+    int rc = check_ws(d, workspace, workspace_bytes, L);
+    if (rc) return rc;
+    if (!words) return bfail(N2B_EINVAL, "words is NULL");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    int32_t host[N2B_BPTT_ERR_WORDS];
+    B_CUDA(cudaMemcpyAsync(host, static_cast<char *>(workspace) + L.err, sizeof(host), cudaMemcpyDeviceToHost, s));
+    B_CUDA(cudaStreamSynchronize(s));
+    for (int k = 0; k < N2B_BPTT_ERR_WORDS; ++k) words[k] = host[k];
+    return N2B_OK;
+}
+
+int n2b_bptt_spikes(const n2b_bptt_desc *d, void *workspace, size_t workspace_bytes, void *out, void *stream) {
+    WsLayout L;
+    int rc = check_ws(d, workspace, workspace_bytes, L);
+    if (rc) return rc;
+    if (!out) return bfail(N2B_EINVAL, "out is NULL");
+    const size_t T = d->steps, NC = d->batch / NS, H = d->hidden;
+    const size_t n = d->smooth ? sizeof(float) * T * NC * H * NS : T * NC * H;
+    B_CUDA(cudaMemcpyAsync(out, static_cast<char *>(workspace) + L.spikes, n, cudaMemcpyDeviceToDevice,
+                           reinterpret_cast<cudaStream_t>(stream)));
+    return N2B_OK;
+}
+
+}  // extern "C"

@@ -39,6 +39,15 @@ int cuda_fail(cudaError_t e, const char *what) {
 
 bool pow2(int32_t x) { return x > 0 && (x & (x - 1)) == 0; }
 
+}  // namespace
+
+// The calling thread's error message, shared with the library's other translation units (bptt.cu).
+namespace n2b_host {
+int set_error(int code, const std::string &msg) { return fail(code, msg); }
+}  // namespace n2b_host
+
+namespace {
+
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 struct Layout {

@@ -35,7 +35,8 @@ def test_struct_layouts_match_the_header(tmp_path):
     src = tmp_path / "layout.c"
     fields = {"n2b_population": [f[0] for f in _lib.Population._fields_],
               "n2b_connection": [f[0] for f in _lib.Connection._fields_],
-              "n2b_options": [f[0] for f in _lib.Options._fields_]}
+              "n2b_options": [f[0] for f in _lib.Options._fields_],
+              "n2b_bptt_desc": [f[0] for f in _lib.BpttDesc._fields_]}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', 'int main(void) {']
     for s, fs in fields.items():
         lines.append(f'printf("{s} %zu\\n", sizeof({s}));')
@@ -48,7 +49,7 @@ def test_struct_layouts_match_the_header(tmp_path):
     out = dict(line.rsplit(" ", 1) for line in subprocess.run([str(exe)], capture_output=True, text=True,
                                                                check=True).stdout.splitlines())
     for s, cls in (("n2b_population", _lib.Population), ("n2b_connection", _lib.Connection),
-                   ("n2b_options", _lib.Options)):
+                   ("n2b_options", _lib.Options), ("n2b_bptt_desc", _lib.BpttDesc)):
         assert int(out[s]) == ctypes.sizeof(cls), s
         for f in fields[s]:
             assert int(out[f"{s}.{f}"]) == getattr(cls, f).offset, f"{s}.{f}"
