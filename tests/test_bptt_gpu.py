@@ -99,15 +99,21 @@ def test_spiking_kernels_match_the_teacher_forced_fp64_reference(cuda, K):
 
 
 def test_checkpoint_interval_changes_nothing(cuda):
+    """The kernels' outputs (dU, dw_rec, dw_out) are bit-identical for any checkpoint interval: the recomputed
+    segments reproduce the forward exactly. (w_in's gradient, x^T dU, comes from torch's sparse product,
+    whose summation order is not fixed.)"""
     out = []
     for K in (1, 7, 60):
         layer, x, y = make(cuda, B=16, T=60, K=K, seed=4)
-        m, loss, grads = kernel_grads(layer, x, y)
-        out.append((m, grads))
-    for m, grads in out[1:]:
-        assert torch.equal(m, out[0][0])
-        for g, g0 in zip(grads, out[0][1]):
-            assert torch.equal(g, g0)
+        with torch.no_grad():
+            U = layer.current(x).contiguous()
+            m, ts = layer.run_forward(U, tape=True)
+            dm = torch.softmax(m, 1) - torch.nn.functional.one_hot(y, m.shape[1]).float()
+            out.append((m, ts) + layer.run_backward(U, dm, ts))
+        assert layer.status(16, 60) == [0, 0, 0, 0]
+    for o in out[1:]:
+        for a, b in zip(o, out[0]):
+            assert torch.equal(a, b)
 
 
 def test_plain_forward_equals_the_taped_one_and_the_tape_is_guarded(cuda):
