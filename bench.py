@@ -393,6 +393,75 @@ def run_batched(args, dev) -> dict:
             "tune": report["trials"] if report else None, "build_s": build_s}
 
 
+def run_bptt(args, dev) -> dict:
+    """Config 4: surrogate-gradient BPTT of the recurrent LIF layer (B 128, T 500, 700 channels, 1024 hidden at
+    10% density, delays 1-5 steps, 20 readouts, checkpoints every 50 steps). One bench step: the plain forward
+    (input current + forward kernel, no tape), then one training step (taped forward + loss + backward through
+    the adjoint kernels and the input projection's gradient), each timed with CUDA events after an L2 flush."""
+    import torch
+
+    from naer2_b200.networks import bptt_task
+
+    t0 = time.perf_counter()
+    layer, x, y = bptt_task.build(seed=1, device=dev)
+    T, B, C = x.shape
+    xs = x.reshape(T * B, C).float().to_sparse()  # the input as spike events
+    build_s = time.perf_counter() - t0
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    def train_step():
+        layer.zero_grad(set_to_none=True)
+        m = layer(xs, steps=T)
+        loss = torch.nn.functional.cross_entropy(m, y)
+        loss.backward()
+        return loss
+
+    U = layer.current(xs, steps=T).detach().contiguous()
+    with torch.no_grad():
+        m0, ts0 = layer.run_forward(U, tape=True)
+        dm0 = torch.softmax(m0, 1) - torch.nn.functional.one_hot(y, m0.shape[1]).float()
+    for _ in range(args.warmup):
+        layer.infer(xs, steps=T)
+        train_step()
+    plain, train, fk, fk_tape, bk = [], [], [], [], []
+    with Clocks(dev.index or 0) as clocks:
+        for _ in range(args.steps):
+            plain.append(timed(lambda: layer.infer(xs, steps=T))[0])
+            train.append(timed(train_step)[0])
+            fk.append(timed(lambda: layer.run_forward(U, tape=False))[0])
+            fk_tape.append(timed(lambda: layer.run_forward(U, tape=True))[0])
+            bk.append(timed(lambda: layer.run_backward(U, dm0, ts0))[0])
+    assert layer.status(B, T) == [0, 0, 0, 0]
+    with torch.no_grad():
+        layer.run_forward(U, tape=True)
+        spikes = layer.spikes(B, T)
+        events = float((spikes.float().sum((0, 1)) * layer.wiring.out_degree.float()).sum())
+    ms_plain, ms_train = sum(plain) / len(plain), sum(train) / len(train)
+    ms_fk, ms_fkt, ms_bk = (sum(v) / len(v) for v in (fk, fk_tape, bk))
+    return {"metric": METRIC, "value": events / (ms_plain / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_plain + ms_train, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Poisson class templates, 20 classes)",
+            "config": {"workload": "bptt_config4", "batch": B, "steps_T": T, "channels": C, "hidden": layer.hidden,
+                       "readouts": layer.readouts, "recurrent_links": layer.wiring.nnz, "checkpoint": layer.checkpoint,
+                       "l2": "flushed before every timed call (256 MiB write)"},
+            "plain_forward_ms": ms_plain, "train_step_ms": ms_train,
+            "bptt_over_plain_forward": ms_train / ms_plain,
+            "kernels_ms": {"forward_plain": ms_fk, "forward_taped": ms_fkt, "backward": ms_bk},
+            "kernel_bptt_over_forward": (ms_fkt + ms_bk) / ms_fk,
+            "recurrent_events_per_forward": events, "spike_rate": float(spikes.float().mean()),
+            "realtime_factor": (ms_plain / 1e3) / (T * 1e-3), "build_s": build_s, "clocks": clocks.summary()}
+
+
 def main() -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -400,9 +469,10 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="naer2_b200", choices=["naer2_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", type=int, default=1, choices=[1, 2, 3],
+    ap.add_argument("--config", type=int, default=1, choices=[1, 2, 3, 4],
                     help="1: Brunel model A at config 1's size (the default workload); 2: the PD14 microcircuit; "
-                         "3: 64 uneven Brunel instances batched against one at a time")
+                         "3: 64 uneven Brunel instances batched against one at a time; 4: BPTT of the "
+                         "recurrent LIF layer (training step against the plain forward)")
     ap.add_argument("--instances", type=int, default=64, help="config 3: instances")
     ap.add_argument("--tune", action="store_true", help="config 3: run the autotuner first")
     ap.add_argument("--scale", type=float, default=1.0, help="config 2: population sizes times this")
@@ -433,10 +503,11 @@ def main() -> int:
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if args.config in (2, 3):
+    if args.config in (2, 3, 4):
         if world > 1:
             raise SystemExit(f"config {args.config} runs on one GPU")
-        print(json.dumps(run_pd14(args, dev) if args.config == 2 else run_batched(args, dev)))
+        run = {2: run_pd14, 3: run_batched, 4: run_bptt}[args.config]
+        print(json.dumps(run(args, dev)))
         return 0
     if world > 1:
         import datetime

@@ -198,7 +198,7 @@ int n2b_destroy(n2b_net *net);
 typedef struct n2b_bptt_desc {
     int32_t batch;       /* B, a multiple of 8 (8 samples per cluster of 8 CTAs) */
     int32_t steps;       /* T */
-    int32_t hidden;      /* H, a multiple of 8, at most 2048 */
+    int32_t hidden;      /* H, a multiple of 32, at most 1024 */
     int32_t readouts;    /* R, at most 32 */
     int32_t checkpoint;  /* K: membrane checkpoint every K steps */
     int32_t smooth;      /* 1: the smooth forward (hidden <= 256), for gradient checks */

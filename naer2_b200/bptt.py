@@ -84,8 +84,8 @@ class RecurrentLIF(torch.nn.Module):
                  slope: float = 10.0, checkpoint: int = 50, seed: int = 0, device="cuda", smooth: bool = False,
                  links=None, w_scale: tuple = (4.0, 0.5, 1.0)):
         super().__init__()
-        if hidden % 8:
-            raise ValueError("hidden must be a multiple of 8")
+        if hidden % 32 or hidden > 1024:
+            raise ValueError("hidden must be a multiple of 32, at most 1024")
         self.n_in, self.hidden, self.readouts = n_in, hidden, readouts
         self.alpha = float(np.float32(math.exp(-dt / tau_mem)))
         self.beta = float(np.float32(math.exp(-dt / tau_out)))

@@ -15,13 +15,15 @@
 //   dU[t][i] = q[t][i];  dw_k = sum_t,b s[t - d_k][pre_k] q[t][post_k];  dw_out[i][r] = sum_t,b s[t][i] o[t][r]
 //
 // Layout: a cluster of 8 CTAs runs 8 samples; CTA `rank` owns hidden neurons [rank*HC, rank*HC + HC), HC = H/8,
-// two threads per neuron (one per 4 samples; the link loops split a row between the two, interleaved).
+// four threads per neuron (two samples each; the link loops split a row among the four, interleaved).
 // Forward: every CTA keeps the spikes of the last 6 steps of all H neurons for its 8 samples (one byte of 8
 // sample bits per neuron, or 8 floats in the smooth model) in shared memory; each step a neuron's new entry
 // is written into all 8 CTAs' rings (distributed shared memory) before one cluster barrier. Backward: each
-// K-step segment is first recomputed from its membrane checkpoint and the stored spikes of every step
-// (same arithmetic, same order: the same Vpre bit for bit), then run backwards; q of all neurons is exchanged
-// the same way, and each neuron pushes its outgoing rows' q sums into a 6-slot ring of its own partials.
+// K-step segment is first recomputed from its membrane checkpoint and the stored spikes of every step by two
+// grid-wide kernels (the recurrent inputs of all its steps at once, then one membrane scan per neuron and
+// sample; same arithmetic, same order: the same Vpre bit for bit), then run backwards by one cluster launch;
+// q of all neurons is exchanged the same way, and each neuron pushes its outgoing rows' q sums into a 6-slot
+// ring of its own partials, kept in global memory between the segments' launches.
 // Every sum has a fixed order (no float atomics), so results are bit-for-bit reproducible.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
@@ -30,6 +32,7 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <type_traits>
 
 #include "../../include/naer2b.h"
 
@@ -37,9 +40,11 @@ namespace cg = cooperative_groups;
 
 namespace n2b_bptt {
 
-constexpr int NS = 8;    // samples per cluster
-constexpr int CL = 8;    // CTAs per cluster
-constexpr int RING = 6;  // spike / partial ring slots (delays 1..5)
+constexpr int NS = 8;          // samples per cluster
+constexpr int CL = 8;          // CTAs per cluster
+constexpr int NT = 4;          // threads per neuron
+constexpr int SPT = NS / NT;   // samples per thread
+constexpr int RING = 6;        // spike / partial ring slots (delays 1..5)
 constexpr int MAXD = 5;
 constexpr unsigned FULL = 0xffffffffu;
 
@@ -57,7 +62,7 @@ struct Args {
     uint8_t *s_bits;    // [T][NC][H]      (spiking)
     float *s_f;         // [T][NC][H][8]   (smooth)
     float *v_ckpt;      // [nseg][B][H]
-    float *g_seg;       // [K][B][H]
+    float *g_seg;       // [K][B][H]: the segment's recurrent input, then its surrogate derivatives
     float *dU;          // [T][B][H]
     const float *w_out; // [H][R]
     float *m;           // [B][R]
@@ -66,6 +71,9 @@ struct Args {
     const int32_t *tstar_in;
     float *dwp;         // [NC][nnz] per-cluster dw, out order
     float *dwo_p;       // [NC][H][R]
+    float *part_st;     // [NC * CL][RING][HC][NS] the adjoint's partial ring between segments
+    float *q_st;        // [B][H] q[t0] of the last segment done
+    float *o_st;        // [B][R] the readout adjoint at t0
     int32_t *err;       // [N2B_BPTT_ERR_WORDS]
 };
 
@@ -76,6 +84,12 @@ __device__ __forceinline__ float surrogate(float x, float slope) {
 
 __device__ __forceinline__ float smooth_spike(float x, float slope) {
     return __fdiv_rn(x, __fadd_rn(1.f, __fmul_rn(slope, fabsf(x))));
+}
+
+// v[k] of a thread's two samples: (sub's samples 2 sub, 2 sub + 1) with compile-time indices only.
+__device__ __forceinline__ void mine(const float v[NS], int sub, float &x0, float &x1) {
+    x0 = sub == 0 ? v[0] : sub == 1 ? v[2] : sub == 2 ? v[4] : v[6];
+    x1 = sub == 0 ? v[1] : sub == 1 ? v[3] : sub == 2 ? v[5] : v[7];
 }
 
 // Shared-memory layout of the forward kernel (identical in every CTA, so that remote addresses match).
@@ -97,15 +111,14 @@ __host__ __device__ inline FwdSmem fwd_smem(int H, int HC, int R, bool smooth, b
 }
 
 struct BwdSmem {
-    size_t pnew, part, ring, wout, dwo, obuf, grp, code, dw, total;
+    size_t pnew, part, wout, dwo, obuf, grp, code, dw, total;
 };
-__host__ __device__ inline BwdSmem bwd_smem(int H, int HC, int R, bool smooth, int out_cta_max) {
+__host__ __device__ inline BwdSmem bwd_smem(int H, int HC, int R, int out_cta_max) {
     BwdSmem L{};
     size_t o = 0;
     auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };
     L.pnew = o; o = a16(o + sizeof(float) * 2 * H * NS);
     L.part = o; o = a16(o + sizeof(float) * RING * HC * NS);
-    L.ring = o; o = a16(o + (smooth ? sizeof(float) * RING * H * NS : (size_t)RING * H));
     L.wout = o; o = a16(o + sizeof(float) * HC * R);
     L.dwo = o; o = a16(o + sizeof(float) * HC * R);
     L.obuf = o; o = a16(o + sizeof(float) * NS * R);
@@ -116,46 +129,64 @@ __host__ __device__ inline BwdSmem bwd_smem(int H, int HC, int R, bool smooth, i
     return L;
 }
 
-// The spikes of neuron j at ring slot `slot`: 8 samples (bits, or floats in the smooth model).
-template <bool SMOOTH>
-__device__ __forceinline__ void load_spikes(const unsigned char *ring, int H, int slot, int j, float s[NS],
-                                            uint32_t &byte) {
-    if constexpr (SMOOTH) {
-        const float4 *p = reinterpret_cast<const float4 *>(ring) + ((size_t)slot * H + j) * 2;
-        const float4 a = p[0], b = p[1];
-        s[0] = a.x; s[1] = a.y; s[2] = a.z; s[3] = a.w;
-        s[4] = b.x; s[5] = b.y; s[6] = b.z; s[7] = b.w;
-        byte = 0xffu;  // every sample may contribute
-    } else {
-        (void)s;
-        byte = ring[(size_t)slot * H + j];
+// The spikes that the incoming links read: the forward's shared-memory ring (6 slots, the slot of step t in
+// t mod 6; slots of steps before 0 are still zero), or the stored spikes of every step (recompute).
+struct RingSrc {
+    const unsigned char *ring;
+    int H, tbase;  // t mod 6
+    __device__ __forceinline__ int slot(int d) const {
+        const int sl = tbase - d;
+        return sl < 0 ? sl + RING : sl;
     }
-}
+};
+struct TapeSrc {
+    const uint8_t *bits;
+    const float *f;
+    int H, NC, q, t;
+};
 
-// R for the 8 samples of post `post`: this thread's half of its incoming row (links rs + half, rs + half + 2,
-// ...), then the two halves added (a + b in both lanes: the same value in each).
-template <bool SMOOTH>
-__device__ __forceinline__ void gather_in(const Args &a, const unsigned char *ring, const uint16_t *code,
-                                          const float *w, int rs, int re, int half, int t, float acc[NS]) {
+// R for the 8 samples of one neuron: this thread's share of its incoming row (links rs + sub, rs + sub + NT,
+// ...), then the NT shares added pairwise ((s0 + s1) + (s2 + s3), the same value in all NT lanes).
+// CHECKED: every code is checked (a bad one counted and skipped); otherwise the rows were validated when they
+// were copied (bad links replaced by a zero-weight link). Both give the same sums for the same rows.
+template <bool SMOOTH, bool CHECKED, class Src>
+__device__ __forceinline__ void gather_in(const Args &a, const Src &src, const uint16_t *code, const float *w,
+                                          int rs, int re, int sub, float acc[NS]) {
 #pragma unroll
     for (int b = 0; b < NS; ++b) acc[b] = 0.f;
-    for (int l = rs + half; l < re; l += 2) {
+#pragma unroll 2
+    for (int l = rs + sub; l < re; l += NT) {
         const uint32_t c = code[l];
+        const float wl = w[l];
         const int pre = (int)(c & 0x7FFu), d = (int)(c >> 11);
-        if (d < 1 || d > MAXD || pre >= a.H) {
+        if (CHECKED && (d < 1 || d > MAXD || pre >= a.H)) {
             atomicAdd(a.err + 0, 1);
             continue;
         }
-        if (t - d < 0) continue;
-        float s[NS];
-        uint32_t byte;
-        load_spikes<SMOOTH>(ring, a.H, (t - d) % RING, pre, s, byte);
-        if (!byte) continue;
-        const float wl = w[l];
         if constexpr (SMOOTH) {
+            float s[NS];
+            if constexpr (std::is_same<Src, RingSrc>::value) {
+                const float4 *p = reinterpret_cast<const float4 *>(src.ring) + ((size_t)src.slot(d) * src.H + pre) * 2;
+                const float4 x = p[0], y = p[1];
+                s[0] = x.x; s[1] = x.y; s[2] = x.z; s[3] = x.w; s[4] = y.x; s[5] = y.y; s[6] = y.z; s[7] = y.w;
+            } else {
+                const int tt = src.t - d;
+                if (tt < 0) continue;
+                const float4 *p = reinterpret_cast<const float4 *>(src.f) + (((size_t)tt * src.NC + src.q) * src.H + pre) * 2;
+                const float4 x = p[0], y = p[1];
+                s[0] = x.x; s[1] = x.y; s[2] = x.z; s[3] = x.w; s[4] = y.x; s[5] = y.y; s[6] = y.z; s[7] = y.w;
+            }
 #pragma unroll
             for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __fmul_rn(wl, s[b]));
         } else {
+            uint32_t byte;
+            if constexpr (std::is_same<Src, RingSrc>::value) {
+                byte = src.ring[(size_t)src.slot(d) * src.H + pre];
+            } else {
+                const int tt = src.t - d;
+                byte = tt >= 0 ? src.bits[((size_t)tt * src.NC + src.q) * src.H + pre] : 0u;
+            }
+            if (!byte) continue;
 #pragma unroll
             for (int b = 0; b < NS; ++b)
                 if ((byte >> b) & 1u) acc[b] = __fadd_rn(acc[b], wl);
@@ -163,9 +194,11 @@ __device__ __forceinline__ void gather_in(const Args &a, const unsigned char *ri
     }
 #pragma unroll
     for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __shfl_xor_sync(FULL, acc[b], 1));
+#pragma unroll
+    for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __shfl_xor_sync(FULL, acc[b], 2));
 }
 
-// One membrane step of one sample: returns the spike value, updates V (and gives Vpre).
+// One membrane step of one sample: returns the spike value, updates V, gives Vpre.
 template <bool SMOOTH>
 __device__ __forceinline__ float lif_step(const Args &a, float &V, float u, float r, float &vpre) {
     const float vp = __fadd_rn(__fadd_rn(__fmul_rn(a.alpha, V), u), r);
@@ -186,7 +219,8 @@ __global__ void __launch_bounds__(512) fwd_kernel(const __grid_constant__ Args a
     const int q = (int)blockIdx.x / CL;
     const int H = a.H, HC = a.HC, R = a.R, B = a.B;
     const int h0 = rank * HC;
-    const FwdSmem L = fwd_smem(H, HC, R, SMOOTH, a.csr_smem != 0, in_cta_max);
+    const bool csr = a.csr_smem != 0;
+    const FwdSmem L = fwd_smem(H, HC, R, SMOOTH, csr, in_cta_max);
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned char *ring = smem + L.ring;
     float *xbuf = reinterpret_cast<float *>(smem + L.xbuf);
@@ -198,78 +232,87 @@ __global__ void __launch_bounds__(512) fwd_kernel(const __grid_constant__ Args a
     for (int k = tid; k < HC * R; k += nthr) wout[k] = a.w_out[(size_t)h0 * R + k];
     const int base = a.in_ptr[h0];
     for (int k = tid; k <= HC; k += nthr) lptr[k] = a.in_ptr[h0 + k] - base;
-    const uint16_t *code = a.in_code + base;
-    const float *wl = a.in_w + base;
+    const uint16_t *gcode = a.in_code + base;
+    const float *gw = a.in_w + base;
     const int n_in = a.in_ptr[h0 + HC] - base;
-    if (a.csr_smem && n_in > in_cta_max && tid == 0) atomicAdd(a.err + 2, 1);  // a wrong in_cta_max: rows stay global
-    if (a.csr_smem && n_in <= in_cta_max) {
-        uint16_t *sc = reinterpret_cast<uint16_t *>(smem + L.code);
-        float *sw = reinterpret_cast<float *>(smem + L.w);
-        for (int k = tid; k < n_in; k += nthr) {
-            sc[k] = code[k];
-            sw[k] = wl[k];
+    const bool in_smem = csr && n_in <= in_cta_max;
+    if (csr && !in_smem && tid == 0) atomicAdd(a.err + 2, 1);  // a wrong in_cta_max: the rows stay global
+    uint16_t *sc = reinterpret_cast<uint16_t *>(smem + L.code);
+    float *sw = reinterpret_cast<float *>(smem + L.w);
+    if (in_smem) {
+        for (int k = tid; k < n_in; k += nthr) {  // validated once: a bad link becomes a zero-weight link
+            const uint32_t c = gcode[k];
+            const bool bad = (c >> 11) < 1 || (c >> 11) > MAXD || (c & 0x7FFu) >= (uint32_t)H;
+            if (bad) atomicAdd(a.err + 0, 1);
+            sc[k] = bad ? (uint16_t)(1u << 11) : (uint16_t)c;
+            sw[k] = bad ? 0.f : gw[k];
         }
-        code = sc;
-        wl = sw;
     }
     __syncthreads();
     cl.sync();  // every CTA's shared memory is initialised before any remote write reaches it
 
-    const bool nt = tid < 2 * HC;
-    const int pl = nt ? tid >> 1 : 0, half = tid & 1;
+    const bool nt = tid < NT * HC;
+    const int pl = nt ? tid / NT : 0, sub = tid % NT;
     const int post = h0 + pl;
     const int rs = nt ? lptr[pl] : 0, re = nt ? lptr[pl + 1] : 0;
-    float V[4] = {0.f, 0.f, 0.f, 0.f};
+    float V0 = 0.f, V1 = 0.f;
     const bool ro = tid < NS * R;
     const int rb = ro ? tid / R : 0, rr = ro ? tid % R : 0;
     float O = 0.f, mx = -INFINITY;
     int ts = -1;
+    const size_t bq = (size_t)q * NS + SPT * sub;  // this thread's first sample
 
     for (int t = 0; t < a.T; ++t) {
         if (a.tape && t % a.K == 0 && nt) {
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                a.v_ckpt[((size_t)(t / a.K) * B + q * NS + 4 * half + j) * H + post] = V[j];
+            a.v_ckpt[((size_t)(t / a.K) * B + bq) * H + post] = V0;
+            a.v_ckpt[((size_t)(t / a.K) * B + bq + 1) * H + post] = V1;
         }
         float acc[NS];
-        gather_in<SMOOTH>(a, ring, code, wl, rs, re, half, t, acc);
-        float s4[4] = {0.f, 0.f, 0.f, 0.f};
-        uint32_t bits = 0;
+        const RingSrc src{ring, H, t % RING};
+        if (in_smem) gather_in<SMOOTH, false>(a, src, sc, sw, rs, re, sub, acc);
+        else gather_in<SMOOTH, true>(a, src, gcode, gw, rs, re, sub, acc);
+        float r0, r1, s0 = 0.f, s1 = 0.f, vp;
+        mine(acc, sub, r0, r1);
         if (nt) {
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int b = 4 * half + j;
-                const float u = __ldg(a.U + ((size_t)t * B + q * NS + b) * H + post);
-                float vp;
-                s4[j] = lif_step<SMOOTH>(a, V[j], u, half ? acc[4 + j] : acc[j], vp);
-                if (s4[j] != 0.f) bits |= 1u << j;
-            }
+            const float u0 = __ldg(a.U + ((size_t)t * B + bq) * H + post);
+            const float u1 = __ldg(a.U + ((size_t)t * B + bq + 1) * H + post);
+            s0 = lif_step<SMOOTH>(a, V0, u0, r0, vp);
+            s1 = lif_step<SMOOTH>(a, V1, u1, r1, vp);
         }
-        const uint32_t other = __shfl_xor_sync(FULL, bits, 1);
         const int slot = t % RING;
-        if (nt) {
-            if constexpr (SMOOTH) {
-                const float4 v = make_float4(s4[0], s4[1], s4[2], s4[3]);
-                float4 *dst = reinterpret_cast<float4 *>(ring) + ((size_t)slot * H + post) * 2 + half;
+        if constexpr (SMOOTH) {
+            if (nt) {
+                const float2 v = make_float2(s0, s1);
+                float2 *dst = reinterpret_cast<float2 *>(ring) + ((size_t)slot * H + post) * 4 + sub;
                 for (int k = 0; k < CL; ++k) *cl.map_shared_rank(dst, k) = v;
-                if (a.tape)
-                    reinterpret_cast<float4 *>(a.s_f)[(((size_t)t * a.NC + q) * H + post) * 2 + half] = v;
-            } else {
-                const uint32_t byte = half ? (other | (bits << 4)) : (bits | (other << 4));
+                if (a.tape) reinterpret_cast<float2 *>(a.s_f)[(((size_t)t * a.NC + q) * H + post) * 4 + sub] = v;
+            }
+        } else {
+            uint32_t bits = ((s0 != 0.f) ? 1u : 0u) | ((s1 != 0.f) ? 2u : 0u);
+            bits <<= SPT * sub;
+            bits |= __shfl_xor_sync(FULL, bits, 1);
+            bits |= __shfl_xor_sync(FULL, bits, 2);
+            if (nt) {
                 unsigned char *dst = ring + (size_t)slot * H + post;
-                for (int k = half; k < CL; k += 2) *cl.map_shared_rank(dst, k) = (unsigned char)byte;
-                if (a.tape && half == 0) a.s_bits[((size_t)t * a.NC + q) * H + post] = (uint8_t)byte;
+                for (int k = sub; k < CL; k += NT) *cl.map_shared_rank(dst, k) = (unsigned char)bits;
+                if (a.tape && sub == 0) a.s_bits[((size_t)t * a.NC + q) * H + post] = (uint8_t)bits;
             }
         }
         __syncthreads();  // this CTA's own neurons' entries are in its ring
         if (ro) {
             float sum = 0.f;
-            for (int p = 0; p < HC; ++p) {
-                float s[NS];
-                uint32_t byte;
-                load_spikes<SMOOTH>(ring, H, slot, h0 + p, s, byte);
-                if constexpr (SMOOTH) sum = __fadd_rn(sum, __fmul_rn(s[rb], wout[p * R + rr]));
-                else if ((byte >> rb) & 1u) sum = __fadd_rn(sum, wout[p * R + rr]);
+            if constexpr (SMOOTH) {
+                const float *rf = reinterpret_cast<const float *>(ring) + ((size_t)slot * H + h0) * NS + rb;
+                for (int p = 0; p < HC; ++p) sum = __fadd_rn(sum, __fmul_rn(rf[(size_t)p * NS], wout[p * R + rr]));
+            } else {  // four neurons' bytes per word, neurons in ascending order
+                const uint32_t *rw = reinterpret_cast<const uint32_t *>(ring + (size_t)slot * H + h0);
+                for (int k = 0; k < HC / 4; ++k) {
+                    const uint32_t word = rw[k];
+                    if (!word) continue;
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        if ((word >> (8 * j + rb)) & 1u) sum = __fadd_rn(sum, wout[(4 * k + j) * R + rr]);
+                }
             }
             float *dst = xbuf + (((size_t)(t & 1) * CL + rank) * NS + rb) * R + rr;
             *cl.map_shared_rank(dst, 0) = sum;
@@ -292,20 +335,70 @@ __global__ void __launch_bounds__(512) fwd_kernel(const __grid_constant__ Args a
     cl.sync();  // no CTA leaves while another may still address its shared memory
 }
 
-// ------------------------------------------------------------------------------------------------ backward
+// ------------------------------------------------------------------------------------------------ recompute
 
+// The recurrent input R of every step of a segment [t0, t1) from the stored spikes: NT threads per
+// (step, cluster, neuron), the forward's link split and addition order (the same sums bit for bit).
 template <bool SMOOTH>
-__global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a, int out_cta_max) {
+__global__ void __launch_bounds__(256) recompute_r_kernel(const __grid_constant__ Args a, int t0, int t1) {
+    const size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t per_t = (size_t)a.NC * a.H * NT;
+    const bool live = gid < (size_t)(t1 - t0) * per_t;  // whole groups of NT lanes live or not together
+    const size_t g = live ? gid : 0;
+    const int t = t0 + (int)(g / per_t);
+    const int rem = (int)(g % per_t);
+    const int q = rem / (a.H * NT), post = (rem / NT) % a.H, sub = rem % NT;
+    const TapeSrc src{a.s_bits, a.s_f, a.H, a.NC, q, t};
+    const int rs = live ? a.in_ptr[post] : 0, re = live ? a.in_ptr[post + 1] : 0;
+    float acc[NS];
+    gather_in<SMOOTH, true>(a, src, a.in_code, a.in_w, rs, re, sub, acc);
+    if (!live) return;
+    float r0, r1;
+    mine(acc, sub, r0, r1);
+    const size_t b = (size_t)q * NS + SPT * sub;
+    a.g_seg[((size_t)(t - t0) * a.B + b) * a.H + post] = r0;
+    a.g_seg[((size_t)(t - t0) * a.B + b + 1) * a.H + post] = r1;
+}
+
+// The membrane of the segment from its checkpoint, one thread per (sample, neuron): Vpre as the forward made it,
+// its surrogate derivative over R in g_seg, and a check that the stored spike is the one Vpre gives.
+template <bool SMOOTH>
+__global__ void __launch_bounds__(256) recompute_v_kernel(const __grid_constant__ Args a, int seg, int t0, int t1) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.B * a.H) return;
+    const int b = k / a.H, j = k % a.H, q = b / NS, bl = b % NS;
+    float V = a.v_ckpt[(size_t)seg * a.B * a.H + k];
+    int bad = 0;
+    for (int t = t0; t < t1; ++t) {
+        float *gp = a.g_seg + (size_t)(t - t0) * a.B * a.H + k;
+        const float u = __ldg(a.U + (size_t)t * a.B * a.H + k);
+        float vp;
+        const float s = lif_step<SMOOTH>(a, V, u, *gp, vp);
+        float stored;
+        if constexpr (SMOOTH) stored = a.s_f[(((size_t)t * a.NC + q) * a.H + j) * NS + bl];
+        else stored = ((a.s_bits[((size_t)t * a.NC + q) * a.H + j] >> bl) & 1u) ? 1.f : 0.f;
+        bad += s != stored;
+        *gp = surrogate(__fadd_rn(vp, -a.theta), a.slope);
+    }
+    if (bad) atomicAdd(a.err + 1, bad);  // the recompute differs from the forward
+}
+
+// ------------------------------------------------------------------------------------------------ adjoint
+
+// The adjoint of segment [t0, t1), run backwards; `first`: the last segment of the sequence (state starts at
+// zero), else the state of the segment after it is loaded (partial ring, q, readout adjoint, dw, dw_out).
+template <bool SMOOTH>
+__global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a, int out_cta_max, int t0, int t1,
+                                                   int first) {
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
     const int q = (int)blockIdx.x / CL;
-    const int H = a.H, HC = a.HC, R = a.R, B = a.B, T = a.T, K = a.K;
+    const int H = a.H, HC = a.HC, R = a.R, B = a.B;
     const int h0 = rank * HC;
-    const BwdSmem L = bwd_smem(H, HC, R, SMOOTH, out_cta_max);
+    const BwdSmem L = bwd_smem(H, HC, R, out_cta_max);
     extern __shared__ __align__(16) unsigned char smem[];
     float *pnew = reinterpret_cast<float *>(smem + L.pnew);
     float *part = reinterpret_cast<float *>(smem + L.part);
-    unsigned char *ring = smem + L.ring;
     float *wout = reinterpret_cast<float *>(smem + L.wout);
     float *dwo = reinterpret_cast<float *>(smem + L.dwo);
     float *obuf = reinterpret_cast<float *>(smem + L.obuf);
@@ -313,6 +406,7 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
     uint16_t *ocode = reinterpret_cast<uint16_t *>(smem + L.code);
     float *dw = reinterpret_cast<float *>(smem + L.dw);
     const int tid = threadIdx.x, nthr = blockDim.x;
+    float *part_st = a.part_st + (size_t)blockIdx.x * RING * HC * NS;
 
     const int obase = a.out_grp[(size_t)h0 * (MAXD + 1)];
     const int on_all = a.out_grp[(size_t)(h0 + HC - 1) * (MAXD + 1) + MAXD] - obase;
@@ -322,21 +416,30 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
     for (int k = tid; k < HC * R; k += nthr) wout[k] = a.w_out[(size_t)h0 * R + k];
     for (int k = tid; k < HC * (MAXD + 1); k += nthr) grp[k] = a.out_grp[(size_t)h0 * (MAXD + 1) + k] - obase;
     for (int k = tid; k < on; k += nthr) ocode[k] = a.out_code[obase + k];
+    if (!first) {
+        for (int k = tid; k < RING * HC * NS; k += nthr) part[k] = part_st[k];
+        for (int k = tid; k < on; k += nthr) dw[k] = a.dwp[(size_t)q * a.nnz + obase + k];
+        for (int k = tid; k < HC * R; k += nthr) dwo[k] = a.dwo_p[((size_t)q * H + h0) * R + k];
+    }
     const float *ow = a.out_w + obase;
     __syncthreads();
     cl.sync();
 
-    const bool nt = tid < 2 * HC;
-    const int pl = nt ? tid >> 1 : 0, half = tid & 1;
-    const int me = h0 + pl;  // this thread's neuron (post of its incoming row, pre of its outgoing row)
-    const int irs = nt ? a.in_ptr[me] : 0, ire = nt ? a.in_ptr[me + 1] : 0;
+    const bool nt = tid < NT * HC;
+    const int pl = nt ? tid / NT : 0, sub = tid % NT;
+    const int me = h0 + pl;  // this thread's neuron (the pre of its outgoing row)
+    const size_t bq = (size_t)q * NS + SPT * sub;
     const bool ro = tid < NS * R;
     const int rb = ro ? tid / R : 0, rr = ro ? tid % R : 0;
     const float dmv = ro ? a.dm[(size_t)(q * NS + rb) * R + rr] : 0.f;
     const int tsv = ro ? a.tstar_in[(size_t)(q * NS + rb) * R + rr] : -1;
-    float o = 0.f;
-    float pprev[4] = {0.f, 0.f, 0.f, 0.f};
-    const int R2 = (R + 1) / 2;
+    float o = (ro && !first) ? a.o_st[(size_t)(q * NS + rb) * R + rr] : 0.f;
+    float qp0 = 0.f, qp1 = 0.f;  // q[t + 1] of this thread's two samples
+    if (nt && !first) {
+        qp0 = a.q_st[bq * H + me];
+        qp1 = a.q_st[(bq + 1) * H + me];
+    }
+    const int R4 = (R + NT - 1) / NT;
 
     // this neuron's 8 samples' spikes at step tt (0 before step 0): a byte of bits, or floats in the smooth model
     auto spikes_at = [&](int tt, float out[NS], uint32_t &byte) {
@@ -356,177 +459,124 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
             byte = a.s_bits[((size_t)tt * a.NC + q) * H + me];
         }
     };
-
-    for (int seg = a.nseg - 1; seg >= 0; --seg) {
-        const int t0 = seg * K, t1 = min(T, t0 + K);
-        // ---- recompute the segment from its checkpoint (no cluster barrier: every spike is stored)
-        float V[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            V[j] = nt ? a.v_ckpt[((size_t)seg * B + q * NS + 4 * half + j) * H + me] : 0.f;
-        __syncthreads();  // the previous use of the ring is over
-        for (int d = 1; d <= MAXD; ++d) {
-            const int tt = t0 - d, slot = ((tt % RING) + RING) % RING;
-            for (int j = tid; j < H; j += nthr) {
-                if constexpr (SMOOTH) {
-                    float4 *dst = reinterpret_cast<float4 *>(ring) + ((size_t)slot * H + j) * 2;
-                    if (tt >= 0) {
-                        const float4 *src = reinterpret_cast<const float4 *>(a.s_f) + (((size_t)tt * a.NC + q) * H + j) * 2;
-                        dst[0] = src[0];
-                        dst[1] = src[1];
-                    } else {
-                        dst[0] = dst[1] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    }
-                } else {
-                    ring[(size_t)slot * H + j] = tt >= 0 ? a.s_bits[((size_t)tt * a.NC + q) * H + j] : 0;
-                }
-            }
+    uint64_t hist = 0;      // spiking: byte d - 1 = the 8 samples' spikes at t - d
+    float histf[MAXD][NS];  // smooth: histf[d - 1] = spikes at t - d
+    for (int d = 1; d <= MAXD; ++d) {
+        uint32_t byte;
+        spikes_at(t1 - 1 - d, histf[d - 1], byte);
+        if constexpr (!SMOOTH) hist |= (uint64_t)byte << (8 * (d - 1));
+    }
+    for (int t = t1 - 1; t >= t0; --t) {
+        if (ro) {
+            o = __fadd_rn(t == tsv ? dmv : 0.f, __fmul_rn(a.beta, o));
+            obuf[rb * R + rr] = o;
         }
-        __syncthreads();
-        for (int t = t0; t < t1; ++t) {
-            if (t > t0) {  // S[t - 1] into its slot (it replaces S[t - 7], no longer read)
-                const int tt = t - 1, slot = tt % RING;
-                for (int j = tid; j < H; j += nthr) {
-                    if constexpr (SMOOTH) {
-                        const float4 *src = reinterpret_cast<const float4 *>(a.s_f) + (((size_t)tt * a.NC + q) * H + j) * 2;
-                        float4 *dst = reinterpret_cast<float4 *>(ring) + ((size_t)slot * H + j) * 2;
-                        dst[0] = src[0];
-                        dst[1] = src[1];
-                    } else {
-                        ring[(size_t)slot * H + j] = a.s_bits[((size_t)tt * a.NC + q) * H + j];
-                    }
-                }
-                __syncthreads();
-            }
-            float acc[NS];
-            gather_in<SMOOTH>(a, ring, a.in_code, a.in_w, irs, ire, half, t, acc);
-            if (nt) {
-                float st[NS];
-                uint32_t byte;
-                spikes_at(t, st, byte);
+        __syncthreads();  // obuf ready; the previous step's partial-ring writes done
+        if (nt) {
+            float qv[SPT];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int b = 4 * half + j;
-                    const float u = __ldg(a.U + ((size_t)t * B + q * NS + b) * H + me);
-                    float vp;
-                    const float s = lif_step<SMOOTH>(a, V[j], u, half ? acc[4 + j] : acc[j], vp);
-                    float stored;
-                    if constexpr (SMOOTH) stored = half ? st[4 + j] : st[j];
-                    else stored = ((byte >> b) & 1u) ? 1.f : 0.f;
-                    if (s != stored) atomicAdd(a.err + 1, 1);  // the replay differs from the forward
-                    a.g_seg[((size_t)(t - t0) * B + q * NS + b) * H + me] = surrogate(__fadd_rn(vp, -a.theta), a.slope);
-                }
+            for (int j = 0; j < SPT; ++j) {
+                const int bl = SPT * sub + j;
+                float *pp = part + ((size_t)(t % RING) * HC + pl) * NS + bl;
+                float sh = *pp;
+                for (int r = 0; r < R; ++r) sh = __fadd_rn(sh, __fmul_rn(wout[pl * R + r], obuf[bl * R + r]));
+                *pp = 0.f;
+                const float g = a.g_seg[((size_t)(t - t0) * B + bq + j) * H + me];
+                const float ap = __fmul_rn(a.alpha, j ? qp1 : qp0);
+                qv[j] = __fadd_rn(ap, __fmul_rn(g, __fadd_rn(sh, -__fmul_rn(a.theta, ap))));
+                a.dU[((size_t)t * B + bq + j) * H + me] = qv[j];
             }
-        }
-        // ---- the segment backwards
-        // this neuron's spikes at t - 1 .. t - 5 (for its outgoing links' dw), shifted in as t falls
-        uint64_t hist = 0;      // spiking: byte d - 1 = the 8 samples' spikes at t - d
-        float histf[MAXD][NS];  // smooth: histf[d - 1] = spikes at t - d
-        for (int d = 1; d <= MAXD; ++d) {
+            qp0 = qv[0];
+            qp1 = qv[1];
+            const float2 v = make_float2(qv[0], qv[1]);
+            float2 *dst = reinterpret_cast<float2 *>(pnew) + ((size_t)(t & 1) * H + me) * 4 + sub;
+            for (int k = 0; k < CL; ++k) *cl.map_shared_rank(dst, k) = v;
+            // dw_out: this neuron's spikes at t times o[t]; each of its NT threads takes a quarter of the readouts
+            float st[NS];
             uint32_t byte;
-            spikes_at(t1 - 1 - d, histf[d - 1], byte);
-            if constexpr (!SMOOTH) hist |= (uint64_t)byte << (8 * (d - 1));
+            spikes_at(t, st, byte);
+            if (byte) {
+                for (int r = sub * R4; r < min(R, (sub + 1) * R4); ++r) {
+                    float acc = dwo[pl * R + r];
+                    for (int b = 0; b < NS; ++b) {
+                        if constexpr (SMOOTH) acc = __fadd_rn(acc, __fmul_rn(st[b], obuf[b * R + r]));
+                        else if ((byte >> b) & 1u) acc = __fadd_rn(acc, obuf[b * R + r]);
+                    }
+                    dwo[pl * R + r] = acc;
+                }
+            }
         }
-        for (int t = t1 - 1; t >= t0; --t) {
-            if (ro) {
-                o = __fadd_rn(t == tsv ? dmv : 0.f, __fmul_rn(a.beta, o));
-                obuf[rb * R + rr] = o;
-            }
-            __syncthreads();  // obuf ready; the previous step's partial-ring writes done
-            if (nt) {
-                float qv[4];
+        cl.sync();  // q[t] of every neuron in every CTA's pnew[t & 1]
+        // outgoing rows: partial[t - d] += w q[t][post]; dw += s[t - d][me] q[t][post]
+        const float *pn = pnew + (size_t)(t & 1) * H * NS;
+        for (int d = 1; d <= MAXD; ++d) {
+            float acc[NS];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int b = 4 * half + j;
-                    float *pp = part + ((size_t)(t % RING) * HC + pl) * NS + b;
-                    float sh = *pp;
-                    for (int r = 0; r < R; ++r) sh = __fadd_rn(sh, __fmul_rn(wout[pl * R + r], obuf[b * R + r]));
-                    *pp = 0.f;
-                    const float g = a.g_seg[((size_t)(t - t0) * B + q * NS + b) * H + me];
-                    const float ap = __fmul_rn(a.alpha, pprev[j]);
-                    qv[j] = __fadd_rn(ap, __fmul_rn(g, __fadd_rn(sh, -__fmul_rn(a.theta, ap))));
-                    pprev[j] = qv[j];
-                    a.dU[((size_t)t * B + q * NS + b) * H + me] = qv[j];
+            for (int b = 0; b < NS; ++b) acc[b] = 0.f;
+            const int gs = nt ? grp[pl * (MAXD + 1) + d - 1] : 0, ge = nt ? grp[pl * (MAXD + 1) + d] : 0;
+            const uint32_t sbyte = SMOOTH ? 0xffu : (uint32_t)((hist >> (8 * (d - 1))) & 0xffu);
+#pragma unroll 2
+            for (int l = gs + sub; l < ge; l += NT) {
+                if (l >= on) {
+                    atomicAdd(a.err + 2, 1);
+                    continue;
                 }
-                const float4 v = make_float4(qv[0], qv[1], qv[2], qv[3]);
-                float4 *dst = reinterpret_cast<float4 *>(pnew) + ((size_t)(t & 1) * H + me) * 2 + half;
-                for (int k = 0; k < CL; ++k) *cl.map_shared_rank(dst, k) = v;
-                // dw_out: this neuron's spikes at t times o[t]; each half takes half of the readouts
-                float st[NS];
-                uint32_t byte;
-                spikes_at(t, st, byte);
-                if (byte) {
-                    for (int r = half * R2; r < min(R, (half + 1) * R2); ++r) {
-                        float acc = dwo[pl * R + r];
-                        for (int b = 0; b < NS; ++b) {
-                            if constexpr (SMOOTH) acc = __fadd_rn(acc, __fmul_rn(st[b], obuf[b * R + r]));
-                            else if ((byte >> b) & 1u) acc = __fadd_rn(acc, obuf[b * R + r]);
-                        }
-                        dwo[pl * R + r] = acc;
+                const uint32_t c = ocode[l];
+                const int post = (int)(c & 0x7FFu);
+                const float wl = __ldg(ow + l);
+                if ((int)(c >> 11) != d || post >= H) {
+                    atomicAdd(a.err + 0, 1);
+                    continue;
+                }
+                const float4 x0 = reinterpret_cast<const float4 *>(pn)[(size_t)post * 2];
+                const float4 x1 = reinterpret_cast<const float4 *>(pn)[(size_t)post * 2 + 1];
+                const float x[NS] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+#pragma unroll
+                for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __fmul_rn(wl, x[b]));
+                if (sbyte) {
+                    float dk = 0.f;
+#pragma unroll
+                    for (int b = 0; b < NS; ++b) {
+                        if constexpr (SMOOTH) dk = __fadd_rn(dk, __fmul_rn(histf[d - 1][b], x[b]));
+                        else if ((sbyte >> b) & 1u) dk = __fadd_rn(dk, x[b]);
                     }
+                    dw[l] = __fadd_rn(dw[l], dk);
                 }
             }
-            cl.sync();  // q[t] of every neuron in every CTA's pnew[t & 1]
-            // outgoing rows: partial[t - d] += w q[t][post]; dw += s[t - d][me] q[t][post]
-            const float *pn = pnew + (size_t)(t & 1) * H * NS;
+#pragma unroll
+            for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __shfl_xor_sync(FULL, acc[b], 1));
+#pragma unroll
+            for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __shfl_xor_sync(FULL, acc[b], 2));
+            if (nt && t - d >= 0) {
+                float x0, x1;
+                mine(acc, sub, x0, x1);
+                float *pp = part + ((size_t)((t - d) % RING) * HC + pl) * NS + SPT * sub;
+                pp[0] = __fadd_rn(pp[0], x0);
+                pp[1] = __fadd_rn(pp[1], x1);
+            }
+        }
+        // the spike history of step t - 1: delays 1..5 reach t - 2 .. t - 6
+        if constexpr (SMOOTH) {
             for (int d = 1; d <= MAXD; ++d) {
-                float acc[NS];
-#pragma unroll
-                for (int b = 0; b < NS; ++b) acc[b] = 0.f;
-                const int gs = nt ? grp[pl * (MAXD + 1) + d - 1] : 0, ge = nt ? grp[pl * (MAXD + 1) + d] : 0;
-                const uint32_t sbyte = SMOOTH ? 0xffu : (uint32_t)((hist >> (8 * (d - 1))) & 0xffu);
-                for (int l = gs + half; l < ge; l += 2) {
-                    if (l >= on) {
-                        atomicAdd(a.err + 2, 1);
-                        continue;
-                    }
-                    const uint32_t c = ocode[l];
-                    const int post = (int)(c & 0x7FFu);
-                    if ((int)(c >> 11) != d || post >= H) {
-                        atomicAdd(a.err + 0, 1);
-                        continue;
-                    }
-                    const float wl = __ldg(ow + l);
-                    const float4 x0 = reinterpret_cast<const float4 *>(pn)[(size_t)post * 2];
-                    const float4 x1 = reinterpret_cast<const float4 *>(pn)[(size_t)post * 2 + 1];
-                    const float x[NS] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-#pragma unroll
-                    for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __fmul_rn(wl, x[b]));
-                    if (sbyte) {
-                        float dk = 0.f;
-#pragma unroll
-                        for (int b = 0; b < NS; ++b) {
-                            if constexpr (SMOOTH) dk = __fadd_rn(dk, __fmul_rn(histf[d - 1][b], x[b]));
-                            else if ((sbyte >> b) & 1u) dk = __fadd_rn(dk, x[b]);
-                        }
-                        dw[l] = __fadd_rn(dw[l], dk);
-                    }
-                }
-#pragma unroll
-                for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __shfl_xor_sync(FULL, acc[b], 1));
-                if (nt && t - d >= 0) {
-                    float *pp = part + ((size_t)((t - d) % RING) * HC + pl) * NS + 4 * half;
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) pp[j] = __fadd_rn(pp[j], half ? acc[4 + j] : acc[j]);
-                }
-            }
-            // the spike history of step t - 1: delays 1..5 reach t - 2 .. t - 6
-            if constexpr (SMOOTH) {
-                for (int d = 1; d <= MAXD; ++d) {
-                    uint32_t byte;
-                    spikes_at(t - 1 - d, histf[d - 1], byte);
-                }
-            } else {
                 uint32_t byte;
-                spikes_at(t - 1 - MAXD, histf[0], byte);
-                hist = (hist >> 8) | ((uint64_t)byte << (8 * (MAXD - 1)));
+                spikes_at(t - 1 - d, histf[d - 1], byte);
             }
+        } else {
+            uint32_t byte;
+            spikes_at(t - 1 - MAXD, histf[0], byte);
+            hist = (hist >> 8) | ((uint64_t)byte << (8 * (MAXD - 1)));
         }
     }
+    // the state for the segment before this one
     __syncthreads();
-    if (nt && half == 0)
-        for (int r = 0; r < R; ++r) a.dwo_p[((size_t)q * H + me) * R + r] = dwo[pl * R + r];
+    for (int k = tid; k < RING * HC * NS; k += nthr) part_st[k] = part[k];
     for (int k = tid; k < on; k += nthr) a.dwp[(size_t)q * a.nnz + obase + k] = dw[k];
+    for (int k = tid; k < HC * R; k += nthr) a.dwo_p[((size_t)q * H + h0) * R + k] = dwo[k];
+    if (nt) {
+        a.q_st[bq * H + me] = qp0;
+        a.q_st[(bq + 1) * H + me] = qp1;
+    }
+    if (ro && rank == 0) a.o_st[(size_t)(q * NS + rb) * R + rr] = o;
     cl.sync();
 }
 
@@ -575,7 +625,7 @@ int bcuda(cudaError_t e, const char *what) {
     } while (0)
 
 struct WsLayout {
-    size_t spikes, vck, gseg, outw, dwp, dwo, err, total;
+    size_t spikes, vck, gseg, outw, dwp, dwo, part, qst, ost, err, total;
 };
 
 size_t a256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -583,8 +633,8 @@ size_t a256(size_t x) { return (x + 255) & ~size_t(255); }
 int check_desc(const n2b_bptt_desc *d) {
     if (!d) return bfail(N2B_EINVAL, "desc is NULL");
     if (d->batch <= 0 || d->batch % NS) return bfail(N2B_EINVAL, "batch must be a positive multiple of 8");
-    if (d->hidden <= 0 || d->hidden % CL || d->hidden > 2048)
-        return bfail(N2B_EINVAL, "hidden must be a multiple of 8, at most 2048");
+    if (d->hidden <= 0 || d->hidden % 32 || d->hidden > 1024)
+        return bfail(N2B_EINVAL, "hidden must be a multiple of 32, at most 1024");
     if (d->readouts <= 0 || d->readouts > 32) return bfail(N2B_EINVAL, "readouts must be in 1..32");
     if (d->steps <= 0 || d->checkpoint <= 0) return bfail(N2B_EINVAL, "steps and checkpoint must be positive");
     if (d->smooth && d->hidden > 256) return bfail(N2B_EINVAL, "the smooth model is for hidden <= 256");
@@ -606,13 +656,16 @@ WsLayout ws_layout(const n2b_bptt_desc *d) {
     L.outw = o; o = a256(o + sizeof(float) * std::max<size_t>(d->nnz, 1));
     L.dwp = o; o = a256(o + sizeof(float) * NC * std::max<size_t>(d->nnz, 1));
     L.dwo = o; o = a256(o + sizeof(float) * NC * H * R);
+    L.part = o; o = a256(o + sizeof(float) * NC * CL * RING * (H / CL) * NS);
+    L.qst = o; o = a256(o + sizeof(float) * B * H);
+    L.ost = o; o = a256(o + sizeof(float) * B * R);
     L.err = o; o = a256(o + sizeof(int32_t) * N2B_BPTT_ERR_WORDS);
     L.total = o;
     return L;
 }
 
 int threads_of(const n2b_bptt_desc *d) {
-    const int n = std::max(2 * (d->hidden / CL), NS * d->readouts);
+    const int n = std::max(NT * (d->hidden / CL), NS * d->readouts);
     return (n + 31) / 32 * 32;
 }
 
@@ -642,6 +695,9 @@ Args args_of(const n2b_bptt_desc *d, char *ws, const WsLayout &L) {
     a.out_w = reinterpret_cast<float *>(ws + L.outw);
     a.dwp = reinterpret_cast<float *>(ws + L.dwp);
     a.dwo_p = reinterpret_cast<float *>(ws + L.dwo);
+    a.part_st = reinterpret_cast<float *>(ws + L.part);
+    a.q_st = reinterpret_cast<float *>(ws + L.qst);
+    a.o_st = reinterpret_cast<float *>(ws + L.ost);
     a.err = reinterpret_cast<int32_t *>(ws + L.err);
     return a;
 }
@@ -655,8 +711,8 @@ int check_ws(const n2b_bptt_desc *d, void *ws, size_t bytes, WsLayout &L) {
     return N2B_OK;
 }
 
-template <class Kern>
-int launch_cluster(Kern kern, int grid, int threads, size_t smem, cudaStream_t s, const Args &a, int extra) {
+template <class Kern, class... Rest>
+int launch_cluster(Kern kern, int grid, int threads, size_t smem, cudaStream_t s, const Args &a, Rest... rest) {
     if (smem > 227 * 1024) return bfail(N2B_EINVAL, "shared memory need " + std::to_string(smem) + " bytes > 227 KiB");
     B_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     cudaLaunchConfig_t cfg = {};
@@ -674,7 +730,7 @@ int launch_cluster(Kern kern, int grid, int threads, size_t smem, cudaStream_t s
     int clusters = 0;
     B_CUDA(cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg));
     if (clusters < 1) return bfail(N2B_ECUDA, "a cluster of 8 CTAs of this size cannot be resident");
-    B_CUDA(cudaLaunchKernelEx(&cfg, kern, a, extra));
+    B_CUDA(cudaLaunchKernelEx(&cfg, kern, a, rest...));
     return N2B_OK;
 }
 
@@ -738,11 +794,26 @@ int n2b_bptt_backward(const n2b_bptt_desc *d, const float *u, const float *w_rec
         B_CUDA(cudaGetLastError());
     }
     const bool smooth = d->smooth != 0;
-    const BwdSmem S = bwd_smem(d->hidden, d->hidden / CL, d->readouts, smooth, d->out_cta_max);
+    const BwdSmem S = bwd_smem(d->hidden, d->hidden / CL, d->readouts, d->out_cta_max);
     const int grid = (d->batch / NS) * CL, threads = threads_of(d);
-    rc = smooth ? launch_cluster(bwd_kernel<true>, grid, threads, S.total, s, a, d->out_cta_max)
-                : launch_cluster(bwd_kernel<false>, grid, threads, S.total, s, a, d->out_cta_max);
-    if (rc) return rc;
+    const int K = d->checkpoint, nseg = a.nseg;
+    for (int seg = nseg - 1; seg >= 0; --seg) {  // each segment: recompute from its checkpoint, then backwards
+        const int t0 = seg * K, t1 = std::min(d->steps, t0 + K);
+        const size_t nr = (size_t)(t1 - t0) * (d->batch / NS) * d->hidden * NT;
+        const unsigned rblocks = (unsigned)((nr + 255) / 256), vblocks = (unsigned)((d->batch * d->hidden + 255) / 256);
+        if (smooth) {
+            recompute_r_kernel<true><<<rblocks, 256, 0, s>>>(a, t0, t1);
+            recompute_v_kernel<true><<<vblocks, 256, 0, s>>>(a, seg, t0, t1);
+        } else {
+            recompute_r_kernel<false><<<rblocks, 256, 0, s>>>(a, t0, t1);
+            recompute_v_kernel<false><<<vblocks, 256, 0, s>>>(a, seg, t0, t1);
+        }
+        B_CUDA(cudaGetLastError());
+        const int first = seg == nseg - 1;
+        rc = smooth ? launch_cluster(bwd_kernel<true>, grid, threads, S.total, s, a, d->out_cta_max, t0, t1, first)
+                    : launch_cluster(bwd_kernel<false>, grid, threads, S.total, s, a, d->out_cta_max, t0, t1, first);
+        if (rc) return rc;
+    }
     const int NC = d->batch / NS;
     if (d->nnz > 0) {
         reduce_dw_kernel<<<(d->nnz + 255) / 256, 256, 0, s>>>(a.dwp, d->out_perm, d->nnz, NC, dw_rec);
