@@ -110,24 +110,32 @@ __host__ __device__ inline FwdSmem fwd_smem(int H, int HC, int R, bool smooth, b
     return L;
 }
 
+constexpr int QROW = 12;  // floats per neuron in the q exchange buffer: 8 samples, padded for the banks
+
 struct BwdSmem {
-    size_t pnew, part, wout, dwo, obuf, grp, code, dw, total;
+    size_t pnew, part, dwo, obuf, grp, code, w, dw, total;
 };
 __host__ __device__ inline BwdSmem bwd_smem(int H, int HC, int R, int out_cta_max) {
     BwdSmem L{};
     size_t o = 0;
     auto a16 = [](size_t x) { return (x + 15) & ~size_t(15); };
-    L.pnew = o; o = a16(o + sizeof(float) * 2 * H * NS);
+    L.pnew = o; o = a16(o + sizeof(float) * H * QROW);
     L.part = o; o = a16(o + sizeof(float) * RING * HC * NS);
-    L.wout = o; o = a16(o + sizeof(float) * HC * R);
     L.dwo = o; o = a16(o + sizeof(float) * HC * R);
     L.obuf = o; o = a16(o + sizeof(float) * NS * R);
     L.grp = o; o = a16(o + sizeof(int32_t) * HC * (MAXD + 1));
     L.code = o; o = a16(o + sizeof(uint16_t) * out_cta_max);
+    L.w = o; o = a16(o + sizeof(float) * out_cta_max);
     L.dw = o; o = a16(o + sizeof(float) * out_cta_max);
     L.total = o;
     return L;
 }
+
+// The two halves of a cluster barrier (every thread of every CTA of the cluster, the same number of times):
+// arrive orders this thread's earlier memory accesses (release), wait returns once every thread has arrived
+// and makes their earlier writes visible (acquire).
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
 
 // The spikes that the incoming links read: the forward's shared-memory ring (6 slots, the slot of step t in
 // t mod 6; slots of steps before 0 are still zero), or the stored spikes of every step (recompute).
@@ -385,8 +393,41 @@ __global__ void __launch_bounds__(256) recompute_v_kernel(const __grid_constant_
 
 // ------------------------------------------------------------------------------------------------ adjoint
 
+// One delay group of a neuron's outgoing row at step t: acc[b] += w q[t][post][b] over this thread's share
+// of the links; with DW (the neuron spiked at t - d in some sample), also dw[l] += sum_b s[b] q[t][post][b].
+// Without DW the loop stores nothing, so the loads of later links are not held behind earlier stores.
+template <bool SMOOTH, bool DW>
+__device__ __forceinline__ void out_group(const uint16_t *ocode, const float *ow, const float *pnew, float *dw,
+                                          int gs, int ge, int sub, uint32_t sbyte, const float *sf, float acc[NS]) {
+#pragma unroll 4
+    for (int l = gs + sub; l < ge; l += NT) {
+        const uint32_t c = ocode[l];
+        if (c == 0xFFFFu) continue;
+        const float wl = ow[l];
+        const size_t post = c & 0x7FFu;  // < H: checked when the rows were copied
+        const float4 y0 = reinterpret_cast<const float4 *>(pnew)[post * (QROW / 4)];
+        const float4 y1 = reinterpret_cast<const float4 *>(pnew)[post * (QROW / 4) + 1];
+        const float x[NS] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
+#pragma unroll
+        for (int b = 0; b < NS; ++b) acc[b] = __fmaf_rn(wl, x[b], acc[b]);
+        if constexpr (DW) {
+            float dk = 0.f;
+#pragma unroll
+            for (int b = 0; b < NS; ++b) {
+                if constexpr (SMOOTH) dk = __fmaf_rn(sf[b], x[b], dk);
+                else if ((sbyte >> b) & 1u) dk = __fadd_rn(dk, x[b]);
+            }
+            dw[l] = __fadd_rn(dw[l], dk);
+        }
+    }
+}
+
 // The adjoint of segment [t0, t1), run backwards; `first`: the last segment of the sequence (state starts at
 // zero), else the state of the segment after it is loaded (partial ring, q, readout adjoint, dw, dw_out).
+// q[t] of all neurons goes through one shared buffer per CTA (pnew), guarded by two cluster barrier phases
+// per step: after the writes (every q[t] in place before any CTA reads it) and after the reads (no CTA
+// overwrites pnew with q[t - 1] while another still reads q[t]); the second phase's wait comes after the
+// next step's local work, so that it rarely waits.
 template <bool SMOOTH>
 __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a, int out_cta_max, int t0, int t1,
                                                    int first) {
@@ -399,35 +440,50 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
     extern __shared__ __align__(16) unsigned char smem[];
     float *pnew = reinterpret_cast<float *>(smem + L.pnew);
     float *part = reinterpret_cast<float *>(smem + L.part);
-    float *wout = reinterpret_cast<float *>(smem + L.wout);
+    const float *wout = a.w_out + (size_t)h0 * R;  // read through L1
     float *dwo = reinterpret_cast<float *>(smem + L.dwo);
     float *obuf = reinterpret_cast<float *>(smem + L.obuf);
     int32_t *grp = reinterpret_cast<int32_t *>(smem + L.grp);
     uint16_t *ocode = reinterpret_cast<uint16_t *>(smem + L.code);
+    float *ow = reinterpret_cast<float *>(smem + L.w);
     float *dw = reinterpret_cast<float *>(smem + L.dw);
     const int tid = threadIdx.x, nthr = blockDim.x;
     float *part_st = a.part_st + (size_t)blockIdx.x * RING * HC * NS;
 
+    const bool nt = tid < NT * HC;
+    const int pl = nt ? tid / NT : 0, sub = tid % NT;
+    const int me = h0 + pl;  // this thread's neuron (the pre of its outgoing row)
     const int obase = a.out_grp[(size_t)h0 * (MAXD + 1)];
     const int on_all = a.out_grp[(size_t)(h0 + HC - 1) * (MAXD + 1) + MAXD] - obase;
     const int on = min(on_all, out_cta_max);  // a wrong out_cta_max: the links past it are skipped, counted
+    if (on_all > on && tid == 0) atomicAdd(a.err + 2, 1);
     for (size_t k = tid; k < L.total / 4; k += nthr) reinterpret_cast<uint32_t *>(smem)[k] = 0u;
     __syncthreads();
-    for (int k = tid; k < HC * R; k += nthr) wout[k] = a.w_out[(size_t)h0 * R + k];
-    for (int k = tid; k < HC * (MAXD + 1); k += nthr) grp[k] = a.out_grp[(size_t)h0 * (MAXD + 1) + k] - obase;
-    for (int k = tid; k < on; k += nthr) ocode[k] = a.out_code[obase + k];
+    for (int k = tid; k < HC * (MAXD + 1); k += nthr) grp[k] = min(a.out_grp[(size_t)h0 * (MAXD + 1) + k] - obase, on);
+    // the outgoing rows, validated once: a link whose target is out of range or whose delay is not its group's
+    // becomes the code 0xFFFF (skipped) and is counted
+    if (nt) {
+        for (int d = 1; d <= MAXD; ++d) {
+            const int gs = min(a.out_grp[(size_t)me * (MAXD + 1) + d - 1] - obase, on);
+            const int ge = min(a.out_grp[(size_t)me * (MAXD + 1) + d] - obase, on);
+            for (int l = gs + sub; l < ge; l += NT) {
+                const uint32_t c = a.out_code[obase + l];
+                const bool bad = (int)(c >> 11) != d || (c & 0x7FFu) >= (uint32_t)H;
+                if (bad) atomicAdd(a.err + 0, 1);
+                ocode[l] = bad ? (uint16_t)0xFFFFu : (uint16_t)c;
+                ow[l] = a.out_w[obase + l];
+            }
+        }
+    }
     if (!first) {
         for (int k = tid; k < RING * HC * NS; k += nthr) part[k] = part_st[k];
         for (int k = tid; k < on; k += nthr) dw[k] = a.dwp[(size_t)q * a.nnz + obase + k];
         for (int k = tid; k < HC * R; k += nthr) dwo[k] = a.dwo_p[((size_t)q * H + h0) * R + k];
     }
-    const float *ow = a.out_w + obase;
     __syncthreads();
     cl.sync();
+    cluster_arrive();  // the "reads done" phase of the step before the first
 
-    const bool nt = tid < NT * HC;
-    const int pl = nt ? tid / NT : 0, sub = tid % NT;
-    const int me = h0 + pl;  // this thread's neuron (the pre of its outgoing row)
     const size_t bq = (size_t)q * NS + SPT * sub;
     const bool ro = tid < NS * R;
     const int rb = ro ? tid / R : 0, rr = ro ? tid % R : 0;
@@ -466,83 +522,75 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
         spikes_at(t1 - 1 - d, histf[d - 1], byte);
         if constexpr (!SMOOTH) hist |= (uint64_t)byte << (8 * (d - 1));
     }
+    // the surrogate derivatives and spikes of the next step down, loaded one step ahead
+    auto g_at = [&](int tt, int j) { return nt ? a.g_seg[((size_t)(tt - t0) * B + bq + j) * H + me] : 0.f; };
+    float gn0 = g_at(t1 - 1, 0), gn1 = g_at(t1 - 1, 1);
+    float stn[NS];
+    uint32_t sbn;
+    spikes_at(t1 - 1, stn, sbn);
     for (int t = t1 - 1; t >= t0; --t) {
         if (ro) {
             o = __fadd_rn(t == tsv ? dmv : 0.f, __fmul_rn(a.beta, o));
             obuf[rb * R + rr] = o;
         }
         __syncthreads();  // obuf ready; the previous step's partial-ring writes done
+        float qv0 = 0.f, qv1 = 0.f;
+        float st[NS];
+#pragma unroll
+        for (int b = 0; b < NS; ++b) st[b] = stn[b];
+        const uint32_t sbyte_t = sbn;
+        const float gc0 = gn0, gc1 = gn1;
+        if (t > t0) {
+            gn0 = g_at(t - 1, 0);
+            gn1 = g_at(t - 1, 1);
+            spikes_at(t - 1, stn, sbn);
+        }
         if (nt) {
-            float qv[SPT];
 #pragma unroll
             for (int j = 0; j < SPT; ++j) {
                 const int bl = SPT * sub + j;
                 float *pp = part + ((size_t)(t % RING) * HC + pl) * NS + bl;
                 float sh = *pp;
-                for (int r = 0; r < R; ++r) sh = __fadd_rn(sh, __fmul_rn(wout[pl * R + r], obuf[bl * R + r]));
+                for (int r = 0; r < R; ++r) sh = __fmaf_rn(__ldg(wout + pl * R + r), obuf[bl * R + r], sh);
                 *pp = 0.f;
-                const float g = a.g_seg[((size_t)(t - t0) * B + bq + j) * H + me];
+                const float g = j ? gc1 : gc0;
                 const float ap = __fmul_rn(a.alpha, j ? qp1 : qp0);
-                qv[j] = __fadd_rn(ap, __fmul_rn(g, __fadd_rn(sh, -__fmul_rn(a.theta, ap))));
-                a.dU[((size_t)t * B + bq + j) * H + me] = qv[j];
+                const float qv = __fmaf_rn(g, __fmaf_rn(-a.theta, ap, sh), ap);
+                a.dU[((size_t)t * B + bq + j) * H + me] = qv;
+                if (j) qv1 = qv;
+                else qv0 = qv;
             }
-            qp0 = qv[0];
-            qp1 = qv[1];
-            const float2 v = make_float2(qv[0], qv[1]);
-            float2 *dst = reinterpret_cast<float2 *>(pnew) + ((size_t)(t & 1) * H + me) * 4 + sub;
-            for (int k = 0; k < CL; ++k) *cl.map_shared_rank(dst, k) = v;
+            qp0 = qv0;
+            qp1 = qv1;
             // dw_out: this neuron's spikes at t times o[t]; each of its NT threads takes a quarter of the readouts
-            float st[NS];
-            uint32_t byte;
-            spikes_at(t, st, byte);
-            if (byte) {
+            if (sbyte_t) {
                 for (int r = sub * R4; r < min(R, (sub + 1) * R4); ++r) {
                     float acc = dwo[pl * R + r];
                     for (int b = 0; b < NS; ++b) {
-                        if constexpr (SMOOTH) acc = __fadd_rn(acc, __fmul_rn(st[b], obuf[b * R + r]));
-                        else if ((byte >> b) & 1u) acc = __fadd_rn(acc, obuf[b * R + r]);
+                        if constexpr (SMOOTH) acc = __fmaf_rn(st[b], obuf[b * R + r], acc);
+                        else if ((sbyte_t >> b) & 1u) acc = __fadd_rn(acc, obuf[b * R + r]);
                     }
                     dwo[pl * R + r] = acc;
                 }
             }
         }
-        cl.sync();  // q[t] of every neuron in every CTA's pnew[t & 1]
+        cluster_wait();  // every CTA has read the previous q from its pnew
+        if (nt) {
+            const float2 v = make_float2(qv0, qv1);
+            float2 *dst = reinterpret_cast<float2 *>(pnew) + (size_t)me * (QROW / 2) + sub;
+            for (int k = 0; k < CL; ++k) *cl.map_shared_rank(dst, k) = v;
+        }
+        cluster_arrive();
+        cluster_wait();  // q[t] of every neuron in every CTA's pnew
         // outgoing rows: partial[t - d] += w q[t][post]; dw += s[t - d][me] q[t][post]
-        const float *pn = pnew + (size_t)(t & 1) * H * NS;
         for (int d = 1; d <= MAXD; ++d) {
             float acc[NS];
 #pragma unroll
             for (int b = 0; b < NS; ++b) acc[b] = 0.f;
             const int gs = nt ? grp[pl * (MAXD + 1) + d - 1] : 0, ge = nt ? grp[pl * (MAXD + 1) + d] : 0;
             const uint32_t sbyte = SMOOTH ? 0xffu : (uint32_t)((hist >> (8 * (d - 1))) & 0xffu);
-#pragma unroll 2
-            for (int l = gs + sub; l < ge; l += NT) {
-                if (l >= on) {
-                    atomicAdd(a.err + 2, 1);
-                    continue;
-                }
-                const uint32_t c = ocode[l];
-                const int post = (int)(c & 0x7FFu);
-                const float wl = __ldg(ow + l);
-                if ((int)(c >> 11) != d || post >= H) {
-                    atomicAdd(a.err + 0, 1);
-                    continue;
-                }
-                const float4 x0 = reinterpret_cast<const float4 *>(pn)[(size_t)post * 2];
-                const float4 x1 = reinterpret_cast<const float4 *>(pn)[(size_t)post * 2 + 1];
-                const float x[NS] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-#pragma unroll
-                for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __fmul_rn(wl, x[b]));
-                if (sbyte) {
-                    float dk = 0.f;
-#pragma unroll
-                    for (int b = 0; b < NS; ++b) {
-                        if constexpr (SMOOTH) dk = __fadd_rn(dk, __fmul_rn(histf[d - 1][b], x[b]));
-                        else if ((sbyte >> b) & 1u) dk = __fadd_rn(dk, x[b]);
-                    }
-                    dw[l] = __fadd_rn(dw[l], dk);
-                }
-            }
+            if (sbyte) out_group<SMOOTH, true>(ocode, ow, pnew, dw, gs, ge, sub, sbyte, histf[d - 1], acc);
+            else out_group<SMOOTH, false>(ocode, ow, pnew, dw, gs, ge, sub, 0u, histf[d - 1], acc);
 #pragma unroll
             for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __shfl_xor_sync(FULL, acc[b], 1));
 #pragma unroll
@@ -555,6 +603,7 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
                 pp[1] = __fadd_rn(pp[1], x1);
             }
         }
+        cluster_arrive();  // this CTA's reads of q[t] are done
         // the spike history of step t - 1: delays 1..5 reach t - 2 .. t - 6
         if constexpr (SMOOTH) {
             for (int d = 1; d <= MAXD; ++d) {
@@ -567,6 +616,7 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
             hist = (hist >> 8) | ((uint64_t)byte << (8 * (MAXD - 1)));
         }
     }
+    cluster_wait();  // the last "reads done" phase
     // the state for the segment before this one
     __syncthreads();
     for (int k = tid; k < RING * HC * NS; k += nthr) part_st[k] = part[k];
