@@ -237,6 +237,30 @@ int n2b_bptt_status(const n2b_bptt_desc *d, void *workspace, size_t workspace_by
  * 8c + j of cluster c; smooth: [T][B/8][H][8] floats. */
 int n2b_bptt_spikes(const n2b_bptt_desc *d, void *workspace, size_t workspace_bytes, void *out, void *stream);
 
+/* ---- Run-time compiled step kernels of user-defined models ---------------
+ * The transpiler (naer2_b200/transpiler) lowers a population's Python hooks
+ * (receive / update / send) to CUDA device code inside a step-kernel template;
+ * these entry points compile that source with NVRTC for the device's
+ * architecture, load it and launch it. Replace the reference's
+ * FusedKernelTemplate.build (naer2/transpiler/templates/fused_template.py:
+ * 166-230, which builds a Triton/Gluon kernel) and its launch in
+ * PopulationRuntime._launch (naer2/runtime.py:506-526). */
+typedef struct n2b_jit_kernel n2b_jit_kernel;
+
+/* Compile `source` (self-contained CUDA C++, no includes) and load its
+ * extern "C" kernel `kernel_name` on `device`. options: extra NVRTC options.
+ * A compile error returns N2B_EINVAL with NVRTC's log in n2b_last_error(). */
+int n2b_jit_compile(const char *source, const char *kernel_name, const char *const *options, int32_t n_options,
+                    int32_t device, n2b_jit_kernel **out);
+
+/* Launch with one by-value parameter block of params_bytes bytes (the
+ * kernel's single parameter), grid x block threads, on `stream`. */
+int n2b_jit_launch(n2b_jit_kernel *k, uint32_t grid, uint32_t block, const void *params, size_t params_bytes,
+                   void *stream);
+
+/* Unload the kernel. */
+int n2b_jit_destroy(n2b_jit_kernel *k);
+
 /* Size of the library's own device scratch used by n2b_run_static. */
 #define N2B_STATIC_SCRATCH_BYTES ((size_t)32 << 20)
 

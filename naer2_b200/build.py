@@ -21,14 +21,14 @@ HERE = pathlib.Path(__file__).resolve().parent
 ROOT = HERE.parent
 CSRC = HERE / "csrc"
 LIB = HERE / "libnaer2b.so"
-SOURCES = [CSRC / "naer2b.cu", CSRC / "bptt.cu"]
+SOURCES = [CSRC / "naer2b.cu", CSRC / "bptt.cu", CSRC / "jit.cu"]
 HEADERS = [CSRC / "n2b_device.cuh", ROOT / "include" / "naer2b.h"]
 PEAK_LIB = HERE / "libn2b_peak.so"
 PEAK_SOURCES = [CSRC / "l2_peak.cu"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC,-O2", "-shared",
-         "-cudart", "static", "-Xptxas", "-v"]
+         "-cudart", "static", "-Xptxas", "-v", "-ldl"]
 
 
 def nvcc() -> str:

@@ -185,7 +185,7 @@ def params_of(pop, dt: float) -> KernelParams:
     cls = type(pop.instance)
     if cls not in BUILTIN:
         raise NotImplementedError(f"{cls.__name__} is not a built-in CUDA model ({', '.join(c.__name__ for c in BUILTIN)}): "
-                                  f"lowering arbitrary hooks to CUDA is not available in this build")
+                                  f"a network with it runs on the transpiled path (naer2_b200.transpiler)")
     kp = cls.kernel_params(pop.instance, dt)
     kp.setdefault("fire_threshold", 0)
     kp["ext_table"] = cdf_table(kp["ext_lambda"]) if kp["ext_lambda"] > 0 and kp["ext_weight"] != 0 else \

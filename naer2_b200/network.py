@@ -67,9 +67,15 @@ class Network:
         if self._runtime is None:
             if self.device is None or self.device.type != "cuda":
                 raise RuntimeError("naer2_b200 steps networks on a CUDA device only (no CPU fallback)")
+            from .models import BUILTIN
             from .runtime import NetworkRuntime
 
-            self._runtime = NetworkRuntime(self)
+            if all(type(p.instance) in BUILTIN for p in self.populations):
+                self._runtime = NetworkRuntime(self)
+            else:  # a model without a built-in kernel: every population's hooks transpiled, compiled at run time
+                from .transpiler import JitRuntime
+
+                self._runtime = JitRuntime(self)
         return self._runtime
 
     def steps_for(self, t_step: float) -> int:

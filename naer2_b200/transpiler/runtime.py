@@ -1,0 +1,221 @@
+"""The run-time compiled path: a network whose populations' hooks are lowered to CUDA and compiled with
+NVRTC (reference naer2/runtime.py:213-526, PopulationRuntime, which builds and launches the generated
+Gluon kernels; here one generated step kernel per population, `n2b_jit_*` in the C ABI).
+
+Built by Network.runtime when a population's model has no built-in kernel (models.params_of raises). Every
+population of such a network runs its own transpiled hooks -- built-in models included, as their hooks
+state them in Python. The interface Network uses is NetworkRuntime's: advance, start_recording, raster,
+spikes, status, check, counters, reset_counters, close.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import hashlib
+
+import numpy as np
+import torch
+
+from .. import _lib
+from ..topology import delay_steps, pull_form
+from .template import build_source, ctype_of, hook_context, params_type
+
+BLOCK = 128
+_CACHE: dict = {}  # (source hash, device) -> n2b_jit_kernel handle, for the process's lifetime
+
+
+def compile_source(source: str, device: int) -> ctypes.c_void_p:
+    key = (hashlib.sha256(source.encode()).hexdigest(), device)
+    if key not in _CACHE:
+        lib = _lib.load()
+        h = ctypes.c_void_p()
+        _lib.check(lib.n2b_jit_compile(source.encode(), b"n2b_user_step", None, 0, device, ctypes.byref(h)),
+                   "n2b_jit_compile")
+        _CACHE[key] = h
+    return _CACHE[key]
+
+
+def edge_values(conn, hook_ctx_names: set):
+    """(per-link names, {hook name: scalar}) of the edge attributes a receive hook reads on this connection."""
+    fabric = conn.fabric
+    rename = {hook_name: real for real, hook_name in (conn._fabric_map or {}).items()}
+    dynamic, static = [], {}
+    for name in sorted(hook_ctx_names):
+        v = fabric.value(rename.get(name, name))
+        if v is None:
+            raise ValueError(f"{conn!r}: the receive hook reads edge.{name}, which the connection does not have")
+        if isinstance(v, torch.Tensor) and v.numel() != 1:
+            dynamic.append(name)
+        else:
+            static[name] = float(v.item() if isinstance(v, torch.Tensor) else v)
+    return dynamic, static
+
+
+class JitRuntime:
+    def __init__(self, net):
+        from ..hook import used_members
+
+        self.net = net
+        dev = self.device = net.device
+        dindex = dev.index if dev.index is not None else 0
+        dt = self.dt = float(net.resolution)
+        pops = self.pops = list(net.populations)
+        index = {id(p): k for k, p in enumerate(pops)}
+        self.keep = []
+        words = [(len(p.shape) + 31) // 32 for p in pops]
+        self.words = words
+        # spike-bit ring depth of each population: above every delay of its outgoing connections
+        steps_of, max_out = {}, [1] * len(pops)
+        for c in net.connections:
+            topo = c.fabric.topology
+            steps = delay_steps(c.fabric.value("delay"), len(topo), dt, device=topo.target_indices.device)
+            steps_of[id(c)] = steps
+            if len(topo):
+                s = index[id(c._source)]
+                max_out[s] = max(max_out[s], int(steps.max()))
+        depth = [max(2, 1 << int(np.ceil(np.log2(m + 1)))) for m in max_out]
+        self.depth = depth
+        self.bits = [torch.zeros(d * w, dtype=torch.int32, device=dev) for d, w in zip(depth, words)]
+        self.err = torch.zeros(len(pops), dtype=torch.int32, device=dev)
+        self.counters_t = torch.zeros(len(pops), 2, dtype=torch.int64, device=dev)
+        self.record_rows = int(net.record_steps)
+        self.rec_step0 = net.step_count
+        self.rasters = [torch.zeros(max(1, self.record_rows) * w, dtype=torch.int32, device=dev) for w in words]
+        self.kernels, self.params, self.sources = [], [], []
+        for k, p in enumerate(pops):
+            node = p.node
+            incoming, ctx_in = [], []
+            conns = [c for c in net.connections if c._target is p]
+            site = 0
+            for c in conns:
+                port = c._target_port or "receive"
+                hook = node.receive.get(port)
+                if hook is None:
+                    raise ValueError(f"{p!r} has no receive port {port!r}")
+                names = used_members(hook.ast, hook.parameter_type_to_name.get(_edge_type(), "edge"))
+                dyn, stat = edge_values(c, names)
+                ctx = hook_context(p, hook, dyn, stat, site_base=site)
+                site += 32
+                incoming.append({"receive": (hook.ast, ctx), "edge_dynamic": dyn, "conn": c})
+            hooks = {"update": (node.update.ast, hook_context(p, node.update, site_base=site)),
+                     "send": (node.send.ast, hook_context(p, node.send, site_base=site + 32))}
+            src, fields = build_source(type(p.instance).__name__, dict(p.dynamic_attrs), hooks, incoming)
+            self.sources.append(src)
+            self.kernels.append(compile_source(src, dindex))
+            P = params_type(fields)()
+            P.n, P.words, P.bit_mask = len(p.shape), words[k], depth[k] - 1
+            P.seed_lo, P.seed_hi = int(p.seed) & 0xFFFFFFFF, (int(p.seed) >> 32) & 0xFFFFFFFF
+            for a, py in p.dynamic_attrs.items():
+                _, _, tdt = ctype_of(py)
+                t = p.state_tensor(a, dev)
+                if t.dtype != tdt:
+                    t = t.to(tdt)
+                if not t.is_contiguous():
+                    t = t.contiguous()
+                p._state[a] = t
+                setattr(P, f"s_{a}", t.data_ptr())
+            P.bits, P.raster = self.bits[k].data_ptr(), self.rasters[k].data_ptr()
+            P.raster_steps, P.rec0 = self.record_rows, self.rec_step0
+            P.err = self.err[k:].data_ptr()
+            P.counters = self.counters_t[k].data_ptr()
+            for ci, inc in enumerate(incoming):
+                c = inc["conn"]
+                s = index[id(c._source)]
+                topo = c.fabric.topology
+                ptr, link, perm = pull_form(topo, steps_of[id(c)], len(p.shape))
+                ptr, link = self._dev(ptr), self._dev(link if link.numel() else torch.zeros(1, dtype=torch.int32))
+                setattr(P, f"c{ci}_ptr", ptr.data_ptr())
+                setattr(P, f"c{ci}_link", link.data_ptr())
+                setattr(P, f"c{ci}_src_bits", self.bits[s].data_ptr())
+                setattr(P, f"c{ci}_src_words", words[s])
+                setattr(P, f"c{ci}_src_mask", depth[s] - 1)
+                rename = {hn: real for real, hn in (c._fabric_map or {}).items()}
+                for e in inc["edge_dynamic"]:
+                    v = c.fabric.value(rename.get(e, e)).detach().reshape(-1).to(torch.float32)
+                    v = self._dev(v.to(perm.device)[perm] if v.numel() else torch.zeros(1))
+                    setattr(P, f"c{ci}_e_{e}", v.data_ptr())
+            self.params.append(P)
+        self.stream = torch.cuda.Stream(device=dev)
+        self._s = ctypes.c_void_p(self.stream.cuda_stream)
+        self.launches = 0
+
+    def _dev(self, t):
+        t = t.to(self.device).contiguous()
+        self.keep.append(t)
+        return t
+
+    # ------------------------------------------------------------------ stepping
+
+    def advance(self, n_steps: int) -> None:
+        lib = _lib.load()
+        self.stream.wait_stream(torch.cuda.current_stream(self.device))
+        step = self.net.step_count
+        for k in range(int(n_steps)):
+            n = step + k
+            for kern, P, p in zip(self.kernels, self.params, self.pops):
+                P.step, P.t = n, (n + 1) * self.dt
+                grid = (len(p.shape) + BLOCK - 1) // BLOCK
+                if grid:
+                    _lib.check(lib.n2b_jit_launch(kern, grid, BLOCK, ctypes.byref(P), ctypes.sizeof(P), self._s),
+                               "n2b_jit_launch")
+                    self.launches += 1
+        torch.cuda.current_stream(self.device).wait_stream(self.stream)
+
+    def start_recording(self, steps: int) -> None:
+        if self.record_rows == 0 or steps > self.record_rows:
+            raise RuntimeError("recording needs Network.record(steps) before the first step "
+                               f"(this runtime keeps {self.record_rows} rows)")
+        self.rec_step0 = self.net.step_count
+        for P in self.params:
+            P.rec0 = self.rec_step0
+
+    # ------------------------------------------------------------------ results
+
+    def raster_words(self, pop) -> np.ndarray:
+        k = self.pops.index(pop)
+        words = self.words[k]
+        rows = min(self.record_rows, self.net.step_count - self.rec_step0)
+        if rows <= 0:
+            return np.zeros((0, words), dtype=np.uint32)
+        self.stream.synchronize()
+        return self.rasters[k][: rows * words].cpu().numpy().view(np.uint32).reshape(rows, words)
+
+    def raster(self, pop) -> np.ndarray:
+        w = self.raster_words(pop)
+        n = len(pop.shape)
+        bits = np.unpackbits(w.view(np.uint8).reshape(len(w), -1, 4), axis=2, bitorder="little")
+        return bits.reshape(len(w), -1)[:, :n].astype(bool)
+
+    def spikes(self, pop):
+        steps, ids = np.nonzero(self.raster(pop))
+        return steps.astype(np.int64) + self.rec_step0, ids.astype(np.int64)
+
+    def status(self) -> list:
+        self.stream.synchronize()
+        return self.err.cpu().tolist()
+
+    def check(self) -> None:
+        bad = sum(self.status())
+        if bad:
+            raise RuntimeError(f"{bad} links with a delay outside their source's spike ring")
+
+    def counters(self) -> dict:
+        self.stream.synchronize()
+        c = self.counters_t.cpu().numpy()
+        return {"events": int(c[:, 0].sum()), "spikes": int(c[:, 1].sum()),
+                "per_population": [int(x) for x in c[:, 1]]}
+
+    def reset_counters(self) -> None:
+        self.stream.synchronize()
+        self.counters_t.zero_()
+        self.err.zero_()
+
+    def close(self) -> None:
+        self.stream.synchronize()
+        self.kernels = []
+
+
+def _edge_type():
+    from .. import receives
+
+    return receives.edge

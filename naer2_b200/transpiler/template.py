@@ -1,0 +1,156 @@
+"""The step-kernel template of a transpiled population (reference naer2/transpiler/templates/fused_template.py:
+85-371, the Gluon kernel it fills: pull -> deliver -> update/send -> emit).
+
+One thread per neuron, one launch per population per step n (time t = (n + 1) dt, the end of the step):
+  1. intake and receive: for each incoming connection (in the network's order), the neuron's pull row (its
+     incoming links, canonical order within the row); a link whose source spiked at step n - d (the source
+     population's spike-bit ring) runs the connection's receive hook once, with its per-link edge values;
+  2. update, then send (n2.spike() anywhere marks the neuron as firing at step n);
+  3. a ballot word per warp into the population's spike-bit ring slot n mod depth (and the raster), the
+     state back to memory, and the spike / arrival counters.
+The source is self-contained (NVRTC compiles it with no includes); its one parameter is the `Params` block,
+mirrored field by field by the ctypes structure `params_type` builds, so that the host fills it directly.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+from .cuda import HookContext, lower_hook
+
+_PRELUDE = r'''
+typedef unsigned int u32;
+typedef unsigned long long u64;
+
+// Philox4x32-10 (Salmon et al., SC 2011): the first output word of counter (c0..c3) under key (k0, k1).
+__device__ __forceinline__ u32 n2_philox_w0(u32 c0, u32 c1, u32 c2, u32 c3, u32 k0, u32 k1) {
+    #pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const u32 h0 = __umulhi(0xD2511F53u, c0), l0 = 0xD2511F53u * c0;
+        const u32 h1 = __umulhi(0xCD9E8D57u, c2), l1 = 0xCD9E8D57u * c2;
+        const u32 n0 = h1 ^ c1 ^ k0, n2 = h0 ^ c3 ^ k1;
+        c0 = n0; c1 = l1; c2 = n2; c3 = l0;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+    return c0;
+}
+
+// Python's % on floats: the result takes the sign of the divisor.
+__device__ __forceinline__ float n2_pymod(float a, float b) {
+    float r = fmodf(a, b);
+    if (r != 0.f && ((r < 0.f) != (b < 0.f))) r += b;
+    return r;
+}
+'''
+
+
+def ctype_of(py) -> tuple[str, object, object]:
+    """(C type, ctypes type, torch dtype) of a dynamic attribute's Python type."""
+    import torch
+
+    if py is bool:
+        return "bool", ctypes.c_bool, torch.bool
+    if py is int:
+        return "int", ctypes.c_int32, torch.int32
+    return "float", ctypes.c_float, torch.float32
+
+
+def build_source(pop_name: str, attrs: dict, hooks: dict, incoming: list) -> tuple[str, list]:
+    """(CUDA source, params fields [(name, C type, ctypes type)]) of one population.
+
+    attrs: dynamic attr -> python type; hooks: {"update": (fn_ast, ctx), "send": (fn_ast, ctx)};
+    incoming: one dict per incoming connection {"receive": (fn_ast, ctx) or None, "edge_dynamic": [names]}."""
+    fields = [("step", "long long", ctypes.c_int64), ("rec0", "long long", ctypes.c_int64),
+              ("raster_steps", "long long", ctypes.c_int64), ("t", "float", ctypes.c_float),
+              ("n", "int", ctypes.c_int32), ("words", "int", ctypes.c_int32), ("bit_mask", "int", ctypes.c_int32),
+              ("seed_lo", "u32", ctypes.c_uint32), ("seed_hi", "u32", ctypes.c_uint32)]
+    for a, py in attrs.items():
+        ct, cty, _ = ctype_of(py)
+        fields.append((f"s_{a}", f"{ct} *", ctypes.c_void_p))
+    fields += [("bits", "u32 *", ctypes.c_void_p), ("raster", "u32 *", ctypes.c_void_p),
+               ("err", "int *", ctypes.c_void_p), ("counters", "u64 *", ctypes.c_void_p)]
+    for c, inc in enumerate(incoming):
+        fields += [(f"c{c}_ptr", "const int *", ctypes.c_void_p), (f"c{c}_link", "const u32 *", ctypes.c_void_p),
+                   (f"c{c}_src_bits", "const u32 *", ctypes.c_void_p),
+                   (f"c{c}_src_words", "int", ctypes.c_int32), (f"c{c}_src_mask", "int", ctypes.c_int32)]
+        for e in inc["edge_dynamic"]:
+            fields.append((f"c{c}_e_{e}", "const float *", ctypes.c_void_p))
+
+    src = [_PRELUDE, "struct Params {\n"]
+    src += [f"    {ct} {name};\n" for name, ct, _ in fields]
+    src.append("};\n\n")
+    src.append(r'''// uniform in [0, 1): 24 bits of the draw for (neuron j, step n, call site, link k)
+__device__ __forceinline__ float n2_uniform(const Params &p, int j, long long n, u32 site, u32 k) {
+    const u32 w = n2_philox_w0((u32)j, (u32)n, (u32)((u64)n >> 32), (site << 24) | (k & 0xFFFFFFu), p.seed_lo,
+                               p.seed_hi);
+    return (float)(w >> 8) * 5.9604644775390625e-08f;
+}
+
+''')
+    src.append(f'// population {pop_name}\nextern "C" __global__ void __launch_bounds__(128) n2b_user_step('
+               "const __grid_constant__ Params p) {\n")
+    src.append("    const int j = blockIdx.x * blockDim.x + threadIdx.x;\n")
+    src.append("    const bool live = j < p.n;\n    const long long n = p.step;\n    const float t = p.t;\n")
+    src.append("    bool fired = false;\n    u32 arrived = 0;\n    u32 link_k = 0xFFFFFFu;\n")
+    for a, py in attrs.items():
+        ct, _, _ = ctype_of(py)
+        src.append(f"    {ct} s_{a} = live ? p.s_{a}[j] : ({ct})0;\n")
+    src.append("    if (live) {\n")
+    for c, inc in enumerate(incoming):
+        if inc["receive"] is None:
+            continue
+        fn, ctx = inc["receive"]
+        body = lower_hook(fn, ctx, f"{pop_name} receive (connection {c})")
+        loads = "".join(f"            const float e_{e} = p.c{c}_e_{e}[l];\n" for e in inc["edge_dynamic"])
+        src.append(f"""        for (int l = p.c{c}_ptr[j]; l < p.c{c}_ptr[j + 1]; ++l) {{
+            const u32 w = p.c{c}_link[l];
+            const int src = (int)(w & 0xFFFFFFu), d = (int)(w >> 24);
+            if (d < 1 || d > p.c{c}_src_mask) {{ atomicAdd(p.err, 1); continue; }}
+            const long long m = n - d;
+            if (m < 0) continue;
+            if (!((p.c{c}_src_bits[(size_t)(m & p.c{c}_src_mask) * p.c{c}_src_words + (src >> 5)] >> (src & 31)) & 1u))
+                continue;
+{loads}            link_k = arrived++;
+""")
+        src.append("            " + body.replace("\n", "\n            ").rstrip() + "\n")
+        src.append("        }\n        link_k = 0xFFFFFFu;\n")
+    for name in ("update", "send"):
+        fn, ctx = hooks[name]
+        body = lower_hook(fn, ctx, f"{pop_name} {name}")
+        src.append("        " + body.replace("\n", "\n        ").rstrip() + "\n")
+    src.append("    }\n")
+    src.append(r'''    const u32 b = __ballot_sync(0xffffffffu, live && fired);
+    const u32 arrivals = __reduce_add_sync(0xffffffffu, arrived);
+    if ((threadIdx.x & 31) == 0) {
+        const int word = j >> 5;
+        if (word < p.words) {
+            p.bits[(size_t)(n & p.bit_mask) * p.words + word] = b;
+            const long long r = n - p.rec0;
+            if (p.raster && r >= 0 && r < p.raster_steps) p.raster[(size_t)r * p.words + word] = b;
+        }
+        if (b) atomicAdd(p.counters + 1, (u64)__popc(b));
+        if (arrivals) atomicAdd(p.counters, (u64)arrivals);
+    }
+''')
+    for a in attrs:
+        src.append(f"    if (live) p.s_{a}[j] = s_{a};\n")
+    src.append("}\n")
+    return "".join(src), fields
+
+
+def params_type(fields: list):
+    """The ctypes structure of a Params block."""
+    return type("Params", (ctypes.Structure,), {"_fields_": [(name, cty) for name, _, cty in fields]})
+
+
+def hook_context(pop, hook, edge_dynamic=(), edge_static=None, site_base: int = 0) -> HookContext:
+    """The names a hook's body may use, from its signature and the population's attributes."""
+    from .. import receives
+
+    names = {ty: nm for ty, nm in hook.parameter_type_to_name.items()}
+    static = {k: v for k, v in pop.instance.__dict__.items()
+              if k not in pop.dynamic_attrs and isinstance(v, (int, float, bool))}
+    return HookContext(self_attrs=dict(pop.dynamic_attrs), self_static=static,
+                       time_name=names.get(receives.time), edge_name=names.get(receives.edge),
+                       source_name=names.get(receives.source), edge_dynamic=set(edge_dynamic),
+                       edge_static=dict(edge_static or {}), site_base=site_base)

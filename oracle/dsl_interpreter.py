@@ -1,0 +1,157 @@
+"""CPU interpreter of the DSL's fixed-step semantics -- test infrastructure only: the tests check the
+transpiled, run-time compiled step kernels (naer2_b200/transpiler) against it.
+
+It runs the models' own hook functions, in Python, one neuron at a time, on float32 state (numpy scalars, so
+that arithmetic rounds to single precision as the kernels' does), in the order the kernels define for one
+step n at time t = (n + 1) dt (the semantics the reference's fused round implements per population,
+naer2/transpiler/templates/fused_template.py:321-371: deliveries, then update and send):
+  for every population, every neuron j: for every incoming connection (network order), every link of j's
+  pull row (canonical order within the row) whose source spiked at step n - d: receive(self, time, edge,
+  source); then update(self, time); then send(self, time); n2.spike() marks j as firing at step n.
+random.random() draws Philox4x32-10 words keyed by the population's seed and counted by (neuron, step,
+call site, arrival); call sites are numbered in the order their calls run, which matches the transpiler's
+source-order numbering when a hook's calls are not conditional.
+"""
+
+from __future__ import annotations
+
+import random as _random
+
+import numpy as np
+import torch
+
+import naer2_b200 as n2
+from naer2_b200 import receives
+from naer2_b200.topology import delay_steps, pull_form
+
+from . import philox
+
+
+class _Self:
+    """self of neuron j: dynamic attributes in float32 / int32 / bool arrays, static ones as float32."""
+
+    def __init__(self, arrays: dict, static: dict):
+        object.__setattr__(self, "_a", arrays)
+        object.__setattr__(self, "_s", static)
+        object.__setattr__(self, "_j", 0)
+
+    def __getattr__(self, name):
+        a = object.__getattribute__(self, "_a")
+        if name in a:
+            return a[name][object.__getattribute__(self, "_j")]
+        s = object.__getattribute__(self, "_s")
+        if name in s:
+            return s[name]
+        raise AttributeError(name)
+
+    def __setattr__(self, name, value):
+        self._a[name][self._j] = value
+
+
+class _Edge:
+    def __init__(self, values: dict):
+        object.__setattr__(self, "_v", values)
+        object.__setattr__(self, "_l", 0)
+
+    def __getattr__(self, name):
+        v = object.__getattribute__(self, "_v")[name]
+        return v[object.__getattribute__(self, "_l")] if isinstance(v, np.ndarray) else v
+
+
+def _f32(v):
+    return np.float32(v) if isinstance(v, float) else v
+
+
+def run(net, n_steps: int):
+    """Run `net` (its populations' current state tensors, on the CPU) for n_steps from step 0; returns
+    (rasters: [bool [n_steps, n]] per population, final state: [{attr: array}] per population)."""
+    dt = float(net.resolution)
+    pops = list(net.populations)
+    index = {id(p): k for k, p in enumerate(pops)}
+    arrays, selves = [], []
+    for p in pops:
+        arr = {}
+        for a, py in p.dynamic_attrs.items():
+            t = p.state_tensor(a).detach().cpu()
+            arr[a] = t.numpy().astype(np.bool_ if py is bool else np.int32 if py is int else np.float32).copy()
+        arrays.append(arr)
+        static = {k: _f32(v) for k, v in p.instance.__dict__.items()
+                  if k not in p.dynamic_attrs and isinstance(v, (int, float, bool))}
+        selves.append(_Self(arr, static))
+    incoming = [[] for _ in pops]
+    for c in net.connections:
+        t = index[id(c._target)]
+        topo = c.fabric.topology
+        steps = delay_steps(c.fabric.value("delay"), len(topo), dt, device="cpu")
+        ptr, link, perm = pull_form(topo.to("cpu") if hasattr(topo, "to") else topo, steps.cpu(), len(pops[t].shape))
+        port = c._target_port or "receive"
+        hook = pops[t].node.receive[port]
+        rename = {hn: real for real, hn in (c._fabric_map or {}).items()}
+        from naer2_b200.hook import used_members
+
+        names = used_members(hook.ast, hook.parameter_type_to_name.get(receives.edge, "edge"))
+        values = {}
+        for nm in names:
+            v = c.fabric.value(rename.get(nm, nm))
+            if isinstance(v, torch.Tensor) and v.numel() != 1:
+                values[nm] = v.detach().reshape(-1).cpu()[perm.cpu()].numpy().astype(np.float32)
+            else:
+                values[nm] = np.float32(float(v.item() if isinstance(v, torch.Tensor) else v))
+        w = link.cpu().numpy().astype(np.int64) & 0xFFFFFFFF
+        incoming[t].append((index[id(c._source)], ptr.cpu().numpy(), w & 0xFFFFFF, w >> 24, hook, _Edge(values)))
+    spikes = [np.zeros((n_steps, len(p.shape)), dtype=bool) for p in pops]
+
+    state = {"fired": False, "j": 0, "n": 0, "k": 0xFFFFFF, "site": 0, "seed": (0, 0)}
+
+    def spike(time=None):
+        state["fired"] = True
+
+    def uniform():
+        c3 = ((state["site"] & 0xFF) << 24) | (state["k"] & 0xFFFFFF)
+        state["site"] += 1
+        n = state["n"]
+        w = philox([state["j"], n & 0xFFFFFFFF, (n >> 32) & 0xFFFFFFFF, c3], state["seed"])[0]
+        return np.float32((w >> 8) * 5.9604644775390625e-08)
+
+    def call(hook, obj, t, edge=None, site_base=0):
+        kw = {}
+        for ty, nm in hook.parameter_type_to_name.items():
+            if ty is receives.time:
+                kw[nm] = t
+            elif ty is receives.edge:
+                kw[nm] = edge
+            elif ty is receives.source:
+                kw[nm] = None
+        state["site"] = site_base
+        hook.function(obj, **kw)
+
+    saved = (n2.spike, _random.random)
+    n2.spike, _random.random = spike, uniform
+    try:
+        for n in range(n_steps):
+            t = np.float32((n + 1) * dt)
+            state["n"] = n
+            for k, p in enumerate(pops):
+                obj = selves[k]
+                state["seed"] = (int(p.seed) & 0xFFFFFFFF, (int(p.seed) >> 32) & 0xFFFFFFFF)
+                node = p.node
+                n_recv = len(incoming[k])
+                for j in range(len(p.shape)):
+                    object.__setattr__(obj, "_j", j)
+                    state["j"], state["fired"], arrived = j, False, 0
+                    for ci, (s, ptr, src, d, hook, edge) in enumerate(incoming[k]):
+                        for l in range(ptr[j], ptr[j + 1]):
+                            m = n - int(d[l])
+                            if m < 0 or not spikes[s][m, src[l]]:
+                                continue
+                            object.__setattr__(edge, "_l", l)
+                            state["k"] = arrived
+                            arrived += 1
+                            call(hook, obj, t, edge, site_base=32 * ci)
+                    state["k"] = 0xFFFFFF
+                    call(node.update, obj, t, site_base=32 * n_recv)
+                    call(node.send, obj, t, site_base=32 * n_recv + 32)
+                    spikes[k][n, j] = state["fired"]
+    finally:
+        n2.spike, _random.random = saved
+    return spikes, arrays

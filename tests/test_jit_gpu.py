@@ -1,0 +1,92 @@
+"""Transpiled, NVRTC-compiled step kernels of user-defined models against the DSL interpreter
+(oracle/dsl_interpreter.py), which runs the same hooks in Python on float32 state.
+
+Parity: identical spike rasters; state within float32 rounding (the kernels' single-precision math
+functions and the interpreter's may differ in the last bits: 1e-5 relative, 1e-6 absolute)."""
+
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from naer2_b200 import _lib
+from naer2_b200.patterns import all_to_all, fixed_indegree
+from naer2_b200.transpiler import JitRuntime
+from oracle import dsl_interpreter
+from tests.dsl_models import DecayLIF, Izhikevich, Pacemaker, Syn, TwoPort
+
+pytestmark = pytest.mark.gpu
+
+
+def check_against_interpreter(net, steps):
+    rasters, state = dsl_interpreter.run(net, steps)  # before the GPU run: the same initial state and seeds
+    net.record(steps)
+    net.run_steps(steps)
+    assert isinstance(net.runtime, JitRuntime)
+    net.check()
+    for k, p in enumerate(net.populations):
+        got = net.runtime.raster(p)
+        if not np.array_equal(got, rasters[k]):
+            bad = np.nonzero((got != rasters[k]).any(1))[0]
+            raise AssertionError(f"population {k}: rasters differ first at step {bad[0]}")
+        for a, want in state[k].items():
+            have = p.state_tensor(a).cpu().numpy()
+            if want.dtype == np.float32:
+                np.testing.assert_allclose(have, want, rtol=1e-5, atol=1e-6, err_msg=f"{k}.{a}")
+            else:
+                assert np.array_equal(have, want), f"{k}.{a}"
+    return rasters
+
+
+def test_decay_lif_driven_by_pacemakers(cuda):
+    g = torch.Generator().manual_seed(1)
+    src = Pacemaker(period=6) * 50
+    tgt = DecayLIF(theta=0.6, tau=5.0) * 70
+    c = src >> Syn() @ fixed_indegree(8, seed=3) >> tgt
+    c.weight = torch.rand(c.shape, generator=g) * 0.3
+    c.delay = (torch.randint(1, 6, c.shape, generator=g) * 0.1).double()
+    src.phase = torch.randint(0, 6, (50,), generator=g, dtype=torch.int32)
+    net = src.network
+    net.resolution = 0.1
+    r = check_against_interpreter(net, 150)
+    assert r[1].sum() > 50
+
+
+def test_recurrent_izhikevich_with_random_drive(cuda):
+    g = torch.Generator().manual_seed(2)
+    pop = Izhikevich() * 200
+    c = pop >> Syn() @ fixed_indegree(10, seed=4) >> pop
+    c.weight = torch.randn(c.shape, generator=g) * 2.0
+    c.delay = 0.3
+    pop.v = -65.0 + 10.0 * torch.rand(200, generator=g)
+    net = pop.network
+    net.resolution = 0.5
+    r = check_against_interpreter(net, 200)
+    assert r[0].sum() > 100
+
+
+def test_two_receive_ports_int_and_bool_state(cuda):
+    g = torch.Generator().manual_seed(5)
+    exc = Pacemaker(period=3) * 20
+    inh = Pacemaker(period=11) * 10
+    tgt = TwoPort(theta=1.5) * 40
+    ce = exc >> Syn(gain=1.5) @ "exc" @ fixed_indegree(4, seed=6) >> tgt
+    ce.weight = torch.rand(ce.shape, generator=g)
+    ci = inh >> Syn(weight=0.4) @ "inh" @ all_to_all() >> tgt
+    ci.delay = 0.2
+    exc.phase = torch.arange(20, dtype=torch.int32)
+    net = exc.network + inh.network
+    net.resolution = 0.1
+    r = check_against_interpreter(net, 120)
+    assert r[2].sum() > 10
+
+
+def test_a_compile_error_carries_the_nvrtc_log(cuda):
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    rc = lib.n2b_jit_compile(b'extern "C" __global__ void n2b_user_step(int x) { undefined_name = x; }',
+                             b"n2b_user_step", None, 0, 0, ctypes.byref(h))
+    assert rc == -1
+    msg = lib.n2b_last_error().decode()
+    assert "NVRTC compile failed" in msg and "undefined_name" in msg
