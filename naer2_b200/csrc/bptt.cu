@@ -346,26 +346,70 @@ __global__ void __launch_bounds__(512) fwd_kernel(const __grid_constant__ Args a
 // ------------------------------------------------------------------------------------------------ recompute
 
 // The recurrent input R of every step of a segment [t0, t1) from the stored spikes: NT threads per
-// (step, cluster, neuron), the forward's link split and addition order (the same sums bit for bit).
+// (chunk of TC steps, cluster, neuron); each thread decodes its share of the neuron's incoming row once and
+// applies every link to the TC steps of its chunk, then the NT shares are added as the forward adds them
+// ((s0 + s1) + (s2 + s3), links in the forward's order within each share): the same sums bit for bit.
+// A link with a bad code (counted by the forward) is clamped into range here instead of checked per step.
+constexpr int TC = 5;
+
 template <bool SMOOTH>
 __global__ void __launch_bounds__(256) recompute_r_kernel(const __grid_constant__ Args a, int t0, int t1) {
-    const size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const size_t per_t = (size_t)a.NC * a.H * NT;
-    const bool live = gid < (size_t)(t1 - t0) * per_t;  // whole groups of NT lanes live or not together
-    const size_t g = live ? gid : 0;
-    const int t = t0 + (int)(g / per_t);
-    const int rem = (int)(g % per_t);
+    const int nchunk = (t1 - t0 + TC - 1) / TC;
+    const int per_c = a.NC * a.H * NT;
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = gid < nchunk * per_c;  // whole groups of NT lanes live or not together
+    const int g = live ? gid : 0;
+    const int tc = t0 + (g / per_c) * TC;
+    const int rem = g % per_c;
     const int q = rem / (a.H * NT), post = (rem / NT) % a.H, sub = rem % NT;
-    const TapeSrc src{a.s_bits, a.s_f, a.H, a.NC, q, t};
     const int rs = live ? a.in_ptr[post] : 0, re = live ? a.in_ptr[post + 1] : 0;
-    float acc[NS];
-    gather_in<SMOOTH, true>(a, src, a.in_code, a.in_w, rs, re, sub, acc);
+    const int row = a.NC * a.H;  // bytes between two steps of the stored spikes
+    float acc[TC][NS];
+#pragma unroll
+    for (int k = 0; k < TC; ++k)
+#pragma unroll
+        for (int b = 0; b < NS; ++b) acc[k][b] = 0.f;
+    for (int l = rs + sub; l < re; l += NT) {
+        const uint32_t c = a.in_code[l];
+        const float wl = a.in_w[l];
+        const int pre = min((int)(c & 0x7FFu), a.H - 1), d = min(max((int)(c >> 11), 1), MAXD);
+        const int base = (tc - d) * row + q * a.H + pre;  // step tc - d
+#pragma unroll
+        for (int k = 0; k < TC; ++k) {
+            const int tt = tc + k - d;
+            if (tt < 0 || tc + k >= t1) continue;
+            if constexpr (SMOOTH) {
+                const float4 *p = reinterpret_cast<const float4 *>(a.s_f) + (size_t)(base + k * row) * 2;
+                const float4 x = p[0], y = p[1];
+                const float s[NS] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
+#pragma unroll
+                for (int b = 0; b < NS; ++b) acc[k][b] = __fadd_rn(acc[k][b], __fmul_rn(wl, s[b]));
+            } else {
+                const uint32_t byte = a.s_bits[base + k * row];
+                if (!byte) continue;
+#pragma unroll
+                for (int b = 0; b < NS; ++b)
+                    if ((byte >> b) & 1u) acc[k][b] = __fadd_rn(acc[k][b], wl);
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < TC; ++k) {
+#pragma unroll
+        for (int b = 0; b < NS; ++b) acc[k][b] = __fadd_rn(acc[k][b], __shfl_xor_sync(FULL, acc[k][b], 1));
+#pragma unroll
+        for (int b = 0; b < NS; ++b) acc[k][b] = __fadd_rn(acc[k][b], __shfl_xor_sync(FULL, acc[k][b], 2));
+    }
     if (!live) return;
-    float r0, r1;
-    mine(acc, sub, r0, r1);
-    const size_t b = (size_t)q * NS + SPT * sub;
-    a.g_seg[((size_t)(t - t0) * a.B + b) * a.H + post] = r0;
-    a.g_seg[((size_t)(t - t0) * a.B + b + 1) * a.H + post] = r1;
+    const size_t bq = (size_t)q * NS + SPT * sub;
+#pragma unroll
+    for (int k = 0; k < TC; ++k) {
+        if (tc + k >= t1) break;
+        float r0, r1;
+        mine(acc[k], sub, r0, r1);
+        a.g_seg[((size_t)(tc + k - t0) * a.B + bq) * a.H + post] = r0;
+        a.g_seg[((size_t)(tc + k - t0) * a.B + bq + 1) * a.H + post] = r1;
+    }
 }
 
 // The membrane of the segment from its checkpoint, one thread per (sample, neuron): Vpre as the forward made it,
@@ -687,6 +731,8 @@ int check_desc(const n2b_bptt_desc *d) {
         return bfail(N2B_EINVAL, "hidden must be a multiple of 32, at most 1024");
     if (d->readouts <= 0 || d->readouts > 32) return bfail(N2B_EINVAL, "readouts must be in 1..32");
     if (d->steps <= 0 || d->checkpoint <= 0) return bfail(N2B_EINVAL, "steps and checkpoint must be positive");
+    if ((int64_t)d->steps * (d->batch / NS) * d->hidden >= ((int64_t)1 << 31))
+        return bfail(N2B_EINVAL, "steps x batch / 8 x hidden must stay below 2^31");
     if (d->smooth && d->hidden > 256) return bfail(N2B_EINVAL, "the smooth model is for hidden <= 256");
     if (d->nnz < 0 || (d->nnz > 0 && (!d->in_code || !d->out_code || !d->out_perm)))
         return bfail(N2B_EINVAL, "missing link arrays");
@@ -849,7 +895,7 @@ int n2b_bptt_backward(const n2b_bptt_desc *d, const float *u, const float *w_rec
     const int K = d->checkpoint, nseg = a.nseg;
     for (int seg = nseg - 1; seg >= 0; --seg) {  // each segment: recompute from its checkpoint, then backwards
         const int t0 = seg * K, t1 = std::min(d->steps, t0 + K);
-        const size_t nr = (size_t)(t1 - t0) * (d->batch / NS) * d->hidden * NT;
+        const size_t nr = (size_t)((t1 - t0 + TC - 1) / TC) * (d->batch / NS) * d->hidden * NT;
         const unsigned rblocks = (unsigned)((nr + 255) / 256), vblocks = (unsigned)((d->batch * d->hidden + 255) / 256);
         if (smooth) {
             recompute_r_kernel<true><<<rblocks, 256, 0, s>>>(a, t0, t1);
