@@ -50,23 +50,35 @@ def literal(v) -> str:
     raise NotImplementedError(f"a constant of type {type(v).__name__} cannot be lowered")
 
 
-class HookContext:
-    """What a hook's names refer to. self_attrs: dynamic attr -> python type; self_static: static attr ->
-    value; edge_dynamic: per-link edge attrs (hook-facing names); edge_static: hook-facing name -> value."""
+class Root:
+    """An object a hook reads attributes of: `prefix` + name for its register copies of dynamic attributes
+    (python type per name), literals for its static ones, and whether the hook may assign it."""
 
-    def __init__(self, self_attrs: dict, self_static: dict, time_name: str | None = None,
-                 edge_name: str | None = None, source_name: str | None = None,
+    def __init__(self, prefix: str, dynamic: dict, static: dict, writable: bool, what: str):
+        self.prefix, self.dynamic, self.static, self.writable, self.what = prefix, dynamic, static, writable, what
+
+
+class HookContext:
+    """What a hook's names refer to. A node hook: self_attrs (dynamic attr -> python type) and self_static
+    (static attr -> value) of its neuron; for receive, edge_dynamic (per-link edge attrs, hook-facing names)
+    and edge_static (hook-facing name -> value). An edge hook (forward/backward) passes `roots` instead:
+    self = the link's edge state, the destination = the neuron's state. `refused`: parameter names whose
+    attributes may not be used (the sending neuron), `random`: whether random.random() may be called."""
+
+    def __init__(self, self_attrs: dict | None = None, self_static: dict | None = None,
+                 time_name: str | None = None, edge_name: str | None = None, source_name: str | None = None,
                  edge_dynamic: set | None = None, edge_static: dict | None = None, site_base: int = 0,
-                 in_receive: bool = False):
-        self.self_attrs = self_attrs
-        self.self_static = self_static
+                 roots: dict | None = None, random: bool = True):
+        self.self_attrs = self_attrs or {}
         self.time_name = time_name
-        self.edge_name = edge_name
-        self.source_name = source_name
-        self.edge_dynamic = edge_dynamic or set()
-        self.edge_static = edge_static or {}
         self.site = site_base  # random call sites numbered from here
-        self.in_receive = in_receive
+        self.random = random
+        self.roots = dict(roots) if roots is not None else {
+            "self": Root("s_", self.self_attrs, dict(self_static or {}), True, "the neuron")}
+        if edge_name is not None and roots is None:
+            self.roots[edge_name] = Root("e_", {n: float for n in (edge_dynamic or ())}, dict(edge_static or {}),
+                                         False, "the link")
+        self.refused = {source_name} if source_name is not None else set()
 
 
 class CudaLowering:
@@ -133,15 +145,22 @@ class CudaLowering:
     def target(self, t) -> str:
         if isinstance(t, ast.Name):
             return f"l_{t.id}"
-        if isinstance(t, ast.Attribute) and isinstance(t.value, ast.Name) and t.value.id == "self":
-            if t.attr not in self.ctx.self_attrs:
-                self.fail(t, f"assigning self.{t.attr}, which is not a dynamic attribute")
-            return f"s_{t.attr}"
+        if isinstance(t, ast.Attribute) and isinstance(t.value, ast.Name):
+            if t.value.id in self.ctx.refused:
+                self.fail(t, f"{t.value.id}.<attr> (the sending neuron's state)")
+            root = self.ctx.roots.get(t.value.id)
+            if root is not None:
+                if not root.writable:
+                    self.fail(t, f"assigning {t.value.id}.{t.attr} ({root.what} is read-only here)")
+                if t.attr not in root.dynamic:
+                    self.fail(t, f"assigning {t.value.id}.{t.attr}, which is not a dynamic attribute")
+                return f"{root.prefix}{t.attr}"
         self.fail(t, "this assignment target")
 
     def cast_for(self, t, expr: str) -> str:
         if isinstance(t, ast.Attribute):
-            ty = self.ctx.self_attrs.get(t.attr, float)
+            root = self.ctx.roots.get(t.value.id) if isinstance(t.value, ast.Name) else None
+            ty = root.dynamic.get(t.attr, float) if root is not None else float
             if ty is bool:
                 return f"(({expr}) != 0)"
             return f"({_CTYPE.get(ty, 'float')})({expr})"
@@ -182,20 +201,15 @@ class CudaLowering:
         if isinstance(e, ast.Attribute):
             if isinstance(e.value, ast.Name):
                 base = e.value.id
-                if base == "self":
-                    if e.attr in c.self_attrs:
-                        return f"s_{e.attr}"
-                    if e.attr in c.self_static:
-                        return literal(c.self_static[e.attr])
-                    self.fail(e, f"self.{e.attr} (not an attribute of the node)")
-                if c.edge_name is not None and base == c.edge_name:
-                    if e.attr in c.edge_dynamic:
-                        return f"e_{e.attr}"
-                    if e.attr in c.edge_static:
-                        return literal(c.edge_static[e.attr])
-                    self.fail(e, f"edge.{e.attr} (the connection has no such attribute)")
-                if c.source_name is not None and base == c.source_name:
-                    self.fail(e, "source.<attr> (reading the sending neuron's state)")
+                root = c.roots.get(base)
+                if root is not None:
+                    if e.attr in root.dynamic:
+                        return f"{root.prefix}{e.attr}"
+                    if e.attr in root.static:
+                        return literal(root.static[e.attr])
+                    self.fail(e, f"{base}.{e.attr} ({root.what} has no such attribute)")
+                if base in c.refused:
+                    self.fail(e, f"{base}.<attr> (reading the sending neuron's state)")
                 if base == "math" and e.attr in ("pi", "e", "inf", "tau"):
                     return flit(getattr(math, e.attr))
             self.fail(e, "this attribute")
@@ -241,6 +255,8 @@ class CudaLowering:
             if mod == "math" and name in _MATH:
                 return f"{_MATH[name]}(" + ", ".join(f"(float)({a})" for a in args) + ")"
             if mod == "random" and name == "random" and not args:
+                if not self.ctx.random:
+                    self.fail(e, "random.random() in an edge hook")
                 site = self.ctx.site
                 self.ctx.site += 1
                 return f"n2_uniform(p, j, n, {site}u, link_k)"

@@ -10,6 +10,7 @@ spikes, status, check, counters, reset_counters, close.
 
 from __future__ import annotations
 
+import ast
 import ctypes
 import hashlib
 
@@ -18,7 +19,7 @@ import torch
 
 from .. import _lib
 from ..topology import delay_steps, pull_form
-from .template import build_source, ctype_of, hook_context, params_type
+from .template import build_source, ctype_of, edge_hook_context, hook_context, params_type
 
 BLOCK = 128
 _CACHE: dict = {}  # (source hash, device) -> n2b_jit_kernel handle, for the process's lifetime
@@ -35,26 +36,58 @@ def compile_source(source: str, device: int) -> ctypes.c_void_p:
     return _CACHE[key]
 
 
-def edge_values(conn, hook_ctx_names: set):
-    """(per-link names, {hook name: scalar}) of the edge attributes a receive hook reads on this connection."""
-    fabric = conn.fabric
-    rename = {hook_name: real for real, hook_name in (conn._fabric_map or {}).items()}
-    dynamic, static = [], {}
-    for name in sorted(hook_ctx_names):
-        v = fabric.value(rename.get(name, name))
-        if v is None:
-            raise ValueError(f"{conn!r}: the receive hook reads edge.{name}, which the connection does not have")
-        if isinstance(v, torch.Tensor) and v.numel() != 1:
-            dynamic.append(name)
-        else:
-            static[name] = float(v.item() if isinstance(v, torch.Tensor) else v)
-    return dynamic, static
+def trivial(hook) -> bool:
+    """A hook whose body does nothing (pass / a docstring)."""
+    if hook is None:
+        return True
+    return all(isinstance(st, ast.Pass) or (isinstance(st, ast.Expr) and isinstance(st.value, ast.Constant))
+               for st in hook.ast.body)
+
+
+class EdgePlan:
+    """What a connection's hooks read and write of its links. recv: {receive-facing name: edge name};
+    per_link: edge names held per link (assigned by the edge hooks, or set as per-link tensors); written:
+    those the edge hooks assign; static: {edge name: value} of the rest; forward / backward: the edge's
+    non-trivial hooks (or None)."""
+
+    def __init__(self, conn, receive_hook):
+        from .. import receives
+        from ..hook import used_members
+
+        fabric = conn.fabric
+        rename = {hook_name: real for real, hook_name in (conn._fabric_map or {}).items()}
+        edge_param = receive_hook.parameter_type_to_name.get(receives.edge, "edge") if receive_hook else "edge"
+        names = used_members(receive_hook.ast, edge_param) if receive_hook is not None else set()
+        self.recv = {h: rename.get(h, h) for h in sorted(names)}
+        has_edge = fabric.instance is not None
+        self.forward = None if not has_edge or trivial(fabric.edge["forward"]) else fabric.edge["forward"]
+        self.backward = None if not has_edge or trivial(fabric.edge["backward"]) else fabric.edge["backward"]
+        used, written = set(self.recv.values()), set()
+        for h in (self.forward, self.backward):
+            if h is not None:
+                used |= used_members(h.ast, "self")
+                written |= h.assigned_members
+        self.written = sorted(written)
+        self.per_link, self.static = [], {}
+        for name in sorted(used):
+            v = fabric.value(name)
+            if v is None:
+                raise ValueError(f"{conn!r}: edge.{name} is read but the connection has no such attribute")
+            if name in written or (isinstance(v, torch.Tensor) and v.numel() != 1):
+                self.per_link.append(name)
+            else:
+                self.static[name] = float(v.item() if isinstance(v, torch.Tensor) else v)
+
+    def initial(self, conn, name: str, n_links: int) -> torch.Tensor:
+        """A per-link array's starting values, canonical order, float32 on the CPU."""
+        v = conn.fabric.value(name)
+        if isinstance(v, torch.Tensor) and v.numel() == n_links:
+            return v.detach().reshape(-1).to("cpu", torch.float32)
+        return torch.full((n_links,), float(v.item() if isinstance(v, torch.Tensor) else v), dtype=torch.float32)
 
 
 class JitRuntime:
     def __init__(self, net):
-        from ..hook import used_members
-
         self.net = net
         dev = self.device = net.device
         dindex = dev.index if dev.index is not None else 0
@@ -82,6 +115,7 @@ class JitRuntime:
         self.rec_step0 = net.step_count
         self.rasters = [torch.zeros(max(1, self.record_rows) * w, dtype=torch.int32, device=dev) for w in words]
         self.kernels, self.params, self.sources = [], [], []
+        self.edge_arrays = {}  # (connection id, edge name) -> (per-link values in pull order, pull permutation)
         for k, p in enumerate(pops):
             node = p.node
             incoming, ctx_in = [], []
@@ -92,11 +126,19 @@ class JitRuntime:
                 hook = node.receive.get(port)
                 if hook is None:
                     raise ValueError(f"{p!r} has no receive port {port!r}")
-                names = used_members(hook.ast, hook.parameter_type_to_name.get(_edge_type(), "edge"))
-                dyn, stat = edge_values(c, names)
+                plan = EdgePlan(c, hook)
+                dyn = [h for h, real in plan.recv.items() if real in plan.per_link]
+                stat = {h: plan.static[real] for h, real in plan.recv.items() if real not in plan.per_link}
                 ctx = hook_context(p, hook, dyn, stat, site_base=site)
                 site += 32
-                incoming.append({"receive": (hook.ast, ctx), "edge_dynamic": dyn, "conn": c})
+                inc = {"receive": (hook.ast, ctx), "edge_dynamic": plan.per_link, "edge_written": plan.written,
+                       "alias": {h: real for h, real in plan.recv.items() if real in plan.per_link and h != real},
+                       "forward": None, "backward": None, "conn": c, "plan": plan}
+                for kind in ("forward", "backward"):
+                    eh = getattr(plan, kind)
+                    if eh is not None:
+                        inc[kind] = (eh.ast, edge_hook_context(p, eh, plan.per_link, plan.static))
+                incoming.append(inc)
             hooks = {"update": (node.update.ast, hook_context(p, node.update, site_base=site)),
                      "send": (node.send.ast, hook_context(p, node.send, site_base=site + 32))}
             src, fields = build_source(type(p.instance).__name__, dict(p.dynamic_attrs), hooks, incoming)
@@ -129,10 +171,11 @@ class JitRuntime:
                 setattr(P, f"c{ci}_src_bits", self.bits[s].data_ptr())
                 setattr(P, f"c{ci}_src_words", words[s])
                 setattr(P, f"c{ci}_src_mask", depth[s] - 1)
-                rename = {hn: real for real, hn in (c._fabric_map or {}).items()}
-                for e in inc["edge_dynamic"]:
-                    v = c.fabric.value(rename.get(e, e)).detach().reshape(-1).to(torch.float32)
-                    v = self._dev(v.to(perm.device)[perm] if v.numel() else torch.zeros(1))
+                plan = inc["plan"]
+                for e in plan.per_link:
+                    v = plan.initial(c, e, len(topo))
+                    v = self._dev(v[perm.cpu()] if v.numel() else torch.zeros(1))
+                    self.edge_arrays[(id(c), e)] = (v, perm.cpu())
                     setattr(P, f"c{ci}_e_{e}", v.data_ptr())
             self.params.append(P)
         self.stream = torch.cuda.Stream(device=dev)
@@ -190,6 +233,17 @@ class JitRuntime:
         steps, ids = np.nonzero(self.raster(pop))
         return steps.astype(np.int64) + self.rec_step0, ids.astype(np.int64)
 
+    def edge_state(self, conn, name: str) -> torch.Tensor:
+        """A per-link edge value (a weight the edge hooks change, ...) in canonical link order."""
+        if (id(conn), name) not in self.edge_arrays:
+            raise KeyError(f"{name} is not held per link on this connection")
+        self.stream.synchronize()
+        v, perm = self.edge_arrays[(id(conn), name)]
+        out = torch.empty_like(v)
+        if perm.numel():
+            out[perm.to(v.device)] = v[: perm.numel()]
+        return out[: perm.numel()]
+
     def status(self) -> list:
         self.stream.synchronize()
         return self.err.cpu().tolist()
@@ -213,9 +267,3 @@ class JitRuntime:
     def close(self) -> None:
         self.stream.synchronize()
         self.kernels = []
-
-
-def _edge_type():
-    from .. import receives
-
-    return receives.edge

@@ -59,7 +59,10 @@ def build_source(pop_name: str, attrs: dict, hooks: dict, incoming: list) -> tup
     """(CUDA source, params fields [(name, C type, ctypes type)]) of one population.
 
     attrs: dynamic attr -> python type; hooks: {"update": (fn_ast, ctx), "send": (fn_ast, ctx)};
-    incoming: one dict per incoming connection {"receive": (fn_ast, ctx) or None, "edge_dynamic": [names]}."""
+    incoming: one dict per incoming connection: "receive": (fn_ast, ctx) or None; "edge_dynamic": the per-link
+    arrays by the edge's own attribute names; "edge_written": those the edge hooks assign (stored back);
+    "alias": {receive-facing name: edge name} where they differ; "forward" / "backward": (fn_ast, ctx) of the
+    edge hooks or None."""
     fields = [("step", "long long", ctypes.c_int64), ("rec0", "long long", ctypes.c_int64),
               ("raster_steps", "long long", ctypes.c_int64), ("t", "float", ctypes.c_float),
               ("n", "int", ctypes.c_int32), ("words", "int", ctypes.c_int32), ("bit_mask", "int", ctypes.c_int32),
@@ -74,7 +77,8 @@ def build_source(pop_name: str, attrs: dict, hooks: dict, incoming: list) -> tup
                    (f"c{c}_src_bits", "const u32 *", ctypes.c_void_p),
                    (f"c{c}_src_words", "int", ctypes.c_int32), (f"c{c}_src_mask", "int", ctypes.c_int32)]
         for e in inc["edge_dynamic"]:
-            fields.append((f"c{c}_e_{e}", "const float *", ctypes.c_void_p))
+            fields.append((f"c{c}_e_{e}", "float *" if e in inc.get("edge_written", ()) else "const float *",
+                           ctypes.c_void_p))
 
     src = [_PRELUDE, "struct Params {\n"]
     src += [f"    {ct} {name};\n" for name, ct, _ in fields]
@@ -97,11 +101,20 @@ __device__ __forceinline__ float n2_uniform(const Params &p, int j, long long n,
         src.append(f"    {ct} s_{a} = live ? p.s_{a}[j] : ({ct})0;\n")
     src.append("    if (live) {\n")
     for c, inc in enumerate(incoming):
-        if inc["receive"] is None:
+        if inc["receive"] is None and inc.get("forward") is None:
             continue
-        fn, ctx = inc["receive"]
-        body = lower_hook(fn, ctx, f"{pop_name} receive (connection {c})")
-        loads = "".join(f"            const float e_{e} = p.c{c}_e_{e}[l];\n" for e in inc["edge_dynamic"])
+        body = ""
+        if inc.get("forward") is not None:
+            fn, ctx = inc["forward"]
+            body += lower_hook(fn, ctx, f"{pop_name} edge forward (connection {c})")
+        body += "".join(f"const float e_{h} = e_{real};\n" for h, real in inc.get("alias", {}).items())
+        if inc["receive"] is not None:
+            fn, ctx = inc["receive"]
+            body += lower_hook(fn, ctx, f"{pop_name} receive (connection {c})")
+        body += "".join(f"p.c{c}_e_{e}[l] = e_{e};\n" for e in inc.get("edge_written", ()))
+        if inc.get("alias"):
+            body = "{\n" + body + "}\n"
+        loads = "".join(f"            float e_{e} = p.c{c}_e_{e}[l];\n" for e in inc["edge_dynamic"])
         src.append(f"""        for (int l = p.c{c}_ptr[j]; l < p.c{c}_ptr[j + 1]; ++l) {{
             const u32 w = p.c{c}_link[l];
             const int src = (int)(w & 0xFFFFFFu), d = (int)(w >> 24);
@@ -118,6 +131,18 @@ __device__ __forceinline__ float n2_uniform(const Params &p, int j, long long n,
         fn, ctx = hooks[name]
         body = lower_hook(fn, ctx, f"{pop_name} {name}")
         src.append("        " + body.replace("\n", "\n        ").rstrip() + "\n")
+    backward = [(c, inc) for c, inc in enumerate(incoming) if inc.get("backward") is not None]
+    if backward:  # the neuron fired: every incoming link's edge backward hook, connection by connection
+        src.append("        if (fired) {\n")
+        for c, inc in backward:
+            fn, ctx = inc["backward"]
+            body = lower_hook(fn, ctx, f"{pop_name} edge backward (connection {c})")
+            body += "".join(f"p.c{c}_e_{e}[l] = e_{e};\n" for e in inc.get("edge_written", ()))
+            loads = "".join(f"                float e_{e} = p.c{c}_e_{e}[l];\n" for e in inc["edge_dynamic"])
+            src.append(f"            for (int l = p.c{c}_ptr[j]; l < p.c{c}_ptr[j + 1]; ++l) {{\n{loads}")
+            src.append("                " + body.replace("\n", "\n                ").rstrip() + "\n")
+            src.append("            }\n")
+        src.append("        }\n")
     src.append("    }\n")
     src.append(r'''    const u32 b = __ballot_sync(0xffffffffu, live && fired);
     const u32 arrivals = __reduce_add_sync(0xffffffffu, arrived);
@@ -141,6 +166,23 @@ __device__ __forceinline__ float n2_uniform(const Params &p, int j, long long n,
 def params_type(fields: list):
     """The ctypes structure of a Params block."""
     return type("Params", (ctypes.Structure,), {"_fields_": [(name, cty) for name, _, cty in fields]})
+
+
+def edge_hook_context(pop, hook, per_link: list, edge_static: dict) -> HookContext:
+    """An edge hook's names: self = the link (per-link arrays, the edge's static values), the destination =
+    the target neuron's state; the source's state and random draws are refused."""
+    from .. import receives
+    from .cuda import Root
+
+    names = {ty: nm for ty, nm in hook.parameter_type_to_name.items()}
+    static = {k: v for k, v in pop.instance.__dict__.items()
+              if k not in pop.dynamic_attrs and isinstance(v, (int, float, bool))}
+    roots = {"self": Root("e_", {n: float for n in per_link}, dict(edge_static), True, "the link")}
+    if receives.destination in names:
+        roots[names[receives.destination]] = Root("s_", dict(pop.dynamic_attrs), static, True,
+                                                  "the destination neuron")
+    return HookContext(time_name=names.get(receives.time), source_name=names.get(receives.source), roots=roots,
+                       random=False)
 
 
 def hook_context(pop, hook, edge_dynamic=(), edge_static=None, site_base: int = 0) -> HookContext:

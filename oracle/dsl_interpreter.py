@@ -48,14 +48,28 @@ class _Self:
         self._a[name][self._j] = value
 
 
-class _Edge:
-    def __init__(self, values: dict):
+class _Link:
+    """A link's edge values: per-link float32 arrays (pull order) and static float32 values; `names` maps the
+    names a hook uses to the edge's own names; the arrays are writable where `writable`."""
+
+    def __init__(self, values: dict, names: dict | None = None, writable: bool = False):
         object.__setattr__(self, "_v", values)
+        object.__setattr__(self, "_n", names)
+        object.__setattr__(self, "_w", writable)
         object.__setattr__(self, "_l", 0)
 
+    def _real(self, name):
+        n = object.__getattribute__(self, "_n")
+        return n.get(name, name) if n is not None else name
+
     def __getattr__(self, name):
-        v = object.__getattribute__(self, "_v")[name]
+        v = object.__getattribute__(self, "_v")[self._real(name)]
         return v[object.__getattribute__(self, "_l")] if isinstance(v, np.ndarray) else v
+
+    def __setattr__(self, name, value):
+        if not self._w:
+            raise AttributeError("the link is read-only in a receive hook")
+        self._v[self._real(name)][self._l] = value
 
 
 def _f32(v):
@@ -64,7 +78,12 @@ def _f32(v):
 
 def run(net, n_steps: int):
     """Run `net` (its populations' current state tensors, on the CPU) for n_steps from step 0; returns
-    (rasters: [bool [n_steps, n]] per population, final state: [{attr: array}] per population)."""
+    (rasters: [bool [n_steps, n]] per population, final state: [{attr: array}] per population, per-link edge
+    values the edge hooks change: {(connection index, name): array in canonical order}).
+
+    Edge hooks: at an arrival the link's forward hook runs before the receive hook; when a neuron fires, the
+    backward hook of every incoming link runs after send (connection order, link order). Their `self` is the
+    link, their destination the neuron."""
     dt = float(net.resolution)
     pops = list(net.populations)
     index = {id(p): k for k, p in enumerate(pops)}
@@ -78,27 +97,26 @@ def run(net, n_steps: int):
         static = {k: _f32(v) for k, v in p.instance.__dict__.items()
                   if k not in p.dynamic_attrs and isinstance(v, (int, float, bool))}
         selves.append(_Self(arr, static))
+    from naer2_b200.transpiler.runtime import EdgePlan
+
     incoming = [[] for _ in pops]
-    for c in net.connections:
+    edge_state = {}
+    for ci, c in enumerate(net.connections):
         t = index[id(c._target)]
         topo = c.fabric.topology
         steps = delay_steps(c.fabric.value("delay"), len(topo), dt, device="cpu")
-        ptr, link, perm = pull_form(topo.to("cpu") if hasattr(topo, "to") else topo, steps.cpu(), len(pops[t].shape))
+        ptr, link, perm = pull_form(topo, steps.cpu(), len(pops[t].shape))
+        perm = perm.cpu()
         port = c._target_port or "receive"
         hook = pops[t].node.receive[port]
-        rename = {hn: real for real, hn in (c._fabric_map or {}).items()}
-        from naer2_b200.hook import used_members
-
-        names = used_members(hook.ast, hook.parameter_type_to_name.get(receives.edge, "edge"))
-        values = {}
-        for nm in names:
-            v = c.fabric.value(rename.get(nm, nm))
-            if isinstance(v, torch.Tensor) and v.numel() != 1:
-                values[nm] = v.detach().reshape(-1).cpu()[perm.cpu()].numpy().astype(np.float32)
-            else:
-                values[nm] = np.float32(float(v.item() if isinstance(v, torch.Tensor) else v))
+        plan = EdgePlan(c, hook)
+        values = {n: plan.initial(c, n, len(topo))[perm].numpy().copy() for n in plan.per_link}
+        values.update({n: np.float32(v) for n, v in plan.static.items()})
+        for n in plan.written:
+            edge_state[(ci, n)] = (values[n], perm.numpy())
         w = link.cpu().numpy().astype(np.int64) & 0xFFFFFFFF
-        incoming[t].append((index[id(c._source)], ptr.cpu().numpy(), w & 0xFFFFFF, w >> 24, hook, _Edge(values)))
+        incoming[t].append((index[id(c._source)], ptr.cpu().numpy(), w & 0xFFFFFF, w >> 24, hook,
+                            _Link(values, plan.recv), plan, _Link(values, None, writable=True)))
     spikes = [np.zeros((n_steps, len(p.shape)), dtype=bool) for p in pops]
 
     state = {"fired": False, "j": 0, "n": 0, "k": 0xFFFFFF, "site": 0, "seed": (0, 0)}
@@ -113,7 +131,7 @@ def run(net, n_steps: int):
         w = philox([state["j"], n & 0xFFFFFFFF, (n >> 32) & 0xFFFFFFFF, c3], state["seed"])[0]
         return np.float32((w >> 8) * 5.9604644775390625e-08)
 
-    def call(hook, obj, t, edge=None, site_base=0):
+    def call(hook, obj, t, edge=None, site_base=0, dst=None):
         kw = {}
         for ty, nm in hook.parameter_type_to_name.items():
             if ty is receives.time:
@@ -122,6 +140,8 @@ def run(net, n_steps: int):
                 kw[nm] = edge
             elif ty is receives.source:
                 kw[nm] = None
+            elif ty is receives.destination:
+                kw[nm] = dst
         state["site"] = site_base
         hook.function(obj, **kw)
 
@@ -139,19 +159,34 @@ def run(net, n_steps: int):
                 for j in range(len(p.shape)):
                     object.__setattr__(obj, "_j", j)
                     state["j"], state["fired"], arrived = j, False, 0
-                    for ci, (s, ptr, src, d, hook, edge) in enumerate(incoming[k]):
+                    for ci, (s, ptr, src, d, hook, edge, plan, link) in enumerate(incoming[k]):
                         for l in range(ptr[j], ptr[j + 1]):
                             m = n - int(d[l])
                             if m < 0 or not spikes[s][m, src[l]]:
                                 continue
                             object.__setattr__(edge, "_l", l)
+                            object.__setattr__(link, "_l", l)
                             state["k"] = arrived
                             arrived += 1
+                            if plan.forward is not None:
+                                call(plan.forward, link, t, dst=obj)
                             call(hook, obj, t, edge, site_base=32 * ci)
                     state["k"] = 0xFFFFFF
                     call(node.update, obj, t, site_base=32 * n_recv)
                     call(node.send, obj, t, site_base=32 * n_recv + 32)
                     spikes[k][n, j] = state["fired"]
+                    if state["fired"]:  # every incoming link's edge backward hook
+                        for (s, ptr, src, d, hook, edge, plan, link) in incoming[k]:
+                            if plan.backward is None:
+                                continue
+                            for l in range(ptr[j], ptr[j + 1]):
+                                object.__setattr__(link, "_l", l)
+                                call(plan.backward, link, t, dst=obj)
     finally:
         n2.spike, _random.random = saved
-    return spikes, arrays
+    edges = {}
+    for (ci, name), (v, perm) in edge_state.items():  # back to canonical link order
+        out = np.empty_like(v)
+        out[perm] = v
+        edges[(ci, name)] = out
+    return spikes, arrays, edges

@@ -124,3 +124,50 @@ class Syn:
 
     def backward(self):
         pass
+
+
+@n2.node
+class TraceLIF:
+    """A leaky neuron keeping a postsynaptic trace (y_post, decaying from its last spike t_post) for STDP."""
+
+    def __init__(self, decay: float = 0.9, theta: float = 1.0, tau_post: float = 2.0):
+        self.decay, self.theta, self.tau_post = decay, theta, tau_post
+        self.v: float = 0.0
+        self.y_post: float = 0.0
+        self.t_post: float = 0.0
+
+    def update(self, time: n2.time):
+        self.v = self.v * self.decay
+
+    def send(self, time: n2.time):
+        if self.v >= self.theta:
+            n2.spike()
+            self.v = 0.0
+            self.y_post = self.y_post * math.exp((self.t_post - time) / self.tau_post) + 1.0
+            self.t_post = time
+
+    def receive(self, time: n2.time, edge: r.edge, source: r.source):
+        self.v += edge.weight
+
+
+@n2.edge
+class PairSTDP:
+    """Pair-based STDP: a presynaptic trace per link, the postsynaptic trace on the target; depression at a
+    presynaptic arrival (forward), potentiation when the target fires (backward), weights kept in [0, w_max]."""
+
+    def __init__(self, weight: float = 0.5, tau_pre: float = 2.0, tau_post: float = 2.0, a_plus: float = 0.05,
+                 a_minus: float = 0.04, w_max: float = 1.0):
+        self.weight = weight
+        self.x_pre = 0.0
+        self.t_last = 0.0
+        self.tau_pre, self.tau_post, self.a_plus, self.a_minus, self.w_max = tau_pre, tau_post, a_plus, a_minus, w_max
+
+    def forward(self, time: n2.time, dst: r.destination):
+        self.x_pre = self.x_pre * math.exp((self.t_last - time) / self.tau_pre) + 1.0
+        self.t_last = time
+        y = dst.y_post * math.exp((dst.t_post - time) / self.tau_post)
+        self.weight = max(self.weight - self.a_minus * y, 0.0)
+
+    def backward(self, time: n2.time, dst: r.destination):
+        x = self.x_pre * math.exp((self.t_last - time) / self.tau_pre)
+        self.weight = min(self.weight + self.a_plus * x, self.w_max)

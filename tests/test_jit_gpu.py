@@ -20,7 +20,7 @@ pytestmark = pytest.mark.gpu
 
 
 def check_against_interpreter(net, steps):
-    rasters, state = dsl_interpreter.run(net, steps)  # before the GPU run: the same initial state and seeds
+    rasters, state, edges = dsl_interpreter.run(net, steps)  # before the GPU run: the same initial state and seeds
     net.record(steps)
     net.run_steps(steps)
     assert isinstance(net.runtime, JitRuntime)
@@ -90,3 +90,30 @@ def test_a_compile_error_carries_the_nvrtc_log(cuda):
     assert rc == -1
     msg = lib.n2b_last_error().decode()
     assert "NVRTC compile failed" in msg and "undefined_name" in msg
+
+
+def test_pair_stdp_edge_hooks_change_the_weights_as_the_interpreter_does(cuda):
+    from tests.dsl_models import PairSTDP, TraceLIF
+
+    g = torch.Generator().manual_seed(9)
+    src = Pacemaker(period=5) * 40
+    tgt = TraceLIF(theta=1.2) * 30
+    c = src >> PairSTDP() @ fixed_indegree(10, seed=10) >> tgt
+    c.weight = 0.2 + 0.6 * torch.rand(c.shape, generator=g)
+    c.delay = (torch.randint(1, 4, c.shape, generator=g) * 0.1).double()
+    src.phase = torch.randint(0, 5, (40,), generator=g, dtype=torch.int32)
+    net = src.network
+    net.resolution = 0.1
+    rasters, state, edges = dsl_interpreter.run(net, 200)
+    net.record(200)
+    net.run_steps(200)
+    net.check()
+    for k, p in enumerate(net.populations):
+        assert np.array_equal(net.runtime.raster(p), rasters[k]), k
+    assert rasters[1].sum() > 20
+    w0 = c.fabric.value("weight").numpy()
+    for name in ("weight", "x_pre", "t_last"):
+        got = net.runtime.edge_state(c, name).cpu().numpy()
+        np.testing.assert_allclose(got, edges[(0, name)], rtol=1e-5, atol=1e-6, err_msg=name)
+    moved = np.abs(net.runtime.edge_state(c, "weight").cpu().numpy() - w0)
+    assert (moved > 1e-3).mean() > 0.5  # learning happened on most links

@@ -90,6 +90,26 @@ def test_interpreter_runs_a_small_network():
     src.phase = torch.arange(8, dtype=torch.int32)
     net = src.network
     net.resolution = 0.1
-    rasters, state = dsl_interpreter.run(net, 30)
+    rasters, state, _ = dsl_interpreter.run(net, 30)
     assert rasters[0].sum() == sum(((np.arange(8) + n + 1) % 5 == 0).sum() for n in range(30))
     assert rasters[1].sum() > 0 and (state[1]["v"] < 0.25).all()
+
+
+def test_edge_hooks_lower_and_refuse_the_source():
+    from tests.dsl_models import PairSTDP, TraceLIF
+
+    tgt = TraceLIF() * 4
+    src = Pacemaker() * 4
+    c = src >> PairSTDP() @ fixed_indegree(2, seed=1) >> tgt
+    from naer2_b200.transpiler.runtime import EdgePlan
+    from naer2_b200.transpiler.template import edge_hook_context
+
+    plan = EdgePlan(c, tgt.node.receive["receive"])
+    assert plan.per_link == ["t_last", "weight", "x_pre"] and plan.written == ["t_last", "weight", "x_pre"]
+    assert plan.static["tau_pre"] == 2.0 and plan.forward is not None and plan.backward is not None
+    out = lower_hook(plan.forward.ast, edge_hook_context(tgt, plan.forward, plan.per_link, plan.static), "fwd")
+    assert "e_x_pre = " in out and "s_y_post" in out and "e_weight = " in out
+    bad = ast.parse("def forward(self, time, src):\n    x = src.v\n").body[0]
+    ctx = HookContext(time_name="time", source_name="src", roots={}, random=False)
+    with pytest.raises(NotImplementedError, match="sending neuron"):
+        lower_hook(bad, ctx, "fwd")
