@@ -111,8 +111,9 @@ typedef struct n2b_connection {
 typedef struct n2b_options {
     int32_t block;   /* neurons (threads) per block: 64, 128 or 256 (0: 128) */
     int32_t device;  /* CUDA device ordinal of every pointer */
-    int32_t grid;    /* blocks per launch (0: two per SM; per-step launches: at least one per tile;
-                        persistent: at most the co-resident blocks, each looping over its tiles) */
+    int32_t grid;    /* blocks per launch (0: per-step launches two per SM and at least one per tile;
+                        persistent one per SM, at least tiles + half an SM's worth, at most the co-resident
+                        blocks, each looping over its tiles) */
     int32_t persistent; /* 1: a window of steps is one cooperative launch, steps separated by a grid
                            barrier; 0: one launch per step */
 } n2b_options;

@@ -351,9 +351,11 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     const int persistent = opt && opt->persistent;
     const bool inl = n_pops <= n2b::INLINE_POPS && (int32_t)push.size() <= n2b::INLINE_PUSH &&
                      (int32_t)pull.size() <= n2b::INLINE_PULL;
-    // default: two blocks per SM, and for persistent windows at least one per tile plus half an SM's worth of
-    // tile-free blocks for the far links (capped by what can be resident)
-    int want = (opt && opt->grid > 0) ? opt->grid : std::max(2 * sms, persistent ? L.n_tiles + sms / 2 : 0);
+    // default: per-step launches two blocks per SM; persistent windows one per SM, and at least one per tile
+    // plus half an SM's worth of tile-free blocks for the far links (capped by what can be resident; a
+    // smaller grid makes the grid barrier cheaper: config 1 steps 2-4% faster at 148 blocks than at 296)
+    int want = (opt && opt->grid > 0) ? opt->grid
+                                      : (persistent ? std::max(sms, L.n_tiles + sms / 2) : 2 * sms);
     int grid = std::max(L.n_tiles, want);
     if (persistent) {
         int most = 0;
