@@ -32,6 +32,8 @@ class Network:
         self.device = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else None
         self.record_steps: int = 0  # raster rows kept per population (Network.record)
         self.tuned: dict = {}  # per connection id: the push/pull choice the tuner measured (naer2_b200.tune)
+        # event-driven intake at exact spike times (the transpiled path; naer2_b200.transpiler.template)
+        self.exact: bool = False
         self.tune_report: dict | None = None
         self._runtime = None
 
@@ -70,7 +72,7 @@ class Network:
             from .models import BUILTIN
             from .runtime import NetworkRuntime
 
-            if all(type(p.instance) in BUILTIN for p in self.populations):
+            if not self.exact and all(type(p.instance) in BUILTIN for p in self.populations):
                 self._runtime = NetworkRuntime(self)
             else:  # a model without a built-in kernel: every population's hooks transpiled, compiled at run time
                 from .transpiler import JitRuntime

@@ -7,7 +7,7 @@ link). Names are resolved as follows:
   edge.<x>   a per-link attribute -> e_<x> (loaded per link); a scalar one -> its literal value
   time       (the parameter annotated n2.time) -> t, the step's time
   locals     -> float l_<name>, declared at the top of the hook (Python locals are function-scoped)
-  n2.spike(...) -> fired = true (the spike is recorded at this step; a time argument is accepted, unused)
+  n2.spike(t) -> the neuron fires at time t (default: the hook's time); the first spike of a step counts
   math.<f>   -> the CUDA single-precision function; abs/min/max/float/int builtins; random.random() ->
              a Philox-based uniform draw keyed by (population, neuron, step, call site, link)
   return     -> leaves the hook (each hook body is wrapped in do { ... } while (0))
@@ -117,7 +117,8 @@ class CudaLowering:
             if isinstance(s.value, ast.Constant) and isinstance(s.value.value, str):
                 return ""  # a docstring
             if self.is_spike(s.value):
-                return pad + "fired = true;\n"
+                when = self.expr(s.value.args[0]) if s.value.args else "t"
+                return pad + f"if (!fired) {{ fired = true; spike_t = (float)({when}); }}\n"
             self.fail(s, "an expression statement other than n2.spike()")
         if isinstance(s, ast.Return):
             if s.value is not None:

@@ -109,11 +109,17 @@ class JitRuntime:
         depth = [max(2, 1 << int(np.ceil(np.log2(m + 1)))) for m in max_out]
         self.depth = depth
         self.bits = [torch.zeros(d * w, dtype=torch.int32, device=dev) for d, w in zip(depth, words)]
+        # each spike's time within its step (event-driven intake reads it; the clocked one ignores it)
+        self.offs = [torch.zeros(d * max(1, len(p.shape)), dtype=torch.float32, device=dev)
+                     for d, p in zip(depth, pops)]
+        self.exact = bool(getattr(net, "exact", False))
         self.err = torch.zeros(len(pops), dtype=torch.int32, device=dev)
         self.counters_t = torch.zeros(len(pops), 2, dtype=torch.int64, device=dev)
         self.record_rows = int(net.record_steps)
         self.rec_step0 = net.step_count
         self.rasters = [torch.zeros(max(1, self.record_rows) * w, dtype=torch.int32, device=dev) for w in words]
+        self.raster_offs = [torch.zeros(max(1, self.record_rows) * max(1, len(p.shape)), dtype=torch.float32,
+                                        device=dev) for p in pops]
         self.kernels, self.params, self.sources = [], [], []
         self.edge_arrays = {}  # (connection id, edge name) -> (per-link values in pull order, pull permutation)
         for k, p in enumerate(pops):
@@ -141,7 +147,8 @@ class JitRuntime:
                 incoming.append(inc)
             hooks = {"update": (node.update.ast, hook_context(p, node.update, site_base=site)),
                      "send": (node.send.ast, hook_context(p, node.send, site_base=site + 32))}
-            src, fields = build_source(type(p.instance).__name__, dict(p.dynamic_attrs), hooks, incoming)
+            src, fields = build_source(type(p.instance).__name__, dict(p.dynamic_attrs), hooks, incoming,
+                                       exact=self.exact)
             self.sources.append(src)
             self.kernels.append(compile_source(src, dindex))
             P = params_type(fields)()
@@ -157,6 +164,7 @@ class JitRuntime:
                 p._state[a] = t
                 setattr(P, f"s_{a}", t.data_ptr())
             P.bits, P.raster = self.bits[k].data_ptr(), self.rasters[k].data_ptr()
+            P.off, P.raster_off = self.offs[k].data_ptr(), self.raster_offs[k].data_ptr()
             P.raster_steps, P.rec0 = self.record_rows, self.rec_step0
             P.err = self.err[k:].data_ptr()
             P.counters = self.counters_t[k].data_ptr()
@@ -171,6 +179,8 @@ class JitRuntime:
                 setattr(P, f"c{ci}_src_bits", self.bits[s].data_ptr())
                 setattr(P, f"c{ci}_src_words", words[s])
                 setattr(P, f"c{ci}_src_mask", depth[s] - 1)
+                setattr(P, f"c{ci}_src_off", self.offs[s].data_ptr())
+                setattr(P, f"c{ci}_src_n", len(pops[s].shape))
                 plan = inc["plan"]
                 for e in plan.per_link:
                     v = plan.initial(c, e, len(topo))
@@ -196,7 +206,7 @@ class JitRuntime:
         for k in range(int(n_steps)):
             n = step + k
             for kern, P, p in zip(self.kernels, self.params, self.pops):
-                P.step, P.t = n, (n + 1) * self.dt
+                P.step, P.t, P.t0 = n, (n + 1) * self.dt, n * self.dt
                 grid = (len(p.shape) + BLOCK - 1) // BLOCK
                 if grid:
                     _lib.check(lib.n2b_jit_launch(kern, grid, BLOCK, ctypes.byref(P), ctypes.sizeof(P), self._s),
@@ -243,6 +253,18 @@ class JitRuntime:
         if perm.numel():
             out[perm.to(v.device)] = v[: perm.numel()]
         return out[: perm.numel()]
+
+    def spike_times(self, pop) -> tuple:
+        """(times ms float32, neuron ids) of the recorded spikes: each spike's step start plus its time within
+        the step (the end of the step for a spike of the clocked send; its own time in the event-driven intake)."""
+        raster = self.raster(pop)
+        steps, ids = np.nonzero(raster)
+        k = self.pops.index(pop)
+        n = len(pop.shape)
+        offs = self.raster_offs[k][: len(raster) * n].cpu().numpy()
+        o = offs[steps * n + ids]
+        t0 = ((steps + self.rec_step0) * self.dt).astype(np.float32)
+        return (t0 + o).astype(np.float32), ids.astype(np.int64)
 
     def status(self) -> list:
         self.stream.synchronize()

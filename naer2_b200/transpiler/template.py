@@ -55,27 +55,54 @@ def ctype_of(py) -> tuple[str, object, object]:
     return "float", ctypes.c_float, torch.float32
 
 
-def build_source(pop_name: str, attrs: dict, hooks: dict, incoming: list) -> tuple[str, list]:
+MAX_ARRIVALS = 64  # exact-time intake: arrivals a neuron can hold in one step (more are counted, dropped)
+
+
+def _arrival_body(pop_name: str, c: int, inc: dict) -> str:
+    """One arrival of connection c: the link's edge values, edge forward, receive, edge values stored."""
+    body = ""
+    if inc.get("forward") is not None:
+        fn, ctx = inc["forward"]
+        body += lower_hook(fn, ctx, f"{pop_name} edge forward (connection {c})")
+    body += "".join(f"const float e_{h} = e_{real};\n" for h, real in inc.get("alias", {}).items())
+    if inc["receive"] is not None:
+        fn, ctx = inc["receive"]
+        body += lower_hook(fn, ctx, f"{pop_name} receive (connection {c})")
+    body += "".join(f"p.c{c}_e_{e}[l] = e_{e};\n" for e in inc.get("edge_written", ()))
+    return body
+
+
+def build_source(pop_name: str, attrs: dict, hooks: dict, incoming: list, exact: bool = False) -> tuple[str, list]:
     """(CUDA source, params fields [(name, C type, ctypes type)]) of one population.
 
     attrs: dynamic attr -> python type; hooks: {"update": (fn_ast, ctx), "send": (fn_ast, ctx)};
     incoming: one dict per incoming connection: "receive": (fn_ast, ctx) or None; "edge_dynamic": the per-link
     arrays by the edge's own attribute names; "edge_written": those the edge hooks assign (stored back);
     "alias": {receive-facing name: edge name} where they differ; "forward" / "backward": (fn_ast, ctx) of the
-    edge hooks or None."""
+    edge hooks or None.
+
+    exact: event-driven intake at exact times. Every spike carries its time (its offset in its step, in the
+    population's offset ring); a link of delay d delivers it at that time plus d steps. A neuron collects its
+    arrivals of the step, sorts them by time (stable: connection order, then link order, among equal times),
+    runs receive (and edge forward) for each at its own time and send after each group of equal times; then
+    update and send at the end of the step, as in the clocked intake."""
     fields = [("step", "long long", ctypes.c_int64), ("rec0", "long long", ctypes.c_int64),
               ("raster_steps", "long long", ctypes.c_int64), ("t", "float", ctypes.c_float),
+              ("t0", "float", ctypes.c_float),
               ("n", "int", ctypes.c_int32), ("words", "int", ctypes.c_int32), ("bit_mask", "int", ctypes.c_int32),
               ("seed_lo", "u32", ctypes.c_uint32), ("seed_hi", "u32", ctypes.c_uint32)]
     for a, py in attrs.items():
         ct, cty, _ = ctype_of(py)
         fields.append((f"s_{a}", f"{ct} *", ctypes.c_void_p))
-    fields += [("bits", "u32 *", ctypes.c_void_p), ("raster", "u32 *", ctypes.c_void_p),
-               ("err", "int *", ctypes.c_void_p), ("counters", "u64 *", ctypes.c_void_p)]
+    fields += [("bits", "u32 *", ctypes.c_void_p), ("off", "float *", ctypes.c_void_p),
+               ("raster", "u32 *", ctypes.c_void_p), ("raster_off", "float *", ctypes.c_void_p),
+               ("err", "int *", ctypes.c_void_p),
+               ("counters", "u64 *", ctypes.c_void_p)]
     for c, inc in enumerate(incoming):
         fields += [(f"c{c}_ptr", "const int *", ctypes.c_void_p), (f"c{c}_link", "const u32 *", ctypes.c_void_p),
-                   (f"c{c}_src_bits", "const u32 *", ctypes.c_void_p),
-                   (f"c{c}_src_words", "int", ctypes.c_int32), (f"c{c}_src_mask", "int", ctypes.c_int32)]
+                   (f"c{c}_src_bits", "const u32 *", ctypes.c_void_p), (f"c{c}_src_off", "const float *", ctypes.c_void_p),
+                   (f"c{c}_src_words", "int", ctypes.c_int32), (f"c{c}_src_mask", "int", ctypes.c_int32),
+                   (f"c{c}_src_n", "int", ctypes.c_int32)]
         for e in inc["edge_dynamic"]:
             fields.append((f"c{c}_e_{e}", "float *" if e in inc.get("edge_written", ()) else "const float *",
                            ctypes.c_void_p))
@@ -95,12 +122,16 @@ __device__ __forceinline__ float n2_uniform(const Params &p, int j, long long n,
                "const __grid_constant__ Params p) {\n")
     src.append("    const int j = blockIdx.x * blockDim.x + threadIdx.x;\n")
     src.append("    const bool live = j < p.n;\n    const long long n = p.step;\n    const float t = p.t;\n")
-    src.append("    bool fired = false;\n    u32 arrived = 0;\n    u32 link_k = 0xFFFFFFu;\n")
+    src.append("    bool fired = false;\n    float spike_t = t;\n    u32 arrived = 0;\n    u32 link_k = 0xFFFFFFu;\n")
     for a, py in attrs.items():
         ct, _, _ = ctype_of(py)
         src.append(f"    {ct} s_{a} = live ? p.s_{a}[j] : ({ct})0;\n")
     src.append("    if (live) {\n")
+    if exact:
+        src.append(_exact_intake(pop_name, incoming, hooks))
     for c, inc in enumerate(incoming):
+        if exact:
+            break
         if inc["receive"] is None and inc.get("forward") is None:
             continue
         body = ""
@@ -132,8 +163,8 @@ __device__ __forceinline__ float n2_uniform(const Params &p, int j, long long n,
         body = lower_hook(fn, ctx, f"{pop_name} {name}")
         src.append("        " + body.replace("\n", "\n        ").rstrip() + "\n")
     backward = [(c, inc) for c, inc in enumerate(incoming) if inc.get("backward") is not None]
-    if backward:  # the neuron fired: every incoming link's edge backward hook, connection by connection
-        src.append("        if (fired) {\n")
+    if backward:  # the neuron fired: every incoming link's edge backward hook at its spike's time
+        src.append("        if (fired) {\n            const float t = spike_t;\n")
         for c, inc in backward:
             fn, ctx = inc["backward"]
             body = lower_hook(fn, ctx, f"{pop_name} edge backward (connection {c})")
@@ -144,6 +175,13 @@ __device__ __forceinline__ float n2_uniform(const Params &p, int j, long long n,
             src.append("            }\n")
         src.append("        }\n")
     src.append("    }\n")
+    src.append("""    if (live && fired) {
+        const float o = spike_t - p.t0;  // the spike's time within its step
+        p.off[(size_t)(n & p.bit_mask) * p.n + j] = o;
+        const long long r = n - p.rec0;
+        if (p.raster_off && r >= 0 && r < p.raster_steps) p.raster_off[(size_t)r * p.n + j] = o;
+    }
+""")
     src.append(r'''    const u32 b = __ballot_sync(0xffffffffu, live && fired);
     const u32 arrivals = __reduce_add_sync(0xffffffffu, arrived);
     if ((threadIdx.x & 31) == 0) {
@@ -161,6 +199,63 @@ __device__ __forceinline__ float n2_uniform(const Params &p, int j, long long n,
         src.append(f"    if (live) p.s_{a}[j] = s_{a};\n")
     src.append("}\n")
     return "".join(src), fields
+
+
+def _exact_intake(pop_name: str, incoming: list, hooks: dict) -> str:
+    """The event-driven intake: collect the step's arrivals with their times, sort, deliver in time order."""
+    out = [f"""        float a_t[{MAX_ARRIVALS}];
+        int a_c[{MAX_ARRIVALS}], a_l[{MAX_ARRIVALS}];
+        int na = 0;
+"""]
+    for c, inc in enumerate(incoming):
+        if inc["receive"] is None and inc.get("forward") is None:
+            continue
+        out.append(f"""        for (int l = p.c{c}_ptr[j]; l < p.c{c}_ptr[j + 1]; ++l) {{
+            const u32 w = p.c{c}_link[l];
+            const int src = (int)(w & 0xFFFFFFu), d = (int)(w >> 24);
+            if (d < 1 || d > p.c{c}_src_mask) {{ atomicAdd(p.err, 1); continue; }}
+            const long long m = n - d;
+            if (m < 0) continue;
+            const size_t slot = (size_t)(m & p.c{c}_src_mask);
+            if (!((p.c{c}_src_bits[slot * p.c{c}_src_words + (src >> 5)] >> (src & 31)) & 1u)) continue;
+            const float tau = p.t0 + p.c{c}_src_off[slot * p.c{c}_src_n + src];
+            if (na == {MAX_ARRIVALS}) {{ atomicAdd(p.err, 1); continue; }}
+            int k = na++;
+            while (k > 0 && a_t[k - 1] > tau) {{ a_t[k] = a_t[k - 1]; a_c[k] = a_c[k - 1]; a_l[k] = a_l[k - 1]; --k; }}
+            a_t[k] = tau; a_c[k] = {c}; a_l[k] = l;
+        }}
+""")
+    out.append("""        for (int i = 0; i < na;) {
+            const float tau = a_t[i];
+            int e = i;
+            while (e < na && a_t[e] == tau) ++e;
+            for (int k = i; k < e; ++k) {
+                const int l = a_l[k];
+                const float t = tau;
+                link_k = arrived++;
+                switch (a_c[k]) {
+""")
+    for c, inc in enumerate(incoming):
+        if inc["receive"] is None and inc.get("forward") is None:
+            continue
+        loads = "".join(f"float e_{x} = p.c{c}_e_{x}[l];\n" for x in inc["edge_dynamic"])
+        body = loads + _arrival_body(pop_name, c, inc)
+        out.append(f"                case {c}: {{\n                    " +
+                   body.replace("\n", "\n                    ").rstrip() + "\n                } break;\n")
+    fn, ctx = hooks["send"]
+    send = lower_hook(fn, ctx, f"{pop_name} send")
+    out.append("""                default: break;
+                }
+            }
+            {
+                const float t = tau;
+                """ + send.replace("\n", "\n                ").rstrip() + """
+            }
+            i = e;
+        }
+        link_k = 0xFFFFFFu;
+""")
+    return "".join(out)
 
 
 def params_type(fields: list):

@@ -118,11 +118,16 @@ def run(net, n_steps: int):
         incoming[t].append((index[id(c._source)], ptr.cpu().numpy(), w & 0xFFFFFF, w >> 24, hook,
                             _Link(values, plan.recv), plan, _Link(values, None, writable=True)))
     spikes = [np.zeros((n_steps, len(p.shape)), dtype=bool) for p in pops]
+    offsets = [np.zeros((n_steps, len(p.shape)), dtype=np.float32) for p in pops]  # time within the step
+    exact = bool(getattr(net, "exact", False))
 
-    state = {"fired": False, "j": 0, "n": 0, "k": 0xFFFFFF, "site": 0, "seed": (0, 0)}
+    state = {"fired": False, "j": 0, "n": 0, "k": 0xFFFFFF, "site": 0, "seed": (0, 0), "t": np.float32(0),
+             "spike_t": np.float32(0)}
 
     def spike(time=None):
-        state["fired"] = True
+        if not state["fired"]:
+            state["fired"] = True
+            state["spike_t"] = np.float32(time) if time is not None else state["t"]
 
     def uniform():
         c3 = ((state["site"] & 0xFF) << 24) | (state["k"] & 0xFFFFFF)
@@ -143,6 +148,7 @@ def run(net, n_steps: int):
             elif ty is receives.destination:
                 kw[nm] = dst
         state["site"] = site_base
+        state["t"] = t
         hook.function(obj, **kw)
 
     saved = (n2.spike, _random.random)
@@ -150,6 +156,7 @@ def run(net, n_steps: int):
     try:
         for n in range(n_steps):
             t = np.float32((n + 1) * dt)
+            t0 = np.float32(n * dt)
             state["n"] = n
             for k, p in enumerate(pops):
                 obj = selves[k]
@@ -159,29 +166,41 @@ def run(net, n_steps: int):
                 for j in range(len(p.shape)):
                     object.__setattr__(obj, "_j", j)
                     state["j"], state["fired"], arrived = j, False, 0
+                    state["spike_t"] = t
+                    arrivals = []  # (time, connection, link) in collection order
                     for ci, (s, ptr, src, d, hook, edge, plan, link) in enumerate(incoming[k]):
                         for l in range(ptr[j], ptr[j + 1]):
                             m = n - int(d[l])
                             if m < 0 or not spikes[s][m, src[l]]:
                                 continue
-                            object.__setattr__(edge, "_l", l)
-                            object.__setattr__(link, "_l", l)
-                            state["k"] = arrived
-                            arrived += 1
-                            if plan.forward is not None:
-                                call(plan.forward, link, t, dst=obj)
-                            call(hook, obj, t, edge, site_base=32 * ci)
+                            tau = np.float32(t0 + offsets[s][m, src[l]]) if exact else t
+                            arrivals.append((tau, ci, l))
+                    if exact:
+                        arrivals.sort(key=lambda a: a[0])  # stable: equal times keep collection order
+                    for idx, (tau, ci, l) in enumerate(arrivals):
+                        s, ptr, src, d, hook, edge, plan, link = incoming[k][ci]
+                        object.__setattr__(edge, "_l", l)
+                        object.__setattr__(link, "_l", l)
+                        state["k"] = arrived
+                        arrived += 1
+                        if plan.forward is not None:
+                            call(plan.forward, link, tau, dst=obj)
+                        call(hook, obj, tau, edge, site_base=32 * ci)
+                        if exact and (idx + 1 == len(arrivals) or arrivals[idx + 1][0] != tau):
+                            state["k"] = 0xFFFFFF  # send after each group of equal times
+                            call(node.send, obj, tau, site_base=32 * n_recv + 32)
                     state["k"] = 0xFFFFFF
                     call(node.update, obj, t, site_base=32 * n_recv)
                     call(node.send, obj, t, site_base=32 * n_recv + 32)
                     spikes[k][n, j] = state["fired"]
-                    if state["fired"]:  # every incoming link's edge backward hook
-                        for (s, ptr, src, d, hook, edge, plan, link) in incoming[k]:
+                    if state["fired"]:
+                        offsets[k][n, j] = np.float32(state["spike_t"] - t0)
+                        for (s, ptr, src, d, hook, edge, plan, link) in incoming[k]:  # edge backward hooks
                             if plan.backward is None:
                                 continue
                             for l in range(ptr[j], ptr[j + 1]):
                                 object.__setattr__(link, "_l", l)
-                                call(plan.backward, link, t, dst=obj)
+                                call(plan.backward, link, state["spike_t"], dst=obj)
     finally:
         n2.spike, _random.random = saved
     edges = {}
@@ -189,4 +208,6 @@ def run(net, n_steps: int):
         out = np.empty_like(v)
         out[perm] = v
         edges[(ci, name)] = out
+    if exact:
+        return spikes, arrays, edges, offsets
     return spikes, arrays, edges

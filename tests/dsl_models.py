@@ -171,3 +171,25 @@ class PairSTDP:
     def backward(self, time: n2.time, dst: r.destination):
         x = self.x_pre * math.exp((self.t_last - time) / self.tau_pre)
         self.weight = min(self.weight + self.a_plus * x, self.w_max)
+
+
+@n2.node
+class JitterPacemaker:
+    """Fires every `period` steps at its own time inside the step: `jitter` ms (its own state) before the step's
+    end."""
+
+    def __init__(self, period: int = 4):
+        self.period = period
+        self.phase: int = 0
+        self.jitter: float = 0.0
+
+    def update(self, time: n2.time):
+        self.phase = self.phase + 1
+        self.jitter = self.jitter * 0.9 + 0.005  # per neuron, drifting inside (0, 0.1)
+
+    def send(self, time: n2.time):
+        if self.phase % self.period == 0:
+            n2.spike(time - self.jitter)
+
+    def receive(self, time: n2.time, edge: r.edge, source: r.source):
+        pass

@@ -117,3 +117,40 @@ def test_pair_stdp_edge_hooks_change_the_weights_as_the_interpreter_does(cuda):
         np.testing.assert_allclose(got, edges[(0, name)], rtol=1e-5, atol=1e-6, err_msg=name)
     moved = np.abs(net.runtime.edge_state(c, "weight").cpu().numpy() - w0)
     assert (moved > 1e-3).mean() > 0.5  # learning happened on most links
+
+
+def test_event_driven_exact_times(cuda):
+    """net.exact: spikes carry their times within the step; arrivals are delivered in time order, each at its
+    own time, with send after each group of equal times (DecayLIF decays exactly between them)."""
+    from tests.dsl_models import JitterPacemaker
+
+    g = torch.Generator().manual_seed(11)
+    src = JitterPacemaker(period=4) * 60
+    tgt = DecayLIF(theta=0.5, tau=3.0, t_ref=0.25) * 50
+    c1 = src >> Syn() @ fixed_indegree(6, seed=12) >> tgt
+    c1.weight = 0.1 + 0.3 * torch.rand(c1.shape, generator=g)
+    c1.delay = (torch.randint(1, 5, c1.shape, generator=g) * 0.1).double()
+    c2 = tgt >> Syn() @ fixed_indegree(3, seed=13) >> tgt
+    c2.weight = 0.15 * torch.rand(c2.shape, generator=g)
+    c2.delay = 0.2
+    src.phase = torch.randint(0, 4, (60,), generator=g, dtype=torch.int32)
+    src.jitter = (0.1 * torch.rand(60, generator=g)).float()
+    net = src.network
+    net.resolution = 0.1
+    net.exact = True
+    rasters, state, _, offsets = dsl_interpreter.run(net, 150)
+    net.record(150)
+    net.run_steps(150)
+    net.check()
+    rt = net.runtime
+    for k, p in enumerate(net.populations):
+        assert np.array_equal(rt.raster(p), rasters[k]), k
+        times, ids = rt.spike_times(p)
+        steps, ids_o = np.nonzero(rasters[k])
+        want = (steps * 0.1).astype(np.float32) + offsets[k][steps, ids_o]
+        np.testing.assert_allclose(times, want, rtol=1e-6, atol=1e-6)
+    v = net.populations[1].state_tensor("v").cpu().numpy()
+    np.testing.assert_allclose(v, state[1]["v"], rtol=1e-5, atol=1e-6)
+    assert rasters[1].sum() > 30
+    frac = offsets[1][np.nonzero(rasters[1])]
+    assert (np.abs(frac - 0.1) > 1e-4).mean() > 0.5  # most target spikes off the step grid

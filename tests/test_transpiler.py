@@ -75,11 +75,15 @@ def test_generated_sources_compile_for_sm100a(tmp_path):
             stat = {"gain": 1.5} if "gain" in ast.unparse(hook.ast) else {}
             incoming.append({"receive": (hook.ast, hook_context(p, hook, dyn, stat, site_base=32 * len(incoming))),
                              "edge_dynamic": dyn})
-        src, fields = _source_of(p, incoming)
-        f = tmp_path / f"k{k}.cu"
-        f.write_text(src)
-        subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-c", str(f), "-o",
-                        str(tmp_path / f"k{k}.o")], check=True, capture_output=True)
+        for exact in (False, True):
+            node = p.node
+            hooks = {"update": (node.update.ast, hook_context(p, node.update)),
+                     "send": (node.send.ast, hook_context(p, node.send))}
+            src, fields = build_source(type(p.instance).__name__, dict(p.dynamic_attrs), hooks, incoming, exact)
+            f = tmp_path / f"k{k}{int(exact)}.cu"
+            f.write_text(src)
+            subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-c", str(f), "-o",
+                            str(tmp_path / f"k{k}{int(exact)}.o")], check=True, capture_output=True)
 
 
 def test_interpreter_runs_a_small_network():
