@@ -702,8 +702,13 @@ __device__ __forceinline__ void far_pair(const StepArgs &a, const SConn *s_conn,
     if (h1) deliver_rec(a, C1, rec1, w1, m, 2);
 }
 
-// 5. the far links of step n - 1: items of NPB links, one link per thread, two items at a time, in a static
-// share per block (the next pair's items loaded under this pair's links)
+// 5. the far links of step n - 1: items of NPB links, one link per thread, two items at a time. With every
+// block holding tiles (no tile-free blocks), the first ~80% of the list is split statically (the next pair's
+// items loaded under this pair's links) and, for long lists, the rest is taken in chunks of FAR_CHUNK pairs by whichever
+// blocks get there first (one claim per chunk on the step's counter), so that blocks whose tiles ran late
+// take less of it. With tile-free blocks, those split the whole list statically.
+constexpr int FAR_CHUNK = 4;
+
 template <int NPB, bool INL>
 __device__ __forceinline__ void far_phase(const StepArgs &a, const long long n, const SConn *s_conn) {
     const long long m = n - 1;
@@ -721,14 +726,39 @@ __device__ __forceinline__ void far_phase(const StepArgs &a, const long long n, 
     int4 pre0 = i < a.item_cap ? __ldcg(list + i) : make_int4(0, 0, 0, 0);
     int4 pre1 = i + G < a.item_cap ? __ldcg(list + i + G) : make_int4(0, 0, 0, 0);
     const int count = min(__ldcg(a.item_count + lst), a.item_cap);  // final: appended before the last barrier
-    for (; i < count; i += 2 * G) {
+    // the static part: whole rounds of 2G items covering ~80% of the list; all of it for tile-free blocks and
+    // for lists under 16 items per block, where the chunk claims would cost more than the imbalance
+    const int stat = (split || count < 16 * G) ? count : (count * 4 / 5) / (2 * G) * (2 * G);
+    for (; i < stat; i += 2 * G) {
         const int4 it0 = pre0, it1 = pre1;
-        const bool two = i + G < count;
-        if (i + 2 * G < count) {
+        const bool two = i + G < stat;
+        if (i + 2 * G < stat) {
             pre0 = __ldcg(list + i + 2 * G);
-            pre1 = i + 3 * G < count ? __ldcg(list + i + 3 * G) : make_int4(0, 0, 0, 0);
+            pre1 = i + 3 * G < stat ? __ldcg(list + i + 3 * G) : make_int4(0, 0, 0, 0);
         }
         far_pair<INL>(a, s_conn, it0, it1, two, m);
+    }
+    if (stat >= count) return;  // the same for every thread of the block
+    __shared__ int s_chunk;
+    int *claim = a.tile_claim + 3 + (int)(((m % 3) + 3) % 3);  // the step's chunk counter, next to the tiles'
+    for (;;) {
+        if (threadIdx.x == 0) s_chunk = atomicAdd(claim, 1);
+        __syncthreads();
+        const int c0 = stat + s_chunk * (2 * FAR_CHUNK);
+        __syncthreads();  // every thread has read s_chunk before the next claim overwrites it
+        if (c0 >= count) break;
+        const int c1 = min(count, c0 + 2 * FAR_CHUNK);
+        int4 p0 = __ldcg(list + c0);
+        int4 p1 = c0 + 1 < c1 ? __ldcg(list + c0 + 1) : make_int4(0, 0, 0, 0);
+        for (int b = c0; b < c1; b += 2) {
+            const int4 it0 = p0, it1 = p1;
+            const bool two = b + 1 < c1;
+            if (b + 2 < c1) {
+                p0 = __ldcg(list + b + 2);
+                p1 = b + 3 < c1 ? __ldcg(list + b + 3) : make_int4(0, 0, 0, 0);
+            }
+            far_pair<INL>(a, s_conn, it0, it1, two, m);
+        }
     }
 }
 
@@ -737,9 +767,10 @@ __device__ __forceinline__ void step_body(const StepArgs &a, const long long n, 
                                           const int *s_cache, const SConn *s_conn) {
     __shared__ Scratch<NPB> sc;
     N2B_STAMP(a, k, 0);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {  // step n + 1's list and tile counter
+    if (blockIdx.x == 0 && threadIdx.x == 0) {  // step n + 1's list and tile counter, list n's chunk counter
         atomicExch(a.item_count + (int)((n + 1) % 3), 0);
         atomicExch(a.tile_claim + (int)((n + 1) % 3), 0);
+        atomicExch(a.tile_claim + 3 + (int)((n + 1) % 3), 0);
     }
     // tile blockIdx.x first (a persistent launch holds it in registers); with fewer blocks than tiles, the
     // tiles past the first gridDim.x are claimed one at a time from the step's counter, so that blocks whose
@@ -867,7 +898,7 @@ __global__ void zero_kernel(int32_t *err, int n_err, unsigned long long *counter
 }
 __global__ void set_step_kernel(long long *step, long long value, int32_t *item_count) {
     *step = value;
-    for (int k = 0; k < 6; ++k) item_count[k] = 0;  // the three list lengths and the three tile counters
+    for (int k = 0; k < 9; ++k) item_count[k] = 0;  // list lengths, tile counters, far-chunk counters
 }
 
 }  // namespace n2b

@@ -81,7 +81,7 @@ Layout layout(const n2b_population *pops, int32_t n_pops, const n2b_connection *
     L.rec0 = o; o = align256(o + sizeof(long long));
     L.err = o; o = align256(o + sizeof(int32_t) * N2B_ERR_WORDS);
     L.counters = o; o = align256(o + sizeof(unsigned long long) * (2 + std::max(n_pops, 1)));
-    L.item_count = o; o = align256(o + sizeof(int32_t) * 6);  // three list lengths, three tile counters
+    L.item_count = o; o = align256(o + sizeof(int32_t) * 9);  // list lengths, tile and far-chunk counters
     L.items = o; o = align256(o + sizeof(int4) * 3 * (size_t)L.item_cap);
     L.barrier = o; o = align256(o + sizeof(unsigned) * n2b::BAR_WORDS);
     L.total = o;
