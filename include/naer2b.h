@@ -193,11 +193,13 @@ int n2b_destroy(n2b_net *net);
  * the transposed (outgoing) rows. */
 
 /* error words: 0 links with a bad code (skipped); 1 recomputed spikes that
- * differ from the forward's; 2 in_cta_max / out_cta_max below the rows' counts */
+ * differ from the forward's; 2 in_cta_max / out_cta_max below the rows' counts;
+ * 3 waits of the backward's per-step exchange that gave up (the results are
+ * then wrong; the kernel still ends) */
 #define N2B_BPTT_ERR_WORDS 4
 
 typedef struct n2b_bptt_desc {
-    int32_t batch;       /* B, a multiple of 8 (8 samples per cluster of 8 CTAs) */
+    int32_t batch;       /* B, a multiple of 8 (8 samples per group of 8 CTAs) */
     int32_t steps;       /* T */
     int32_t hidden;      /* H, a multiple of 32, at most 1024 */
     int32_t readouts;    /* R, at most 32 */
@@ -215,7 +217,7 @@ typedef struct n2b_bptt_desc {
 } n2b_bptt_desc;
 
 /* Device workspace bytes of the layer (spike tape, checkpoints, one segment's
- * surrogate derivatives, per-cluster gradient partials). */
+ * surrogate derivatives, per-group gradient partials). */
 int n2b_bptt_workspace_bytes(const n2b_bptt_desc *d, size_t *bytes);
 
 /* Forward over all steps: u [T][B][H] input current, w_rec [nnz] (incoming
@@ -235,7 +237,7 @@ int n2b_bptt_backward(const n2b_bptt_desc *d, const float *u, const float *w_rec
 int n2b_bptt_status(const n2b_bptt_desc *d, void *workspace, size_t workspace_bytes, int32_t *words, void *stream);
 
 /* Copy the taped spikes into out (device): [T][B/8][H] bytes, bit j = sample
- * 8c + j of cluster c; smooth: [T][B/8][H][8] floats. */
+ * 8c + j of group c; smooth: [T][B/8][H][8] floats. */
 int n2b_bptt_spikes(const n2b_bptt_desc *d, void *workspace, size_t workspace_bytes, void *out, void *stream);
 
 /* ---- Run-time compiled step kernels of user-defined models ---------------

@@ -14,16 +14,19 @@
 //                                           + sum_r w_out[i][r] o[t][r] - theta alpha q[t+1][i])
 //   dU[t][i] = q[t][i];  dw_k = sum_t,b s[t - d_k][pre_k] q[t][post_k];  dw_out[i][r] = sum_t,b s[t][i] o[t][r]
 //
-// Layout: a cluster of 8 CTAs runs 8 samples; CTA `rank` owns hidden neurons [rank*HC, rank*HC + HC), HC = H/8,
-// four threads per neuron (two samples each; the link loops split a row among the four, interleaved).
+// Layout: a group of 8 CTAs runs 8 samples; CTA `rank` owns hidden neurons [rank*HC, rank*HC + HC), HC = H/8,
+// four threads per neuron (two samples each; the link loops split a row among the four, interleaved). The
+// forward's group is a thread-block cluster; the adjoint's is a plain group of one cooperative launch (one
+// CTA per SM: at that size only 15 clusters of 8 are resident on 148 SMs, but every group must be).
 // Forward: every CTA keeps the spikes of the last 6 steps of all H neurons for its 8 samples (one byte of 8
 // sample bits per neuron, or 8 floats in the smooth model) in shared memory; each step a neuron's new entry
 // is written into all 8 CTAs' rings (distributed shared memory) before one cluster barrier. Backward: each
 // K-step segment is first recomputed from its membrane checkpoint and the stored spikes of every step by two
 // grid-wide kernels (the recurrent inputs of all its steps at once, then one membrane scan per neuron and
-// sample; same arithmetic, same order: the same Vpre bit for bit), then run backwards by one cluster launch;
-// q of all neurons is exchanged the same way, and each neuron pushes its outgoing rows' q sums into a 6-slot
-// ring of its own partials, kept in global memory between the segments' launches.
+// sample; same arithmetic, same order: the same Vpre bit for bit), then run backwards by one
+// cooperative launch; q of all neurons is exchanged through a two-slot ring in global memory (L2) with one
+// counted arrival per CTA and step, and each neuron pushes its outgoing rows' q sums into a 6-slot ring of its
+// own partials, kept in global memory between the segments' launches.
 // Every sum has a fixed order (no float atomics), so results are bit-for-bit reproducible.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
@@ -74,6 +77,8 @@ struct Args {
     float *part_st;     // [NC * CL][RING][HC][NS] the adjoint's partial ring between segments
     float *q_st;        // [B][H] q[t0] of the last segment done
     float *o_st;        // [B][R] the readout adjoint at t0
+    float *qx;          // [NC][2][H][8] the adjoint's q exchange ring (slot t & 1)
+    uint32_t *xcnt;     // [NC] the adjoint's arrivals per group (zeroed before each launch)
     int32_t *err;       // [N2B_BPTT_ERR_WORDS]
 };
 
@@ -136,6 +141,27 @@ __host__ __device__ inline BwdSmem bwd_smem(int H, int HC, int R, int out_cta_ma
 // and makes their earlier writes visible (acquire).
 __device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
 __device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
+
+// One CTA's arrival at a group step (thread 0, after a __syncthreads that follows the CTA's writes): a release
+// add on the group's counter, then a bounded acquire spin until `target` arrivals (every CTA of the group at
+// this step). A wait that gives up counts in err[3] and sets `aborted`, after which the CTA still arrives but
+// no longer waits, so that neither it nor the CTAs that wait for its arrivals can hang.
+constexpr int XCHG_SPIN_LIMIT = 1 << 21;  // polls of an L2 round trip each: about a second
+__device__ __forceinline__ void group_arrive_wait(uint32_t *cnt, uint32_t target, int32_t *err, int &aborted) {
+    __threadfence();
+    asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(cnt) : "memory");
+    if (aborted) return;
+    for (int it = 0;; ++it) {
+        uint32_t v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(cnt) : "memory");
+        if (v >= target) return;
+        if (it >= XCHG_SPIN_LIMIT) {
+            atomicAdd(err + 3, 1);
+            aborted = 1;
+            return;
+        }
+    }
+}
 
 // The spikes that the incoming links read: the forward's shared-memory ring (6 slots, the slot of step t in
 // t mod 6; slots of steps before 0 are still zero), or the stored spikes of every step (recompute).
@@ -468,16 +494,16 @@ __device__ __forceinline__ void out_group(const uint16_t *ocode, const float *ow
 
 // The adjoint of segment [t0, t1), run backwards; `first`: the last segment of the sequence (state starts at
 // zero), else the state of the segment after it is loaded (partial ring, q, readout adjoint, dw, dw_out).
-// q[t] of all neurons goes through one shared buffer per CTA (pnew), guarded by two cluster barrier phases
-// per step: after the writes (every q[t] in place before any CTA reads it) and after the reads (no CTA
-// overwrites pnew with q[t - 1] while another still reads q[t]); the second phase's wait comes after the
-// next step's local work, so that it rarely waits.
+// Each step, every CTA writes the q[t] of its neurons into slot t & 1 of the group's ring in global memory,
+// arrives on the group's counter, waits for all 8 arrivals and copies q[t] of all H neurons into its own
+// shared buffer (pnew). Two slots suffice: a CTA writes slot t & 1 only after every CTA of the group arrived
+// at step t + 1, which each does after its copy of slot t & 1 at step t + 2. The launch is cooperative, so
+// the CTAs of a group are resident together; `g0` is the launch's first group.
 template <bool SMOOTH>
 __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a, int out_cta_max, int t0, int t1,
-                                                   int first) {
-    cg::cluster_group cl = cg::this_cluster();
-    const int rank = (int)cl.block_rank();
-    const int q = (int)blockIdx.x / CL;
+                                                   int first, int g0) {
+    const int rank = (int)blockIdx.x % CL;
+    const int q = g0 + (int)blockIdx.x / CL;
     const int H = a.H, HC = a.HC, R = a.R, B = a.B;
     const int h0 = rank * HC;
     const BwdSmem L = bwd_smem(H, HC, R, out_cta_max);
@@ -524,9 +550,11 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
         for (int k = tid; k < on; k += nthr) dw[k] = a.dwp[(size_t)q * a.nnz + obase + k];
         for (int k = tid; k < HC * R; k += nthr) dwo[k] = a.dwo_p[((size_t)q * H + h0) * R + k];
     }
+    __shared__ int aborted;
+    if (tid == 0) aborted = 0;
     __syncthreads();
-    cl.sync();
-    cluster_arrive();  // the "reads done" phase of the step before the first
+    uint32_t *xcnt = a.xcnt + q;
+    uint32_t target = 0;
 
     const size_t bq = (size_t)q * NS + SPT * sub;
     const bool ro = tid < NS * R;
@@ -618,14 +646,16 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
                 }
             }
         }
-        cluster_wait();  // every CTA has read the previous q from its pnew
-        if (nt) {
-            const float2 v = make_float2(qv0, qv1);
-            float2 *dst = reinterpret_cast<float2 *>(pnew) + (size_t)me * (QROW / 2) + sub;
-            for (int k = 0; k < CL; ++k) *cl.map_shared_rank(dst, k) = v;
-        }
-        cluster_arrive();
-        cluster_wait();  // q[t] of every neuron in every CTA's pnew
+        float *slot = a.qx + ((size_t)q * 2 + (t & 1)) * H * NS;
+        if (nt) reinterpret_cast<float2 *>(slot)[(size_t)me * (NS / 2) + sub] = make_float2(qv0, qv1);
+        __syncthreads();  // this CTA's q[t] written
+        target += CL;
+        if (tid == 0) group_arrive_wait(xcnt, target, a.err, aborted);
+        __syncthreads();  // every CTA's q[t] written: copy all of them (past L1) into pnew
+        for (int j = tid; j < H * (NS / 4); j += nthr)
+            reinterpret_cast<float4 *>(pnew)[(size_t)(j >> 1) * (QROW / 4) + (j & 1)] =
+                __ldcg(reinterpret_cast<const float4 *>(slot) + j);
+        __syncthreads();
         // outgoing rows: partial[t - d] += w q[t][post]; dw += s[t - d][me] q[t][post]
         for (int d = 1; d <= MAXD; ++d) {
             float acc[NS];
@@ -647,7 +677,6 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
                 pp[1] = __fadd_rn(pp[1], x1);
             }
         }
-        cluster_arrive();  // this CTA's reads of q[t] are done
         // the spike history of step t - 1: delays 1..5 reach t - 2 .. t - 6
         if constexpr (SMOOTH) {
             for (int d = 1; d <= MAXD; ++d) {
@@ -660,7 +689,6 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
             hist = (hist >> 8) | ((uint64_t)byte << (8 * (MAXD - 1)));
         }
     }
-    cluster_wait();  // the last "reads done" phase
     // the state for the segment before this one
     __syncthreads();
     for (int k = tid; k < RING * HC * NS; k += nthr) part_st[k] = part[k];
@@ -671,7 +699,6 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
         a.q_st[(bq + 1) * H + me] = qp1;
     }
     if (ro && rank == 0) a.o_st[(size_t)(q * NS + rb) * R + rr] = o;
-    cl.sync();
 }
 
 // dw_rec in the caller's (incoming, canonical) order: the clusters' partials added in cluster order.
@@ -719,7 +746,7 @@ int bcuda(cudaError_t e, const char *what) {
     } while (0)
 
 struct WsLayout {
-    size_t spikes, vck, gseg, outw, dwp, dwo, part, qst, ost, err, total;
+    size_t spikes, vck, gseg, outw, dwp, dwo, part, qst, ost, qx, xcnt, err, total;
 };
 
 size_t a256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -755,6 +782,8 @@ WsLayout ws_layout(const n2b_bptt_desc *d) {
     L.part = o; o = a256(o + sizeof(float) * NC * CL * RING * (H / CL) * NS);
     L.qst = o; o = a256(o + sizeof(float) * B * H);
     L.ost = o; o = a256(o + sizeof(float) * B * R);
+    L.qx = o; o = a256(o + sizeof(float) * NC * 2 * H * NS);
+    L.xcnt = o; o = a256(o + sizeof(uint32_t) * NC);
     L.err = o; o = a256(o + sizeof(int32_t) * N2B_BPTT_ERR_WORDS);
     L.total = o;
     return L;
@@ -794,6 +823,8 @@ Args args_of(const n2b_bptt_desc *d, char *ws, const WsLayout &L) {
     a.part_st = reinterpret_cast<float *>(ws + L.part);
     a.q_st = reinterpret_cast<float *>(ws + L.qst);
     a.o_st = reinterpret_cast<float *>(ws + L.ost);
+    a.qx = reinterpret_cast<float *>(ws + L.qx);
+    a.xcnt = reinterpret_cast<uint32_t *>(ws + L.xcnt);
     a.err = reinterpret_cast<int32_t *>(ws + L.err);
     return a;
 }
@@ -826,6 +857,36 @@ int launch_cluster(Kern kern, int grid, int threads, size_t smem, cudaStream_t s
     int clusters = 0;
     B_CUDA(cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg));
     if (clusters < 1) return bfail(N2B_ECUDA, "a cluster of 8 CTAs of this size cannot be resident");
+    B_CUDA(cudaLaunchKernelEx(&cfg, kern, a, rest...));
+    return N2B_OK;
+}
+
+// The groups of 8 CTAs that one cooperative launch of `kern` can hold (all resident at once).
+template <class Kern>
+int coop_groups(Kern kern, int threads, size_t smem, int &groups) {
+    if (smem > 227 * 1024) return bfail(N2B_EINVAL, "shared memory need " + std::to_string(smem) + " bytes > 227 KiB");
+    B_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int dev = 0, sms = 0, per_sm = 0;
+    B_CUDA(cudaGetDevice(&dev));
+    B_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    B_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+    groups = per_sm * sms / CL;
+    if (groups < 1) return bfail(N2B_ECUDA, "a group of 8 CTAs of this size cannot be resident");
+    return N2B_OK;
+}
+
+template <class Kern, class... Rest>
+int launch_coop(Kern kern, int grid, int threads, size_t smem, cudaStream_t s, const Args &a, Rest... rest) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
     B_CUDA(cudaLaunchKernelEx(&cfg, kern, a, rest...));
     return N2B_OK;
 }
@@ -891,8 +952,12 @@ int n2b_bptt_backward(const n2b_bptt_desc *d, const float *u, const float *w_rec
     }
     const bool smooth = d->smooth != 0;
     const BwdSmem S = bwd_smem(d->hidden, d->hidden / CL, d->readouts, d->out_cta_max);
-    const int grid = (d->batch / NS) * CL, threads = threads_of(d);
+    const int NC = d->batch / NS, threads = threads_of(d);
     const int K = d->checkpoint, nseg = a.nseg;
+    int per_launch = 0;  // groups per cooperative launch
+    rc = smooth ? coop_groups(bwd_kernel<true>, threads, S.total, per_launch)
+                : coop_groups(bwd_kernel<false>, threads, S.total, per_launch);
+    if (rc) return rc;
     for (int seg = nseg - 1; seg >= 0; --seg) {  // each segment: recompute from its checkpoint, then backwards
         const int t0 = seg * K, t1 = std::min(d->steps, t0 + K);
         const size_t nr = (size_t)((t1 - t0 + TC - 1) / TC) * (d->batch / NS) * d->hidden * NT;
@@ -906,11 +971,14 @@ int n2b_bptt_backward(const n2b_bptt_desc *d, const float *u, const float *w_rec
         }
         B_CUDA(cudaGetLastError());
         const int first = seg == nseg - 1;
-        rc = smooth ? launch_cluster(bwd_kernel<true>, grid, threads, S.total, s, a, d->out_cta_max, t0, t1, first)
-                    : launch_cluster(bwd_kernel<false>, grid, threads, S.total, s, a, d->out_cta_max, t0, t1, first);
-        if (rc) return rc;
+        B_CUDA(cudaMemsetAsync(a.xcnt, 0, sizeof(uint32_t) * NC, s));
+        for (int g0 = 0; g0 < NC; g0 += per_launch) {
+            const int grid = std::min(per_launch, NC - g0) * CL;
+            rc = smooth ? launch_coop(bwd_kernel<true>, grid, threads, S.total, s, a, d->out_cta_max, t0, t1, first, g0)
+                        : launch_coop(bwd_kernel<false>, grid, threads, S.total, s, a, d->out_cta_max, t0, t1, first, g0);
+            if (rc) return rc;
+        }
     }
-    const int NC = d->batch / NS;
     if (d->nnz > 0) {
         reduce_dw_kernel<<<(d->nnz + 255) / 256, 256, 0, s>>>(a.dwp, d->out_perm, d->nnz, NC, dw_rec);
         B_CUDA(cudaGetLastError());
