@@ -37,9 +37,51 @@ def draw_links(hidden: int, density: float, max_delay: int = MAX_DELAY, seed: in
     return pre.astype(np.int64), post.astype(np.int64), delay.astype(np.int64)
 
 
+def bank_order(post: np.ndarray, grp: np.ndarray) -> np.ndarray:
+    """An order of the outgoing links within each (pre, delay) group for the adjoint's shared-memory gather.
+
+    The adjoint gives each neuron four threads; the thread `sub` of a neuron takes the links 4k + sub of each
+    of its delay groups (k = 0, 1, ...), and one 128-bit load of a quarter warp serves the 8 threads of two
+    neurons 2i, 2i + 1 at the same k. Each thread reads the q row of its link's target, rows 48 bytes apart,
+    so the load touches the 16-byte bank group (3 post + half) mod 8: targets with distinct post mod 8 are
+    served in one pass, equal ones in several. Greedily, each chunk k of the two neurons' groups takes links
+    with distinct residues mod 8, the most frequent remaining residues first. Returns positions into `post`
+    (a permutation within each group); the sums are the same up to their order."""
+    hidden = grp.shape[0]
+    perm = np.arange(len(post))
+    res = post % 8
+    for i in range(0, hidden, 2):
+        for d in range(MAX_DELAY):
+            spans = [(grp[j, d], grp[j, d + 1]) for j in (i, i + 1) if j < hidden]
+            pools = []
+            for s, e in spans:
+                pool = [[] for _ in range(8)]
+                for j in range(s, e):
+                    pool[res[j]].append(j)
+                pools.append(pool)
+            outs = [[] for _ in spans]
+            while any(len(o) < e - s for o, (s, e) in zip(outs, spans)):
+                used = set()
+                for pool, out, (s, e) in zip(pools, outs, spans):
+                    take, got = min(4, e - s - len(out)), 0
+                    for r in sorted(range(8), key=lambda r: -len(pool[r])):
+                        if got == take:
+                            break
+                        if pool[r] and r not in used:
+                            out.append(pool[r].pop())
+                            used.add(r)
+                            got += 1
+                    while got < take:  # no distinct residue left: the fullest one
+                        out.append(pool[max(range(8), key=lambda r: len(pool[r]))].pop())
+                        got += 1
+            for out, (s, e) in zip(outs, spans):
+                perm[s:e] = out
+    return perm
+
+
 class Wiring:
     """The recurrent links as the kernels read them: incoming rows (the weights' order) and outgoing rows
-    sorted by delay, with the permutation between the two."""
+    sorted by delay (each delay group in `bank_order`), with the permutation between the two."""
 
     def __init__(self, pre, post, delay, hidden: int, device):
         pre, post, delay = (np.asarray(a, dtype=np.int64) for a in (pre, post, delay))
@@ -63,6 +105,8 @@ class Wiring:
         row_start = np.concatenate([[0], np.cumsum(counts.sum(1))[:-1]])
         grp[:, 0] = row_start
         grp[:, 1:] = row_start[:, None] + np.cumsum(counts, axis=1)
+        out_order = out_order[bank_order(out_post, grp)]
+        out_post, out_delay = post[out_order], delay[out_order]
         hc = hidden // 8
         self.in_cta_max = int(max((in_ptr[(r + 1) * hc] - in_ptr[r * hc] for r in range(8)), default=0))
         self.out_cta_max = int(max((grp[(r + 1) * hc - 1, -1] - grp[r * hc, 0] for r in range(8)), default=0))

@@ -464,30 +464,51 @@ __global__ void __launch_bounds__(256) recompute_v_kernel(const __grid_constant_
 // ------------------------------------------------------------------------------------------------ adjoint
 
 // One delay group of a neuron's outgoing row at step t: acc[b] += w q[t][post][b] over this thread's share
-// of the links; with DW (the neuron spiked at t - d in some sample), also dw[l] += sum_b s[b] q[t][post][b].
-// Without DW the loop stores nothing, so the loads of later links are not held behind earlier stores.
+// of the links (gs + sub, gs + sub + NT, ...), OUT_U links a round: all loads of a round (codes, weights, q
+// rows, dw) are issued before its arithmetic and stores, so that a round costs one chain of shared-memory
+// latencies. With DW (warp-uniform: some lane's neuron spiked at t - d), the lanes with `dwl` also add
+// sum_b s[b] q[t][post][b] to dw[l]. A skipped code (0xFFFF) reads row 0 and adds nothing.
+constexpr int OUT_U = 4;
 template <bool SMOOTH, bool DW>
 __device__ __forceinline__ void out_group(const uint16_t *ocode, const float *ow, const float *pnew, float *dw,
-                                          int gs, int ge, int sub, uint32_t sbyte, const float *sf, float acc[NS]) {
-#pragma unroll 4
-    for (int l = gs + sub; l < ge; l += NT) {
-        const uint32_t c = ocode[l];
-        if (c == 0xFFFFu) continue;
-        const float wl = ow[l];
-        const size_t post = c & 0x7FFu;  // < H: checked when the rows were copied
-        const float4 y0 = reinterpret_cast<const float4 *>(pnew)[post * (QROW / 4)];
-        const float4 y1 = reinterpret_cast<const float4 *>(pnew)[post * (QROW / 4) + 1];
-        const float x[NS] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
+                                          int gs, int ge, int sub, bool dwl, uint32_t sbyte, const float *sf,
+                                          float acc[NS]) {
+    for (int base = gs + sub; base < ge; base += OUT_U * NT) {
+        uint32_t c[OUT_U];
+        float wl[OUT_U], od[OUT_U];
+        float4 y0[OUT_U], y1[OUT_U];
+        bool ok[OUT_U];
 #pragma unroll
-        for (int b = 0; b < NS; ++b) acc[b] = __fmaf_rn(wl, x[b], acc[b]);
-        if constexpr (DW) {
-            float dk = 0.f;
+        for (int u = 0; u < OUT_U; ++u) {
+            const int l = base + u * NT;
+            c[u] = l < ge ? ocode[l] : 0xFFFFu;
+            wl[u] = l < ge ? ow[l] : 0.f;
+        }
 #pragma unroll
-            for (int b = 0; b < NS; ++b) {
-                if constexpr (SMOOTH) dk = __fmaf_rn(sf[b], x[b], dk);
-                else if ((sbyte >> b) & 1u) dk = __fadd_rn(dk, x[b]);
+        for (int u = 0; u < OUT_U; ++u) {
+            ok[u] = c[u] != 0xFFFFu;
+            const size_t post = ok[u] ? (c[u] & 0x7FFu) : 0u;  // < H: checked when the rows were copied
+            y0[u] = reinterpret_cast<const float4 *>(pnew)[post * (QROW / 4)];
+            y1[u] = reinterpret_cast<const float4 *>(pnew)[post * (QROW / 4) + 1];
+            if constexpr (DW) od[u] = (dwl && ok[u]) ? dw[base + u * NT] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < OUT_U; ++u) {
+            if (!ok[u]) continue;
+            const float x[NS] = {y0[u].x, y0[u].y, y0[u].z, y0[u].w, y1[u].x, y1[u].y, y1[u].z, y1[u].w};
+#pragma unroll
+            for (int b = 0; b < NS; ++b) acc[b] = __fmaf_rn(wl[u], x[b], acc[b]);
+            if constexpr (DW) {
+                if (dwl) {
+                    float dk = 0.f;
+#pragma unroll
+                    for (int b = 0; b < NS; ++b) {
+                        if constexpr (SMOOTH) dk = __fmaf_rn(sf[b], x[b], dk);
+                        else if ((sbyte >> b) & 1u) dk = __fadd_rn(dk, x[b]);
+                    }
+                    dw[base + u * NT] = __fadd_rn(od[u], dk);
+                }
             }
-            dw[l] = __fadd_rn(dw[l], dk);
         }
     }
 }
@@ -663,8 +684,10 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
             for (int b = 0; b < NS; ++b) acc[b] = 0.f;
             const int gs = nt ? grp[pl * (MAXD + 1) + d - 1] : 0, ge = nt ? grp[pl * (MAXD + 1) + d] : 0;
             const uint32_t sbyte = SMOOTH ? 0xffu : (uint32_t)((hist >> (8 * (d - 1))) & 0xffu);
-            if (sbyte) out_group<SMOOTH, true>(ocode, ow, pnew, dw, gs, ge, sub, sbyte, histf[d - 1], acc);
-            else out_group<SMOOTH, false>(ocode, ow, pnew, dw, gs, ge, sub, 0u, histf[d - 1], acc);
+            if (__any_sync(FULL, sbyte != 0u))  // the same branch for the whole warp
+                out_group<SMOOTH, true>(ocode, ow, pnew, dw, gs, ge, sub, sbyte != 0u, sbyte, histf[d - 1], acc);
+            else
+                out_group<SMOOTH, false>(ocode, ow, pnew, dw, gs, ge, sub, false, 0u, histf[d - 1], acc);
 #pragma unroll
             for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __shfl_xor_sync(FULL, acc[b], 1));
 #pragma unroll

@@ -82,6 +82,32 @@ def test_wiring_rows_and_permutation():
         Wiring(pre[::-1].copy(), post[::-1].copy(), delay, H, "cpu")  # not in canonical order
 
 
+def test_bank_order_spreads_the_gather_over_the_banks():
+    """The outgoing order keeps every (pre, delay) group and lowers the passes of the adjoint's quarter-warp
+    loads (8 threads of two neurons at the same chunk k; a pass per repeat of post mod 8)."""
+    H = 1024
+    pre, post, delay = draw_links(H, 0.1, seed=3)
+    w = Wiring(pre, post, delay, H, "cpu")
+    grp = w.out_grp.numpy().reshape(H, MAX_DELAY + 1)
+    oc = w.out_code.numpy().astype(np.int64)
+    sorted_post = post[np.lexsort((post, delay, pre))]
+
+    def passes(targets):
+        n = 0
+        for i in range(0, H, 2):
+            for d in range(MAX_DELAY):
+                a, b = (targets[grp[j, d]:grp[j, d + 1]] % 8 for j in (i, i + 1))
+                for k in range(0, max(len(a), len(b)), 4):
+                    n += np.bincount(np.concatenate([a[k:k + 4], b[k:k + 4]]), minlength=8).max()
+        return n
+
+    for i in range(0, H, 97):
+        for d in range(MAX_DELAY):
+            seg = slice(grp[i, d], grp[i, d + 1])
+            assert np.array_equal(np.sort(oc[seg] & 0x7FF), np.sort(sorted_post[seg]))
+    assert passes(oc & 0x7FF) < 0.8 * passes(sorted_post)
+
+
 def test_task_templates_and_samples():
     rates = bptt_task.templates(classes=5, channels=50, steps=60, seed=2)
     assert rates.shape == (5, 60, 50) and rates.min() >= 0 and rates.max() <= 50
