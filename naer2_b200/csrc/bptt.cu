@@ -376,43 +376,70 @@ __global__ void __launch_bounds__(512) fwd_kernel(const __grid_constant__ Args a
 // applies every link to the TC steps of its chunk, then the NT shares are added as the forward adds them
 // ((s0 + s1) + (s2 + s3), links in the forward's order within each share): the same sums bit for bit.
 // A link with a bad code (counted by the forward) is clamped into range here instead of checked per step.
+// Spiking model: a block is blockDim / NT neurons of one (chunk, cluster); it first stages the spike bytes of
+// the MAXD + TC - 1 steps its links read, of every neuron of the cluster, as one 16-byte row per neuron in
+// shared memory (steps before 0 as zero), so that a link's TC steps are one 128-bit load. Launch: grid
+// (H / (blockDim / NT), NC, chunks).
 constexpr int TC = 5;
+constexpr int RWIN = MAXD + TC - 1;  // steps tc - MAXD .. tc + TC - 2
+static_assert(RWIN <= 16, "a staged row is 16 bytes");
 
 template <bool SMOOTH>
 __global__ void __launch_bounds__(256) recompute_r_kernel(const __grid_constant__ Args a, int t0, int t1) {
-    const int nchunk = (t1 - t0 + TC - 1) / TC;
-    const int per_c = a.NC * a.H * NT;
-    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = gid < nchunk * per_c;  // whole groups of NT lanes live or not together
-    const int g = live ? gid : 0;
-    const int tc = t0 + (g / per_c) * TC;
-    const int rem = g % per_c;
-    const int q = rem / (a.H * NT), post = (rem / NT) % a.H, sub = rem % NT;
-    const int rs = live ? a.in_ptr[post] : 0, re = live ? a.in_ptr[post + 1] : 0;
-    const int row = a.NC * a.H;  // bytes between two steps of the stored spikes
+    extern __shared__ __align__(16) unsigned char rows[];  // spiking: [H][16] bytes
+    const int ppb = blockDim.x / NT;  // neurons per block
+    const int q = blockIdx.y, tc = t0 + blockIdx.z * TC;
+    const int post = blockIdx.x * ppb + threadIdx.x / NT, sub = threadIdx.x % NT;
+    const int rs = a.in_ptr[post], re = a.in_ptr[post + 1];
+    const int kend = min(TC, t1 - tc);  // steps of this chunk inside the segment
     float acc[TC][NS];
 #pragma unroll
     for (int k = 0; k < TC; ++k)
 #pragma unroll
         for (int b = 0; b < NS; ++b) acc[k][b] = 0.f;
-    for (int l = rs + sub; l < re; l += NT) {
-        const uint32_t c = a.in_code[l];
-        const float wl = a.in_w[l];
-        const int pre = min((int)(c & 0x7FFu), a.H - 1), d = min(max((int)(c >> 11), 1), MAXD);
-        const int base = (tc - d) * row + q * a.H + pre;  // step tc - d
+    if constexpr (SMOOTH) {
+        const int row = a.NC * a.H;  // entries between two steps of the stored spikes
+        for (int l = rs + sub; l < re; l += NT) {
+            const uint32_t c = a.in_code[l];
+            const float wl = a.in_w[l];
+            const int pre = min((int)(c & 0x7FFu), a.H - 1), d = min(max((int)(c >> 11), 1), MAXD);
+            const int base = (tc - d) * row + q * a.H + pre;  // step tc - d
 #pragma unroll
-        for (int k = 0; k < TC; ++k) {
-            const int tt = tc + k - d;
-            if (tt < 0 || tc + k >= t1) continue;
-            if constexpr (SMOOTH) {
+            for (int k = 0; k < TC; ++k) {
+                if (tc + k - d < 0 || k >= kend) continue;
                 const float4 *p = reinterpret_cast<const float4 *>(a.s_f) + (size_t)(base + k * row) * 2;
                 const float4 x = p[0], y = p[1];
-                const float s[NS] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
+                const float sv[NS] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
 #pragma unroll
-                for (int b = 0; b < NS; ++b) acc[k][b] = __fadd_rn(acc[k][b], __fmul_rn(wl, s[b]));
-            } else {
-                const uint32_t byte = a.s_bits[base + k * row];
-                if (!byte) continue;
+                for (int b = 0; b < NS; ++b) acc[k][b] = __fadd_rn(acc[k][b], __fmul_rn(wl, sv[b]));
+            }
+        }
+    } else {
+        // stage: thread j packs the RWIN bytes of neurons j, j + blockDim, ... (coalesced byte loads per step)
+        for (int pre = threadIdx.x; pre < a.H; pre += blockDim.x) {
+            uint32_t w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+            for (int sidx = 0; sidx < RWIN; ++sidx) {
+                const int tt = tc - MAXD + sidx;
+                const uint32_t byte = (tt >= 0 && tt < a.T) ? a.s_bits[((size_t)tt * a.NC + q) * a.H + pre] : 0u;
+                w[sidx / 4] |= byte << (8 * (sidx % 4));
+            }
+            reinterpret_cast<uint4 *>(rows)[pre] = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+        __syncthreads();
+        for (int l = rs + sub; l < re; l += NT) {
+            const uint32_t c = a.in_code[l];
+            const float wl = a.in_w[l];
+            const int pre = min((int)(c & 0x7FFu), a.H - 1), d = min(max((int)(c >> 11), 1), MAXD);
+            const uint4 v = reinterpret_cast<const uint4 *>(rows)[pre];
+            const uint64_t lo = ((uint64_t)v.y << 32) | v.x, hi = ((uint64_t)v.w << 32) | v.z;
+            const int sh = 8 * (MAXD - d);  // byte of step tc - d
+            const uint64_t win = sh ? (lo >> sh) | (hi << (64 - sh)) : lo;  // steps tc - d ...
+            if (!(win & ((1ull << (8 * TC)) - 1))) continue;
+#pragma unroll
+            for (int k = 0; k < TC; ++k) {
+                const uint32_t byte = (uint32_t)(win >> (8 * k)) & 0xffu;
+                if (!byte || k >= kend) continue;
 #pragma unroll
                 for (int b = 0; b < NS; ++b)
                     if ((byte >> b) & 1u) acc[k][b] = __fadd_rn(acc[k][b], wl);
@@ -426,11 +453,10 @@ __global__ void __launch_bounds__(256) recompute_r_kernel(const __grid_constant_
 #pragma unroll
         for (int b = 0; b < NS; ++b) acc[k][b] = __fadd_rn(acc[k][b], __shfl_xor_sync(FULL, acc[k][b], 2));
     }
-    if (!live) return;
     const size_t bq = (size_t)q * NS + SPT * sub;
 #pragma unroll
     for (int k = 0; k < TC; ++k) {
-        if (tc + k >= t1) break;
+        if (k >= kend) break;
         float r0, r1;
         mine(acc[k], sub, r0, r1);
         a.g_seg[((size_t)(tc + k - t0) * a.B + bq) * a.H + post] = r0;
@@ -977,19 +1003,21 @@ int n2b_bptt_backward(const n2b_bptt_desc *d, const float *u, const float *w_rec
     const BwdSmem S = bwd_smem(d->hidden, d->hidden / CL, d->readouts, d->out_cta_max);
     const int NC = d->batch / NS, threads = threads_of(d);
     const int K = d->checkpoint, nseg = a.nseg;
+    const int rthreads = d->hidden % 64 == 0 ? 256 : 128;  // whole neurons of NT threads; hidden % 32 == 0
+    const size_t rsmem = smooth ? 0 : (size_t)16 * d->hidden;  // the staged spike rows
     int per_launch = 0;  // groups per cooperative launch
     rc = smooth ? coop_groups(bwd_kernel<true>, threads, S.total, per_launch)
                 : coop_groups(bwd_kernel<false>, threads, S.total, per_launch);
     if (rc) return rc;
     for (int seg = nseg - 1; seg >= 0; --seg) {  // each segment: recompute from its checkpoint, then backwards
         const int t0 = seg * K, t1 = std::min(d->steps, t0 + K);
-        const size_t nr = (size_t)((t1 - t0 + TC - 1) / TC) * (d->batch / NS) * d->hidden * NT;
-        const unsigned rblocks = (unsigned)((nr + 255) / 256), vblocks = (unsigned)((d->batch * d->hidden + 255) / 256);
+        const dim3 rgrid((unsigned)(d->hidden / (rthreads / NT)), (unsigned)NC, (unsigned)((t1 - t0 + TC - 1) / TC));
+        const unsigned vblocks = (unsigned)((d->batch * d->hidden + 255) / 256);
         if (smooth) {
-            recompute_r_kernel<true><<<rblocks, 256, 0, s>>>(a, t0, t1);
+            recompute_r_kernel<true><<<rgrid, rthreads, 0, s>>>(a, t0, t1);
             recompute_v_kernel<true><<<vblocks, 256, 0, s>>>(a, seg, t0, t1);
         } else {
-            recompute_r_kernel<false><<<rblocks, 256, 0, s>>>(a, t0, t1);
+            recompute_r_kernel<false><<<rgrid, rthreads, rsmem, s>>>(a, t0, t1);
             recompute_v_kernel<false><<<vblocks, 256, 0, s>>>(a, seg, t0, t1);
         }
         B_CUDA(cudaGetLastError());
