@@ -402,12 +402,13 @@ def run_bptt(args, dev) -> dict:
     the adjoint kernels and the input projection's gradient), each timed with CUDA events after an L2 flush."""
     import torch
 
+    from naer2_b200.bptt import SpikeEvents
     from naer2_b200.networks import bptt_task
 
     t0 = time.perf_counter()
     layer, x, y = bptt_task.build(seed=1, device=dev)
     T, B, C = x.shape
-    xs = x.reshape(T * B, C).float().to_sparse()  # the input as spike events
+    xs = SpikeEvents.from_dense(x)  # the input as spike event lists, built once like a loader's output
     build_s = time.perf_counter() - t0
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)

@@ -240,6 +240,24 @@ int n2b_bptt_status(const n2b_bptt_desc *d, void *workspace, size_t workspace_by
  * 8c + j of group c; smooth: [T][B/8][H][8] floats. */
 int n2b_bptt_spikes(const n2b_bptt_desc *d, void *workspace, size_t workspace_bytes, void *out, void *stream);
 
+/* The layer's input projection over spike events (no counterpart in the
+ * reference; it replaces a sparse-dense library product). Input row r is
+ * sample b of step t (r = t * B + b); its spiking channels are
+ * channel[row_ptr[r] .. row_ptr[r + 1]), ascending. Writes u [rows][hidden] =
+ * the sum of those channels' rows of w_in [channels][hidden], in channel
+ * order. hidden a multiple of 4 (at most 1024); w_in and u 16-byte aligned. */
+int n2b_project_forward(const int32_t *row_ptr, const int32_t *channel, int32_t rows, int32_t channels,
+                        int32_t hidden, const float *w_in, float *u, void *stream);
+
+/* dw_in [channels][hidden] = x^T du for the same events, grouped by channel:
+ * chunk k is the rows row_idx[chunk_ptr[k] .. chunk_ptr[k + 1]) (ascending,
+ * one channel's), channel c owns chunks channel_chunk[c] .. channel_chunk[c + 1];
+ * partials [n_chunks][hidden] is the caller's scratch. Each chunk is summed,
+ * then each channel's chunks in order: the same result on every call. */
+int n2b_project_backward(const int32_t *chunk_ptr, int32_t n_chunks, const int32_t *row_idx,
+                         const int32_t *channel_chunk, int32_t channels, int32_t rows, int32_t hidden,
+                         const float *du, float *partials, float *dw_in, void *stream);
+
 /* ---- Run-time compiled step kernels of user-defined models ---------------
  * The transpiler (naer2_b200/transpiler) lowers a population's Python hooks
  * (receive / update / send) to CUDA device code inside a step-kernel template;

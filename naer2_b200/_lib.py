@@ -82,6 +82,9 @@ SIGNATURES = {
     "n2b_bptt_status": (ctypes.c_int, [ctypes.POINTER(BpttDesc), _P, ctypes.c_size_t,
                                        ctypes.POINTER(ctypes.c_int32), _P]),
     "n2b_bptt_spikes": (ctypes.c_int, [ctypes.POINTER(BpttDesc), _P, ctypes.c_size_t, _P, _P]),
+    "n2b_project_forward": (ctypes.c_int, [_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P, _P]),
+    "n2b_project_backward": (ctypes.c_int, [_P, ctypes.c_int32, _P, _P, ctypes.c_int32, ctypes.c_int32,
+                                            ctypes.c_int32, _P, _P, _P, _P]),
     "n2b_jit_compile": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_char_p),
                                        ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(_P)]),
     "n2b_jit_launch": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32, _P, ctypes.c_size_t, _P]),

@@ -119,6 +119,100 @@ class Wiring:
         self.out_degree = torch.from_numpy(np.bincount(pre, minlength=hidden)).to(dev)
 
 
+class SpikeEvents:
+    """Binary input spikes x [T, B, C] as the projection kernels read them, built once per input (like a data
+    loader's output): by input row r = t * B + b (`row_ptr` [T*B + 1], `channel`: its spiking channels,
+    ascending) and by channel in chunks of at most CHUNK rows (`row_idx`: rows ascending per channel,
+    `chunk_ptr` [n_chunks + 1], `channel_chunk` [C + 1]: each channel's first chunk)."""
+
+    CHUNK = 128
+
+    def __init__(self, rows: torch.Tensor, chans: torch.Tensor, steps: int, batch: int, channels: int):
+        n_rows = steps * batch
+        rows, chans = rows.long().reshape(-1), chans.long().reshape(-1)
+        if rows.numel() and (int(rows.min()) < 0 or int(rows.max()) >= n_rows or int(chans.min()) < 0
+                             or int(chans.max()) >= channels):
+            raise ValueError("spike event out of range")
+        dev = rows.device
+        key = torch.unique(rows * channels + chans)  # sorted by (row, channel), duplicates merged
+        r, c = key // channels, key % channels
+        self.steps, self.batch, self.channels, self.nnz = steps, batch, channels, int(key.numel())
+        self.row_ptr = torch.zeros(n_rows + 1, dtype=torch.int32, device=dev)
+        self.row_ptr[1:] = torch.cumsum(torch.bincount(r, minlength=n_rows), 0)
+        self.channel = c.int()
+        key2 = torch.sort(c * n_rows + r).values  # by (channel, row)
+        c2 = key2 // n_rows
+        self.row_idx = (key2 % n_rows).int()
+        counts = torch.bincount(c2, minlength=channels)
+        col_start = torch.zeros(channels + 1, dtype=torch.long, device=dev)
+        col_start[1:] = torch.cumsum(counts, 0)
+        chunks = (counts + self.CHUNK - 1) // self.CHUNK
+        self.channel_chunk = torch.zeros(channels + 1, dtype=torch.int32, device=dev)
+        self.channel_chunk[1:] = torch.cumsum(chunks, 0)
+        self.n_chunks = int(self.channel_chunk[-1])
+        owner = torch.repeat_interleave(torch.arange(channels, device=dev), chunks)
+        j = torch.arange(self.n_chunks, device=dev) - self.channel_chunk[owner].long()
+        start = col_start[owner] + j * self.CHUNK
+        self.chunk_ptr = torch.cat([start, torch.tensor([self.nnz], device=dev)]).int()
+
+    @classmethod
+    def from_dense(cls, x: torch.Tensor) -> "SpikeEvents":
+        T, B, C = x.shape
+        if bool(((x != 0) & (x != 1)).any()):
+            raise ValueError("the input must be binary spikes")
+        idx = torch.nonzero(x.reshape(T * B, C))
+        return cls(idx[:, 0], idx[:, 1], T, B, C)
+
+    @classmethod
+    def from_sparse(cls, x: torch.Tensor, steps: int) -> "SpikeEvents":
+        x = x.coalesce()
+        if bool((x.values() != 1).any()):
+            raise ValueError("the input must be binary spikes")
+        n_rows, C = x.shape
+        if n_rows % steps:
+            raise ValueError("rows of the sparse input must be steps x batch")
+        return cls(x.indices()[0], x.indices()[1], steps, n_rows // steps, C)
+
+
+def project(events: SpikeEvents, w_in: torch.Tensor) -> torch.Tensor:
+    """U [T, B, H] = x @ w_in through n2b_project_forward (channel order per row)."""
+    C, H = w_in.shape
+    if C != events.channels or not w_in.is_cuda or w_in.dtype != torch.float32:
+        raise RuntimeError("w_in must be a CUDA fp32 [channels, hidden] tensor (no CPU fallback)")
+    w = w_in.detach().contiguous()
+    u = torch.empty(events.steps, events.batch, H, dtype=torch.float32, device=w.device)
+    s = ctypes.c_void_p(torch.cuda.current_stream(w.device).cuda_stream)
+    _lib.check(_lib.load().n2b_project_forward(events.row_ptr.data_ptr(), events.channel.data_ptr(),
+                                               events.steps * events.batch, C, H, w.data_ptr(), u.data_ptr(), s),
+               "n2b_project_forward")
+    return u
+
+
+def project_grad(events: SpikeEvents, du: torch.Tensor) -> torch.Tensor:
+    """dw_in [C, H] = x^T du through n2b_project_backward (per channel: chunks of rows, then the chunks in order)."""
+    du = du.contiguous()
+    H = du.shape[-1]
+    partials = torch.empty(max(events.n_chunks, 1), H, dtype=torch.float32, device=du.device)
+    dw = torch.empty(events.channels, H, dtype=torch.float32, device=du.device)
+    s = ctypes.c_void_p(torch.cuda.current_stream(du.device).cuda_stream)
+    _lib.check(_lib.load().n2b_project_backward(events.chunk_ptr.data_ptr(), events.n_chunks,
+                                                events.row_idx.data_ptr(), events.channel_chunk.data_ptr(),
+                                                events.channels, events.steps * events.batch, H, du.data_ptr(),
+                                                partials.data_ptr(), dw.data_ptr(), s), "n2b_project_backward")
+    return dw
+
+
+class _ProjectFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, w_in, events):
+        ctx.events = events
+        return project(events, w_in)
+
+    @staticmethod
+    def backward(ctx, du):
+        return (project_grad(ctx.events, du) if ctx.needs_input_grad[0] else None), None
+
+
 class RecurrentLIF(torch.nn.Module):
     """The BPTT workload's layer. Parameters: w_in [C, H], w_rec [nnz] (canonical order: by post, then pre),
     w_out [H, R]. `forward(x)` returns m [B, R]; `infer(x)` is the plain forward (no tape, no autograd)."""
@@ -172,15 +266,18 @@ class RecurrentLIF(torch.nn.Module):
             self._ws_key = key
         return self._ws
 
-    def current(self, x: torch.Tensor, steps: int | None = None) -> torch.Tensor:
-        """U [T, B, H] = x @ w_in. x: binary [T, B, C] (dense), or a sparse COO matrix [T * B, C] (row t * B + b)
-        with `steps` = T."""
-        if x.is_sparse:
-            if steps is None:
-                raise ValueError("a sparse input needs steps=T")
-            return torch.sparse.mm(x, self.w_in).reshape(steps, -1, self.hidden)
-        T, B, C = x.shape
-        return torch.sparse.mm(x.reshape(T * B, C).float().to_sparse(), self.w_in).reshape(T, B, self.hidden)
+    def current(self, x, steps: int | None = None) -> torch.Tensor:
+        """U [T, B, H] = x @ w_in (autograd to w_in). x: SpikeEvents, binary [T, B, C] (dense), or a sparse COO
+        matrix [T * B, C] (row t * B + b) with `steps` = T; the last two are turned into SpikeEvents on every
+        call, so a caller that reuses an input builds its SpikeEvents once."""
+        if not isinstance(x, SpikeEvents):
+            if x.is_sparse:
+                if steps is None:
+                    raise ValueError("a sparse input needs steps=T")
+                x = SpikeEvents.from_sparse(x, steps)
+            else:
+                x = SpikeEvents.from_dense(x)
+        return _ProjectFn.apply(self.w_in, x)
 
     def forward(self, x: torch.Tensor, steps: int | None = None) -> torch.Tensor:
         U = self.current(x, steps)

@@ -772,6 +772,78 @@ __global__ void gather_kernel(const float *src, const int32_t *perm, int n, floa
     if (l < n) dst[l] = src[perm[l]];
 }
 
+// ------------------------------------------------------------------------------------------------ input projection
+
+// U[r] = sum over the spiking channels c of input row r (ascending) of w_in[c]: H / 4 threads per row, one float4
+// of hidden units each, blockDim / (H / 4) rows per block; the channel indices of a row four at a time, then their
+// weight rows. An index outside [0, C) adds nothing (the event lists are checked when they are built).
+__global__ void __launch_bounds__(256) project_fwd_kernel(const int32_t *row_ptr, const int32_t *ch, int rows,
+                                                          int C, int H, const float *w, float *u) {
+    const int h4 = H / 4;
+    const int r = blockIdx.x * (blockDim.x / h4) + threadIdx.x / h4, c4 = threadIdx.x % h4;
+    if (r >= rows) return;
+    const int k0 = row_ptr[r], k1 = row_ptr[r + 1];
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int k = k0; k < k1; k += 4) {
+        int c[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) c[j] = k + j < k1 ? __ldg(ch + k + j) : -1;
+        float4 v[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            v[j] = (c[j] >= 0 && c[j] < C) ? __ldg(reinterpret_cast<const float4 *>(w + (size_t)c[j] * H) + c4)
+                                           : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (c[j] < 0 || c[j] >= C) continue;
+            acc.x = __fadd_rn(acc.x, v[j].x);
+            acc.y = __fadd_rn(acc.y, v[j].y);
+            acc.z = __fadd_rn(acc.z, v[j].z);
+            acc.w = __fadd_rn(acc.w, v[j].w);
+        }
+    }
+    reinterpret_cast<float4 *>(u + (size_t)r * H)[c4] = acc;
+}
+
+// dw_in, first pass: chunk k (rows row_idx[chunk_ptr[k] .. chunk_ptr[k + 1]) of one channel, ascending) summed
+// into partials[k]; a block per chunk, H / 4 threads, four rows' loads in flight. A row outside [0, rows) adds
+// nothing.
+__global__ void __launch_bounds__(256) project_bwd_chunk_kernel(const int32_t *chunk_ptr, const int32_t *row_idx,
+                                                                int rows, int H, const float *du, float *partials) {
+    const int k = blockIdx.x, c4 = threadIdx.x;
+    const int j0 = chunk_ptr[k], j1 = chunk_ptr[k + 1];
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int j = j0; j < j1; j += 4) {
+        int r[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) r[i] = j + i < j1 ? __ldg(row_idx + j + i) : -1;
+        float4 v[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            v[i] = (r[i] >= 0 && r[i] < rows) ? __ldcs(reinterpret_cast<const float4 *>(du + (size_t)r[i] * H) + c4)
+                                              : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if (r[i] < 0 || r[i] >= rows) continue;
+            acc.x = __fadd_rn(acc.x, v[i].x);
+            acc.y = __fadd_rn(acc.y, v[i].y);
+            acc.z = __fadd_rn(acc.z, v[i].z);
+            acc.w = __fadd_rn(acc.w, v[i].w);
+        }
+    }
+    reinterpret_cast<float4 *>(partials + (size_t)k * H)[c4] = acc;
+}
+
+// dw_in, second pass: channel c's chunks (ch_chunk[c] .. ch_chunk[c + 1]) added in chunk order.
+__global__ void project_bwd_reduce_kernel(const int32_t *ch_chunk, int C, int H, const float *partials, float *dw) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (size_t)C * H) return;
+    const int c = (int)(e / H), h = (int)(e % H);
+    float s = 0.f;
+    for (int k = ch_chunk[c]; k < ch_chunk[c + 1]; ++k) s = __fadd_rn(s, partials[(size_t)k * H + h]);
+    dw[e] = s;
+}
+
 }  // namespace n2b_bptt
 
 // ------------------------------------------------------------------------------------------------ host
@@ -1062,6 +1134,43 @@ int n2b_bptt_spikes(const n2b_bptt_desc *d, void *workspace, size_t workspace_by
     const size_t n = d->smooth ? sizeof(float) * T * NC * H * NS : T * NC * H;
     B_CUDA(cudaMemcpyAsync(out, static_cast<char *>(workspace) + L.spikes, n, cudaMemcpyDeviceToDevice,
                            reinterpret_cast<cudaStream_t>(stream)));
+    return N2B_OK;
+}
+
+int n2b_project_forward(const int32_t *row_ptr, const int32_t *channel, int32_t rows, int32_t channels,
+                        int32_t hidden, const float *w_in, float *u, void *stream) {
+    if (rows < 0 || channels <= 0 || hidden <= 0 || hidden % 4 || hidden > 1024)
+        return bfail(N2B_EINVAL, "project: rows >= 0, channels > 0, hidden a multiple of 4 up to 1024");
+    if (rows == 0) return N2B_OK;
+    if (!row_ptr || !channel || !w_in || !u) return bfail(N2B_EINVAL, "project: missing arguments");
+    if ((reinterpret_cast<uintptr_t>(w_in) | reinterpret_cast<uintptr_t>(u)) & 15)
+        return bfail(N2B_EINVAL, "project: w_in and u must be 16-byte aligned");
+    const int h4 = hidden / 4, rpb = std::max(1, 256 / h4);
+    project_fwd_kernel<<<(unsigned)((rows + rpb - 1) / rpb), (unsigned)(rpb * h4), 0,
+                         reinterpret_cast<cudaStream_t>(stream)>>>(row_ptr, channel, rows, channels, hidden, w_in, u);
+    B_CUDA(cudaGetLastError());
+    return N2B_OK;
+}
+
+int n2b_project_backward(const int32_t *chunk_ptr, int32_t n_chunks, const int32_t *row_idx,
+                         const int32_t *channel_chunk, int32_t channels, int32_t rows, int32_t hidden,
+                         const float *du, float *partials, float *dw_in, void *stream) {
+    if (n_chunks < 0 || rows < 0 || channels <= 0 || hidden <= 0 || hidden % 4 || hidden > 1024)
+        return bfail(N2B_EINVAL, "project: n_chunks, rows >= 0, channels > 0, hidden a multiple of 4 up to 1024");
+    if (!channel_chunk || !dw_in || (n_chunks > 0 && (!chunk_ptr || !row_idx || !du || !partials)))
+        return bfail(N2B_EINVAL, "project: missing arguments");
+    if ((reinterpret_cast<uintptr_t>(du) | reinterpret_cast<uintptr_t>(partials)) & 15)
+        return bfail(N2B_EINVAL, "project: du and partials must be 16-byte aligned");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    if (n_chunks > 0) {
+        project_bwd_chunk_kernel<<<(unsigned)n_chunks, (unsigned)(hidden / 4), 0, s>>>(chunk_ptr, row_idx, rows,
+                                                                                     hidden, du, partials);
+        B_CUDA(cudaGetLastError());
+    }
+    const size_t n = (size_t)channels * hidden;
+    project_bwd_reduce_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(channel_chunk, channels, hidden, partials,
+                                                                          dw_in);
+    B_CUDA(cudaGetLastError());
     return N2B_OK;
 }
 

@@ -108,6 +108,36 @@ def test_bank_order_spreads_the_gather_over_the_banks():
     assert passes(oc & 0x7FF) < 0.8 * passes(sorted_post)
 
 
+def test_spike_events_by_row_and_by_channel_chunks():
+    """SpikeEvents (CPU tensors here): the row lists reproduce x; the chunks cover each channel's rows in
+    ascending order, at most CHUNK rows each, never two channels in one chunk; dense and sparse inputs agree."""
+    from naer2_b200.bptt import SpikeEvents
+
+    g = torch.Generator().manual_seed(3)
+    T, B, C = 30, 8, 40
+    x = (torch.rand(T, B, C, generator=g) < torch.linspace(0.0, 0.9, C)).float()  # channel 0 silent
+    ev = SpikeEvents.from_dense(x)
+    dense = torch.zeros(T * B, C)
+    rows = torch.repeat_interleave(torch.arange(T * B), (ev.row_ptr[1:] - ev.row_ptr[:-1]).long())
+    dense[rows, ev.channel.long()] = 1.0
+    assert torch.equal(dense, x.reshape(T * B, C))
+    for r in range(0, T * B, 17):
+        ch = ev.channel[ev.row_ptr[r]:ev.row_ptr[r + 1]]
+        assert torch.equal(ch, torch.sort(ch).values)
+    cp, cc = ev.chunk_ptr.long(), ev.channel_chunk.long()
+    assert int(cp[-1]) == ev.nnz == int(x.sum())
+    for c in range(C):
+        got = ev.row_idx[cp[cc[c]]:cp[cc[c + 1]]].long()
+        assert torch.equal(got, torch.nonzero(x.reshape(T * B, C)[:, c]).reshape(-1))
+        assert all(0 < int(cp[k + 1] - cp[k]) <= SpikeEvents.CHUNK for k in range(int(cc[c]), int(cc[c + 1])))
+    assert int(cc[1]) == 0 and int((cc[1:] - cc[:-1]).max()) > 1
+    sp = SpikeEvents.from_sparse(x.reshape(T * B, C).to_sparse(), T)
+    for name in ("row_ptr", "channel", "row_idx", "chunk_ptr", "channel_chunk"):
+        assert torch.equal(getattr(sp, name), getattr(ev, name))
+    with pytest.raises(ValueError):
+        SpikeEvents.from_dense(x * 2)
+
+
 def test_task_templates_and_samples():
     rates = bptt_task.templates(classes=5, channels=50, steps=60, seed=2)
     assert rates.shape == (5, 60, 50) and rates.min() >= 0 and rates.max() <= 50

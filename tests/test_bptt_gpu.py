@@ -100,8 +100,8 @@ def test_spiking_kernels_match_the_teacher_forced_fp64_reference(cuda, K):
 
 def test_checkpoint_interval_changes_nothing(cuda):
     """The kernels' outputs (dU, dw_rec, dw_out) are bit-identical for any checkpoint interval: the recomputed
-    segments reproduce the forward exactly. (w_in's gradient, x^T dU, comes from torch's sparse product,
-    whose summation order is not fixed.)"""
+    segments reproduce the forward exactly. (w_in's gradient, x^T dU, does not depend on them: its kernels
+    are tested on their own.)"""
     out = []
     for K in (1, 7, 60):
         layer, x, y = make(cuda, B=16, T=60, K=K, seed=4)
@@ -144,3 +144,32 @@ def test_workload_gradients_match_the_fp64_reference(cuda):
     assert rel(m, m64) < 1e-5
     for g, r in zip(grads, g64):
         assert rel(g, r) < 1e-4
+
+
+def test_projection_kernels_match_the_dense_product_and_repeat(cuda):
+    """n2b_project_forward / n2b_project_backward against x @ w_in and x^T dU in float64 (1e-6 and 1e-5
+    relative), on the BPTT workload's input statistics (some channels with far more events than others, so that
+    channels span several chunks), bit-identical on a second call; empty rows and channels included."""
+    from naer2_b200.bptt import SpikeEvents, project, project_grad
+
+    T, B, C, H = 120, 64, 700, 1024
+    rates = bptt_task.templates(classes=20, channels=C, steps=T, seed=5)
+    x, _ = bptt_task.sample(rates, B, seed=6, device=cuda)
+    x = x.clone()
+    x[:, :, 3] = 0  # a channel without events
+    x[7] = 0  # a step without events
+    g = torch.Generator(device="cpu").manual_seed(7)
+    w = torch.randn(C, H, generator=g).to(cuda)
+    du = torch.randn(T, B, H, generator=g).to(cuda)
+    ev = SpikeEvents.from_dense(x)
+    assert ev.n_chunks > C // 2 and int((ev.channel_chunk[1:] - ev.channel_chunk[:-1]).max()) > 1
+    xd = x.reshape(T * B, C).double()
+    u, u2 = project(ev, w), project(ev, w)
+    ref_u = (xd @ w.double()).reshape(T, B, H)
+    assert torch.equal(u, u2)
+    assert float((u.double() - ref_u).abs().max() / ref_u.abs().max()) < 1e-6
+    dw, dw2 = project_grad(ev, du), project_grad(ev, du)
+    ref_dw = xd.t() @ du.reshape(T * B, H).double()
+    assert torch.equal(dw, dw2)
+    assert float((dw.double() - ref_dw).abs().max() / ref_dw.abs().max()) < 1e-5
+    assert float(dw[3].abs().max()) == 0.0
