@@ -34,6 +34,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <type_traits>
 
@@ -896,7 +897,7 @@ WsLayout ws_layout(const n2b_bptt_desc *d) {
     size_t o = 0;
     L.spikes = o; o = a256(o + (d->smooth ? sizeof(float) * T * NC * H * NS : T * NC * H));
     L.vck = o; o = a256(o + sizeof(float) * nseg * B * H);
-    L.gseg = o; o = a256(o + sizeof(float) * K * B * H);
+    L.gseg = o; o = a256(o + sizeof(float) * 2 * K * B * H);  // two segments: one recomputed, one run back
     L.outw = o; o = a256(o + sizeof(float) * std::max<size_t>(d->nnz, 1));
     L.dwp = o; o = a256(o + sizeof(float) * NC * std::max<size_t>(d->nnz, 1));
     L.dwo = o; o = a256(o + sizeof(float) * NC * H * R);
@@ -996,6 +997,39 @@ int coop_groups(Kern kern, int threads, size_t smem, int &groups) {
     return N2B_OK;
 }
 
+// The backward's two internal streams on a device, made on first use and kept: the adjoint on the highest
+// priority, the next segment's recompute on the lowest, so that when both are ready the adjoint's CTAs are placed
+// first and the recompute fills the SMs the adjoint leaves free.
+struct SideStreams {
+    cudaStream_t hi = nullptr, lo = nullptr;
+};
+int side_streams(SideStreams &out) {
+    static std::mutex mu;
+    static SideStreams per_dev[64];
+    int dev = 0;
+    B_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return bfail(N2B_EINVAL, "device index above 63");
+    std::lock_guard<std::mutex> lock(mu);
+    SideStreams &st = per_dev[dev];
+    if (!st.hi) {
+        int least = 0, greatest = 0;
+        B_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        B_CUDA(cudaStreamCreateWithPriority(&st.hi, cudaStreamNonBlocking, greatest));
+        B_CUDA(cudaStreamCreateWithPriority(&st.lo, cudaStreamNonBlocking, least));
+    }
+    out = st;
+    return N2B_OK;
+}
+
+// Events of one backward call, destroyed on every return (pending work keeps them alive as long as it needs).
+struct CallEvents {
+    cudaEvent_t e[6] = {};
+    ~CallEvents() {
+        for (cudaEvent_t x : e)
+            if (x) cudaEventDestroy(x);
+    }
+};
+
 template <class Kern, class... Rest>
 int launch_coop(Kern kern, int grid, int threads, size_t smem, cudaStream_t s, const Args &a, Rest... rest) {
     cudaLaunchConfig_t cfg = {};
@@ -1081,34 +1115,69 @@ int n2b_bptt_backward(const n2b_bptt_desc *d, const float *u, const float *w_rec
     rc = smooth ? coop_groups(bwd_kernel<true>, threads, S.total, per_launch)
                 : coop_groups(bwd_kernel<false>, threads, S.total, per_launch);
     if (rc) return rc;
-    for (int seg = nseg - 1; seg >= 0; --seg) {  // each segment: recompute from its checkpoint, then backwards
+    SideStreams st;
+    rc = side_streams(st);
+    if (rc) return rc;
+    CallEvents ev;  // fork, recomputed[2], adjoint done[2], join
+    for (cudaEvent_t &x : ev.e) B_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+    cudaEvent_t fork = ev.e[0], join = ev.e[5], *rec = ev.e + 1, *adj = ev.e + 3;
+    B_CUDA(cudaEventRecord(fork, s));
+    B_CUDA(cudaStreamWaitEvent(st.hi, fork, 0));
+    B_CUDA(cudaStreamWaitEvent(st.lo, fork, 0));
+    float *gbuf[2] = {a.g_seg, a.g_seg + (size_t)std::min(K, d->steps) * d->batch * d->hidden};
+    // segment seg recomputed from its checkpoint into gbuf[seg & 1] on the low-priority stream
+    auto recompute = [&](int seg) -> int {
         const int t0 = seg * K, t1 = std::min(d->steps, t0 + K);
+        Args ra = a;
+        ra.g_seg = gbuf[seg & 1];
         const dim3 rgrid((unsigned)(d->hidden / (rthreads / NT)), (unsigned)NC, (unsigned)((t1 - t0 + TC - 1) / TC));
         const unsigned vblocks = (unsigned)((d->batch * d->hidden + 255) / 256);
         if (smooth) {
-            recompute_r_kernel<true><<<rgrid, rthreads, 0, s>>>(a, t0, t1);
-            recompute_v_kernel<true><<<vblocks, 256, 0, s>>>(a, seg, t0, t1);
+            recompute_r_kernel<true><<<rgrid, rthreads, 0, st.lo>>>(ra, t0, t1);
+            recompute_v_kernel<true><<<vblocks, 256, 0, st.lo>>>(ra, seg, t0, t1);
         } else {
-            recompute_r_kernel<false><<<rgrid, rthreads, rsmem, s>>>(a, t0, t1);
-            recompute_v_kernel<false><<<vblocks, 256, 0, s>>>(a, seg, t0, t1);
+            recompute_r_kernel<false><<<rgrid, rthreads, rsmem, st.lo>>>(ra, t0, t1);
+            recompute_v_kernel<false><<<vblocks, 256, 0, st.lo>>>(ra, seg, t0, t1);
         }
         B_CUDA(cudaGetLastError());
+        B_CUDA(cudaEventRecord(rec[seg & 1], st.lo));
+        return N2B_OK;
+    };
+    // Segments run backwards. The recompute of segment seg - 1 overlaps the adjoint of seg; it reuses the buffer
+    // of seg + 1, so it waits for that adjoint.
+    rc = recompute(nseg - 1);
+    if (rc) return rc;
+    for (int seg = nseg - 1; seg >= 0; --seg) {
+        const int t0 = seg * K, t1 = std::min(d->steps, t0 + K);
         const int first = seg == nseg - 1;
-        B_CUDA(cudaMemsetAsync(a.xcnt, 0, sizeof(uint32_t) * NC, s));
+        Args ba = a;
+        ba.g_seg = gbuf[seg & 1];
+        B_CUDA(cudaStreamWaitEvent(st.hi, rec[seg & 1], 0));
+        B_CUDA(cudaMemsetAsync(a.xcnt, 0, sizeof(uint32_t) * NC, st.hi));
         for (int g0 = 0; g0 < NC; g0 += per_launch) {
             const int grid = std::min(per_launch, NC - g0) * CL;
-            rc = smooth ? launch_coop(bwd_kernel<true>, grid, threads, S.total, s, a, d->out_cta_max, t0, t1, first, g0)
-                        : launch_coop(bwd_kernel<false>, grid, threads, S.total, s, a, d->out_cta_max, t0, t1, first, g0);
+            rc = smooth ? launch_coop(bwd_kernel<true>, grid, threads, S.total, st.hi, ba, d->out_cta_max, t0, t1,
+                                      first, g0)
+                        : launch_coop(bwd_kernel<false>, grid, threads, S.total, st.hi, ba, d->out_cta_max, t0, t1,
+                                      first, g0);
+            if (rc) return rc;
+        }
+        B_CUDA(cudaEventRecord(adj[seg & 1], st.hi));
+        if (seg > 0) {
+            if (seg + 1 < nseg) B_CUDA(cudaStreamWaitEvent(st.lo, adj[(seg + 1) & 1], 0));
+            rc = recompute(seg - 1);
             if (rc) return rc;
         }
     }
     if (d->nnz > 0) {
-        reduce_dw_kernel<<<(d->nnz + 255) / 256, 256, 0, s>>>(a.dwp, d->out_perm, d->nnz, NC, dw_rec);
+        reduce_dw_kernel<<<(d->nnz + 255) / 256, 256, 0, st.hi>>>(a.dwp, d->out_perm, d->nnz, NC, dw_rec);
         B_CUDA(cudaGetLastError());
     }
     const int n = d->hidden * d->readouts;
-    reduce_dwo_kernel<<<(n + 255) / 256, 256, 0, s>>>(a.dwo_p, n, NC, dw_out);
+    reduce_dwo_kernel<<<(n + 255) / 256, 256, 0, st.hi>>>(a.dwo_p, n, NC, dw_out);
     B_CUDA(cudaGetLastError());
+    B_CUDA(cudaEventRecord(join, st.hi));
+    B_CUDA(cudaStreamWaitEvent(s, join, 0));
     return N2B_OK;
 }
 
