@@ -128,7 +128,7 @@ __host__ __device__ inline BwdSmem bwd_smem(int H, int HC, int R, int out_cta_ma
     L.pnew = o; o = a16(o + sizeof(float) * H * QROW);
     L.part = o; o = a16(o + sizeof(float) * RING * HC * NS);
     L.dwo = o; o = a16(o + sizeof(float) * HC * R);
-    L.obuf = o; o = a16(o + sizeof(float) * NS * R);
+    L.obuf = o; o = a16(o + sizeof(float) * 2 * NS * R);  // o[t] in half t & 1
     L.grp = o; o = a16(o + sizeof(int32_t) * HC * (MAXD + 1));
     L.code = o; o = a16(o + sizeof(uint16_t) * out_cta_max);
     L.w = o; o = a16(o + sizeof(float) * out_cta_max);
@@ -437,13 +437,13 @@ __global__ void __launch_bounds__(256) recompute_r_kernel(const __grid_constant_
             const int sh = 8 * (MAXD - d);  // byte of step tc - d
             const uint64_t win = sh ? (lo >> sh) | (hi << (64 - sh)) : lo;  // steps tc - d ...
             if (!(win & ((1ull << (8 * TC)) - 1))) continue;
+            // branch-free: a clear bit adds +0.0f, which leaves a sum that started at +0 unchanged bit for bit
+            // (it is never -0), so the sums stay the forward's
 #pragma unroll
             for (int k = 0; k < TC; ++k) {
-                const uint32_t byte = (uint32_t)(win >> (8 * k)) & 0xffu;
-                if (!byte || k >= kend) continue;
+                const uint32_t byte = k < kend ? (uint32_t)(win >> (8 * k)) & 0xffu : 0u;
 #pragma unroll
-                for (int b = 0; b < NS; ++b)
-                    if ((byte >> b) & 1u) acc[k][b] = __fadd_rn(acc[k][b], wl);
+                for (int b = 0; b < NS; ++b) acc[k][b] = __fadd_rn(acc[k][b], ((byte >> b) & 1u) ? wl : 0.f);
             }
         }
     }
@@ -648,12 +648,15 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
     float stn[NS];
     uint32_t sbn;
     spikes_at(t1 - 1, stn, sbn);
+    // the readout adjoint o[t] does not depend on q: it is made one step ahead, into the other half of obuf, so
+    // that no barrier is needed for it (the half of o[t - 1] was last read at step t + 1, three barriers back)
+    if (ro) {
+        o = __fadd_rn(t1 - 1 == tsv ? dmv : 0.f, __fmul_rn(a.beta, o));
+        obuf[(size_t)((t1 - 1) & 1) * NS * R + rb * R + rr] = o;
+    }
+    __syncthreads();  // o[t1 - 1] ready
     for (int t = t1 - 1; t >= t0; --t) {
-        if (ro) {
-            o = __fadd_rn(t == tsv ? dmv : 0.f, __fmul_rn(a.beta, o));
-            obuf[rb * R + rr] = o;
-        }
-        __syncthreads();  // obuf ready; the previous step's partial-ring writes done
+        const float *ob = obuf + (size_t)(t & 1) * NS * R;  // o[t]
         float qv0 = 0.f, qv1 = 0.f;
         float st[NS];
 #pragma unroll
@@ -671,7 +674,7 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
                 const int bl = SPT * sub + j;
                 float *pp = part + ((size_t)(t % RING) * HC + pl) * NS + bl;
                 float sh = *pp;
-                for (int r = 0; r < R; ++r) sh = __fmaf_rn(__ldg(wout + pl * R + r), obuf[bl * R + r], sh);
+                for (int r = 0; r < R; ++r) sh = __fmaf_rn(__ldg(wout + pl * R + r), ob[bl * R + r], sh);
                 *pp = 0.f;
                 const float g = j ? gc1 : gc0;
                 const float ap = __fmul_rn(a.alpha, j ? qp1 : qp0);
@@ -687,12 +690,16 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
                 for (int r = sub * R4; r < min(R, (sub + 1) * R4); ++r) {
                     float acc = dwo[pl * R + r];
                     for (int b = 0; b < NS; ++b) {
-                        if constexpr (SMOOTH) acc = __fmaf_rn(st[b], obuf[b * R + r], acc);
-                        else if ((sbyte_t >> b) & 1u) acc = __fadd_rn(acc, obuf[b * R + r]);
+                        if constexpr (SMOOTH) acc = __fmaf_rn(st[b], ob[b * R + r], acc);
+                        else if ((sbyte_t >> b) & 1u) acc = __fadd_rn(acc, ob[b * R + r]);
                     }
                     dwo[pl * R + r] = acc;
                 }
             }
+        }
+        if (ro && t > t0) {  // o[t - 1]; o keeps o[t0] for the segment before this one
+            o = __fadd_rn(t - 1 == tsv ? dmv : 0.f, __fmul_rn(a.beta, o));
+            obuf[(size_t)((t - 1) & 1) * NS * R + rb * R + rr] = o;
         }
         float *slot = a.qx + ((size_t)q * 2 + (t & 1)) * H * NS;
         if (nt) reinterpret_cast<float2 *>(slot)[(size_t)me * (NS / 2) + sub] = make_float2(qv0, qv1);
