@@ -144,13 +144,15 @@ __device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster
 __device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
 
 // One CTA's arrival at a group step (thread 0, after a __syncthreads that follows the CTA's writes): a release
-// add on the group's counter, then a bounded acquire spin until `target` arrivals (every CTA of the group at
-// this step). A wait that gives up counts in err[3] and sets `aborted`, after which the CTA still arrives but
-// no longer waits, so that neither it nor the CTAs that wait for its arrivals can hang.
+// add on the group's counter; later (other work in between), a bounded acquire spin until `target` arrivals
+// (every CTA of the group at this step). A wait that gives up counts in err[3] and sets `aborted`, after which
+// the CTA still arrives but no longer waits, so that neither it nor the CTAs that wait for its arrivals can hang.
 constexpr int XCHG_SPIN_LIMIT = 1 << 21;  // polls of an L2 round trip each: about a second
-__device__ __forceinline__ void group_arrive_wait(uint32_t *cnt, uint32_t target, int32_t *err, int &aborted) {
+__device__ __forceinline__ void group_arrive(uint32_t *cnt) {
     __threadfence();
     asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(cnt) : "memory");
+}
+__device__ __forceinline__ void group_wait(const uint32_t *cnt, uint32_t target, int32_t *err, int &aborted) {
     if (aborted) return;
     for (int it = 0;; ++it) {
         uint32_t v;
@@ -648,6 +650,29 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
     float stn[NS];
     uint32_t sbn;
     spikes_at(t1 - 1, stn, sbn);
+    // outgoing rows of neuron me, delay group d, at step u (q[u] in pnew): partial[u - d] += w q[u][post];
+    // dw += s[u - d][me] q[u][post] (sbyte, sf: the spikes at u - d). Every thread of the CTA calls it.
+    auto out_rows = [&](int u, int d, uint32_t sbyte, const float *sf) {
+        float acc[NS];
+#pragma unroll
+        for (int b = 0; b < NS; ++b) acc[b] = 0.f;
+        const int gs = nt ? grp[pl * (MAXD + 1) + d - 1] : 0, ge = nt ? grp[pl * (MAXD + 1) + d] : 0;
+        if (__any_sync(FULL, sbyte != 0u))  // the same branch for the whole warp
+            out_group<SMOOTH, true>(ocode, ow, pnew, dw, gs, ge, sub, sbyte != 0u, sbyte, sf, acc);
+        else
+            out_group<SMOOTH, false>(ocode, ow, pnew, dw, gs, ge, sub, false, 0u, sf, acc);
+#pragma unroll
+        for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __shfl_xor_sync(FULL, acc[b], 1));
+#pragma unroll
+        for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __shfl_xor_sync(FULL, acc[b], 2));
+        if (nt && u - d >= 0) {
+            float x0, x1;
+            mine(acc, sub, x0, x1);
+            float *pp = part + ((size_t)((u - d) % RING) * HC + pl) * NS + SPT * sub;
+            pp[0] = __fadd_rn(pp[0], x0);
+            pp[1] = __fadd_rn(pp[1], x1);
+        }
+    };
     // the readout adjoint o[t] does not depend on q: it is made one step ahead, into the other half of obuf, so
     // that no barrier is needed for it (the half of o[t - 1] was last read at step t + 1, three barriers back)
     if (ro) {
@@ -705,35 +730,21 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
         if (nt) reinterpret_cast<float2 *>(slot)[(size_t)me * (NS / 2) + sub] = make_float2(qv0, qv1);
         __syncthreads();  // this CTA's q[t] written
         target += CL;
-        if (tid == 0) group_arrive_wait(xcnt, target, a.err, aborted);
-        __syncthreads();  // every CTA's q[t] written: copy all of them (past L1) into pnew
+        if (tid == 0) group_arrive(xcnt);
+        // while the group's other CTAs arrive: step t + 1's delay groups 2..5 (pnew still holds q[t + 1]; their
+        // partials are for steps t - 1 and earlier, so only the delay-1 group waits for q[t])
+        if (t + 1 < t1) {
+#pragma unroll
+            for (int d = 2; d <= MAXD; ++d)
+                out_rows(t + 1, d, SMOOTH ? 0xffu : (uint32_t)((hist >> (8 * (d - 2))) & 0xffu), histf[d - 2]);
+        }
+        if (tid == 0) group_wait(xcnt, target, a.err, aborted);
+        __syncthreads();  // every CTA's q[t] written, every read of q[t + 1] done: copy q[t] (past L1) into pnew
         for (int j = tid; j < H * (NS / 4); j += nthr)
             reinterpret_cast<float4 *>(pnew)[(size_t)(j >> 1) * (QROW / 4) + (j & 1)] =
                 __ldcg(reinterpret_cast<const float4 *>(slot) + j);
         __syncthreads();
-        // outgoing rows: partial[t - d] += w q[t][post]; dw += s[t - d][me] q[t][post]
-        for (int d = 1; d <= MAXD; ++d) {
-            float acc[NS];
-#pragma unroll
-            for (int b = 0; b < NS; ++b) acc[b] = 0.f;
-            const int gs = nt ? grp[pl * (MAXD + 1) + d - 1] : 0, ge = nt ? grp[pl * (MAXD + 1) + d] : 0;
-            const uint32_t sbyte = SMOOTH ? 0xffu : (uint32_t)((hist >> (8 * (d - 1))) & 0xffu);
-            if (__any_sync(FULL, sbyte != 0u))  // the same branch for the whole warp
-                out_group<SMOOTH, true>(ocode, ow, pnew, dw, gs, ge, sub, sbyte != 0u, sbyte, histf[d - 1], acc);
-            else
-                out_group<SMOOTH, false>(ocode, ow, pnew, dw, gs, ge, sub, false, 0u, histf[d - 1], acc);
-#pragma unroll
-            for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __shfl_xor_sync(FULL, acc[b], 1));
-#pragma unroll
-            for (int b = 0; b < NS; ++b) acc[b] = __fadd_rn(acc[b], __shfl_xor_sync(FULL, acc[b], 2));
-            if (nt && t - d >= 0) {
-                float x0, x1;
-                mine(acc, sub, x0, x1);
-                float *pp = part + ((size_t)((t - d) % RING) * HC + pl) * NS + SPT * sub;
-                pp[0] = __fadd_rn(pp[0], x0);
-                pp[1] = __fadd_rn(pp[1], x1);
-            }
-        }
+        out_rows(t, 1, SMOOTH ? 0xffu : (uint32_t)(hist & 0xffu), histf[0]);
         // the spike history of step t - 1: delays 1..5 reach t - 2 .. t - 6
         if constexpr (SMOOTH) {
             for (int d = 1; d <= MAXD; ++d) {
@@ -746,6 +757,10 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
             hist = (hist >> 8) | ((uint64_t)byte << (8 * (MAXD - 1)));
         }
     }
+    // step t0's delay groups 2..5 (q[t0] is still in pnew)
+#pragma unroll
+    for (int d = 2; d <= MAXD; ++d)
+        out_rows(t0, d, SMOOTH ? 0xffu : (uint32_t)((hist >> (8 * (d - 2))) & 0xffu), histf[d - 2]);
     // the state for the segment before this one
     __syncthreads();
     for (int k = tid; k < RING * HC * NS; k += nthr) part_st[k] = part[k];
