@@ -568,7 +568,7 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
     float *ow = reinterpret_cast<float *>(smem + L.w);
     float *dw = reinterpret_cast<float *>(smem + L.dw);
     const int tid = threadIdx.x, nthr = blockDim.x;
-    float *part_st = a.part_st + (size_t)blockIdx.x * RING * HC * NS;
+    float *part_st = a.part_st + ((size_t)q * CL + rank) * RING * HC * NS;  // this group's CTA, in any launch
 
     const bool nt = tid < NT * HC;
     const int pl = nt ? tid / NT : 0, sub = tid % NT;

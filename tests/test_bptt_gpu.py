@@ -173,3 +173,26 @@ def test_projection_kernels_match_the_dense_product_and_repeat(cuda):
     assert torch.equal(dw, dw2)
     assert float((dw.double() - ref_dw).abs().max() / ref_dw.abs().max()) < 1e-5
     assert float(dw[3].abs().max()) == 0.0
+
+
+def test_groups_beyond_one_cooperative_launch(cuda):
+    """B = 152 at H = 1024: 19 groups of 8 samples, more than one cooperative adjoint launch holds at one CTA per
+    SM on 148 SMs (18 groups), so the last group runs in a second launch of each segment. Groups are
+    independent: its samples' m, t* and dU equal those of the same 8 samples run alone, bit for bit."""
+    T, B, C = 30, 152, 40
+    layer = RecurrentLIF(n_in=C, hidden=1024, readouts=5, density=0.1, checkpoint=11, seed=9, device=cuda)
+    rates = bptt_task.templates(classes=5, channels=C, steps=T, seed=9)
+    x, y = bptt_task.sample(rates, B, seed=10, device=cuda)
+    out = []
+    for xb, yb in ((x, y), (x[:, B - 8:].contiguous(), y[B - 8:])):
+        nb = xb.shape[1]
+        with torch.no_grad():
+            U = layer.current(xb).contiguous()
+            m, ts = layer.run_forward(U, tape=True)
+            dm = torch.softmax(m, 1) - torch.nn.functional.one_hot(yb, m.shape[1]).float()
+            du, _, _ = layer.run_backward(U, dm, ts)
+        torch.cuda.synchronize()
+        assert layer.status(nb, T) == [0, 0, 0, 0]
+        out.append((m[-8:], ts[-8:], du[:, -8:]))
+    for a, b in zip(*out):
+        assert torch.equal(a, b)
