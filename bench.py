@@ -232,6 +232,48 @@ def run_reference(args) -> None:
     print(json.dumps(line))
 
 
+def run_transpiled(args, dev) -> dict:
+    """Config 1's network with TranspiledLIF neurons (the built-in LIF's dynamics, its Poisson drive drawn in its
+    own hook): the run-time compiled step kernels, launched from the host once per population and step (no
+    persistent window, no graph), events/s over the timed steps."""
+    import torch
+
+    from naer2_b200.networks import brunel
+
+    t0 = time.perf_counter()
+    net, pops = brunel.build(**brunel.CONFIG1, seed=1, device=dev, transpiled=True)
+    net.run_steps(1)  # builds the runtime: transpiles and compiles the hooks
+    rt = net.runtime
+    build_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        net.run_steps(SIM_STEPS_PER_STEP)
+    torch.cuda.synchronize(dev)
+    ev0, l0 = rt.counters()["events"], rt.launches
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with Clocks(dev.index or 0) as clocks:
+        for k in range(args.steps):
+            flush.zero_()
+            rt.stream.wait_stream(torch.cuda.current_stream(dev))
+            starts[k].record(rt.stream)
+            net.run_steps(SIM_STEPS_PER_STEP)
+            ends[k].record(rt.stream)
+        torch.cuda.synchronize(dev)
+    dev_ms = sum(st.elapsed_time(e) for st, e in zip(starts, ends))
+    events = rt.counters()["events"] - ev0
+    net.check()
+    return {"metric": METRIC, "value": events / (dev_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded draws on the GPU, Brunel model A at config 1's size)",
+            "config": {"workload": "brunel_config1_transpiled", "neurons": sum(len(p.shape) for p in pops.values()),
+                       "sim_steps_per_step": SIM_STEPS_PER_STEP, "launch": "one per population and step, from the host",
+                       "l2": "flushed before every timed step (256 MiB write)"},
+            "us_per_sim_step": dev_ms * 1e3 / (args.steps * SIM_STEPS_PER_STEP),
+            "gpu_launches": rt.launches - l0, "build_s": build_s, "clocks": clocks.summary()}
+
+
 def run_pd14(args, dev) -> dict:
     """Config 2: the full PD14 microcircuit (77,169 neurons, ~3e8 synapses) built on the GPU; events/s over the
     timed steps, population rates and CV-ISI over them."""
@@ -481,6 +523,8 @@ def main() -> int:
     ap.add_argument("--scale", type=float, default=1.0, help="config 2: population sizes times this")
     ap.add_argument("--mode", choices=["persistent", "per-step"], default="persistent",
                     help="a window of steps per cooperative launch, or one launch per step")
+    ap.add_argument("--transpiled", action="store_true",
+                    help="config 1 with the neurons' hooks transpiled and compiled at run time (TranspiledLIF)")
     ap.add_argument("--sim-steps", type=int, default=1000,
                     help="simulation steps per bench step (default 1000; small values for profiling runs)")
     args = ap.parse_args()
@@ -506,6 +550,11 @@ def main() -> int:
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.transpiled:
+        if args.config != 1 or world > 1:
+            raise SystemExit("--transpiled runs config 1 on one GPU")
+        print(json.dumps(run_transpiled(args, dev)))
+        return 0
     if args.config in (2, 3, 4):
         if world > 1:
             raise SystemExit(f"config {args.config} runs on one GPU")

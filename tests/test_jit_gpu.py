@@ -154,3 +154,14 @@ def test_event_driven_exact_times(cuda):
     assert rasters[1].sum() > 30
     frac = offsets[1][np.nonzero(rasters[1])]
     assert (np.abs(frac - 0.1) > 1e-4).mean() > 0.5  # most target spikes off the step grid
+
+
+def test_brunel_with_its_drive_in_the_hooks(cuda):
+    """Brunel's model A as TranspiledLIF (the built-in LIF's dynamics, its Poisson drive drawn in its update
+    hook): excitatory and inhibitory populations, recurrent delayed links, one uniform draw per neuron and step."""
+    from naer2_b200.networks import brunel
+
+    net, pops = brunel.build(NE=400, NI=100, CE=40, CI=10, delay="uniform", max_delay_steps=8, seed=3,
+                             transpiled=True)
+    r = check_against_interpreter(net, 120)
+    assert r[0].sum() > 200 and r[1].sum() > 50

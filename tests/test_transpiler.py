@@ -67,7 +67,9 @@ def _source_of(pop, incoming):
                     reason="nvcc not found")
 def test_generated_sources_compile_for_sm100a(tmp_path):
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
-    pops = [Izhikevich() * 40, DecayLIF() * 40, TwoPort() * 40]
+    from naer2_b200.networks.brunel import TranspiledLIF
+
+    pops = [Izhikevich() * 40, DecayLIF() * 40, TwoPort() * 40, TranspiledLIF(ext_rate=20.0, ext_weight=0.1) * 40]
     for k, p in enumerate(pops):
         incoming = []
         for port, hook in p.node.receive.items():
