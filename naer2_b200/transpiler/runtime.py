@@ -19,9 +19,9 @@ import torch
 
 from .. import _lib
 from ..topology import delay_steps, pull_form
-from .template import build_source, ctype_of, edge_hook_context, hook_context, params_type
+from .template import NPB_C, SCAN, build_source, ctype_of, edge_hook_context, hook_context, params_type
 
-BLOCK = 128
+BLOCK = 128  # exact-time intake: one thread per neuron
 _CACHE: dict = {}  # (source hash, device) -> n2b_jit_kernel handle, for the process's lifetime
 
 
@@ -207,9 +207,11 @@ class JitRuntime:
             n = step + k
             for kern, P, p in zip(self.kernels, self.params, self.pops):
                 P.step, P.t, P.t0 = n, (n + 1) * self.dt, n * self.dt
-                grid = (len(p.shape) + BLOCK - 1) // BLOCK
+                per = BLOCK if self.exact else NPB_C  # neurons per block (clocked: SCAN threads each)
+                grid = (len(p.shape) + per - 1) // per
                 if grid:
-                    _lib.check(lib.n2b_jit_launch(kern, grid, BLOCK, ctypes.byref(P), ctypes.sizeof(P), self._s),
+                    threads = BLOCK if self.exact else SCAN * NPB_C
+                    _lib.check(lib.n2b_jit_launch(kern, grid, threads, ctypes.byref(P), ctypes.sizeof(P), self._s),
                                "n2b_jit_launch")
                     self.launches += 1
         torch.cuda.current_stream(self.device).wait_stream(self.stream)

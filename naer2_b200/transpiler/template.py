@@ -1,10 +1,14 @@
 """The step-kernel template of a transpiled population (reference naer2/transpiler/templates/fused_template.py:
 85-371, the Gluon kernel it fills: pull -> deliver -> update/send -> emit).
 
-One thread per neuron, one launch per population per step n (time t = (n + 1) dt, the end of the step):
+One launch per population per step n (time t = (n + 1) dt, the end of the step); clocked intake: 32 neurons
+per block, SCAN threads per neuron (the neuron's first thread runs its hooks); exact-time intake: one thread
+per neuron.
   1. intake and receive: for each incoming connection (in the network's order), the neuron's pull row (its
      incoming links, canonical order within the row); a link whose source spiked at step n - d (the source
-     population's spike-bit ring) runs the connection's receive hook once, with its per-link edge values;
+     population's spike-bit ring) runs the connection's receive hook once, with its per-link edge values
+     (clocked: the SCAN threads list the arrivals of their row segments first, the hooks then run over the
+     lists in link order);
   2. update, then send (n2.spike() anywhere marks the neuron as firing at step n);
   3. a ballot word per warp into the population's spike-bit ring slot n mod depth (and the raster), the
      state back to memory, and the spike / arrival counters.
@@ -72,6 +76,142 @@ def _arrival_body(pop_name: str, c: int, inc: dict) -> str:
     return body
 
 
+SCAN = 8    # clocked intake: threads scanning one neuron's incoming row
+NPB_C = 32  # clocked intake: neurons per block (one spike-bit word), SCAN * NPB_C threads
+CAP = 16    # arrivals a scanner lists per connection and step (more: its segment is walked again)
+
+
+def _clocked_kernel(pop_name: str, attrs: dict, hooks: dict, incoming: list) -> str:
+    """The clocked step kernel: SCAN threads per neuron split each incoming row into SCAN contiguous segments
+    and list the arrivals of their segment in shared memory (link words and spike bits of many links in
+    flight); the neuron's first thread (the owner) then runs the hooks over the lists in segment order, i.e.
+    in link order, with the same arrival numbers and draws as one link at a time. A segment with more than CAP
+    arrivals is walked again by the owner, link by link."""
+    src = [f"constexpr int SCAN = {SCAN}, NPB_C = {NPB_C}, CAP = {CAP};\n\n"]
+    src.append(f'// population {pop_name}\nextern "C" __global__ void __launch_bounds__({SCAN * NPB_C}) '
+               "n2b_user_step(const __grid_constant__ Params p) {\n")
+    src.append("""    __shared__ u32 s_list[NPB_C * SCAN * CAP];
+    __shared__ int s_cnt[NPB_C * SCAN];
+    __shared__ u32 s_word, s_arrivals;
+    const int jl = threadIdx.x / SCAN, sc = threadIdx.x % SCAN;
+    const int j = blockIdx.x * NPB_C + jl;
+    const bool live = j < p.n, own = sc == 0;
+    const long long n = p.step;
+    const float t = p.t;
+    bool fired = false;
+    float spike_t = t;
+    u32 arrived = 0;
+    u32 link_k = 0xFFFFFFu;
+    if (threadIdx.x == 0) { s_word = 0u; s_arrivals = 0u; }
+""")
+    for a, py in attrs.items():
+        ct, _, _ = ctype_of(py)
+        src.append(f"    {ct} s_{a} = (live && own) ? p.s_{a}[j] : ({ct})0;\n")
+    src.append("    __syncthreads();\n")
+    for c, inc in enumerate(incoming):
+        if inc["receive"] is None and inc.get("forward") is None:
+            continue
+        body = ""
+        if inc.get("forward") is not None:
+            fn, ctx = inc["forward"]
+            body += lower_hook(fn, ctx, f"{pop_name} edge forward (connection {c})")
+        body += "".join(f"const float e_{h} = e_{real};\n" for h, real in inc.get("alias", {}).items())
+        if inc["receive"] is not None:
+            fn, ctx = inc["receive"]
+            body += lower_hook(fn, ctx, f"{pop_name} receive (connection {c})")
+        body += "".join(f"p.c{c}_e_{e}[l] = e_{e};\n" for e in inc.get("edge_written", ()))
+        body = "{\n" + body + "}\n"
+        loads = "".join(f"float e_{e} = p.c{c}_e_{e}[l];\n" for e in inc["edge_dynamic"])
+        arrival = loads + "link_k = arrived++;\n" + body
+        hit = (f"(p.c{c}_src_bits[(size_t)(m & p.c{c}_src_mask) * p.c{c}_src_words + (src >> 5)] >> (src & 31)) & 1u")
+        src.append(f"""    {{  // connection {c}: scan
+        const int r0 = live ? p.c{c}_ptr[j] : 0, r1 = live ? p.c{c}_ptr[j + 1] : 0;
+        const int seg = (r1 - r0 + SCAN - 1) / SCAN;
+        const int a = min(r1, r0 + sc * seg), b = min(r1, a + seg);
+        int cnt = 0;
+        for (int l = a; l < b; ++l) {{
+            const u32 w = p.c{c}_link[l];
+            const int src = (int)(w & 0xFFFFFFu), d = (int)(w >> 24);
+            if (d < 1 || d > p.c{c}_src_mask) {{ atomicAdd(p.err, 1); continue; }}
+            const long long m = n - d;
+            if (m < 0 || !({hit})) continue;
+            if (cnt < CAP) s_list[(jl * SCAN + sc) * CAP + cnt] = (u32)l;
+            ++cnt;
+        }}
+        s_cnt[jl * SCAN + sc] = cnt;
+        __syncthreads();
+        if (live && own) {{  // the hooks, in link order
+            for (int s = 0; s < SCAN; ++s) {{
+                const int cs = s_cnt[jl * SCAN + s];
+                if (cs <= CAP) {{
+                    for (int i = 0; i < cs; ++i) {{
+                        const int l = (int)s_list[(jl * SCAN + s) * CAP + i];
+""")
+        src.append("                        " + arrival.replace("\n", "\n                        ").rstrip() + "\n")
+        src.append(f"""                    }}
+                }} else {{  // the segment again, one link at a time
+                    const int as = min(r1, r0 + s * seg), bs = min(r1, as + seg);
+                    for (int l = as; l < bs; ++l) {{
+                        const u32 w = p.c{c}_link[l];
+                        const int src = (int)(w & 0xFFFFFFu), d = (int)(w >> 24);
+                        if (d < 1 || d > p.c{c}_src_mask) continue;
+                        const long long m = n - d;
+                        if (m < 0 || !({hit})) continue;
+""")
+        src.append("                        " + arrival.replace("\n", "\n                        ").rstrip() + "\n")
+        src.append("""                    }
+                }
+            }
+        }
+        link_k = 0xFFFFFFu;
+        __syncthreads();  // the lists are rewritten by the next connection
+    }
+""")
+    src.append("    if (live && own) {\n")
+    for name in ("update", "send"):
+        fn, ctx = hooks[name]
+        body = lower_hook(fn, ctx, f"{pop_name} {name}")
+        src.append("        " + body.replace("\n", "\n        ").rstrip() + "\n")
+    backward = [(c, inc) for c, inc in enumerate(incoming) if inc.get("backward") is not None]
+    if backward:  # the neuron fired: every incoming link's edge backward hook at its spike's time
+        src.append("        if (fired) {\n            const float t = spike_t;\n")
+        for c, inc in backward:
+            fn, ctx = inc["backward"]
+            body = lower_hook(fn, ctx, f"{pop_name} edge backward (connection {c})")
+            body += "".join(f"p.c{c}_e_{e}[l] = e_{e};\n" for e in inc.get("edge_written", ()))
+            loads = "".join(f"                float e_{e} = p.c{c}_e_{e}[l];\n" for e in inc["edge_dynamic"])
+            src.append(f"            for (int l = p.c{c}_ptr[j]; l < p.c{c}_ptr[j + 1]; ++l) {{\n{loads}")
+            src.append("                " + body.replace("\n", "\n                ").rstrip() + "\n")
+            src.append("            }\n")
+        src.append("        }\n")
+    src.append("""        if (fired) {
+            const float o = spike_t - p.t0;  // the spike's time within its step
+            p.off[(size_t)(n & p.bit_mask) * p.n + j] = o;
+            const long long r = n - p.rec0;
+            if (p.raster_off && r >= 0 && r < p.raster_steps) p.raster_off[(size_t)r * p.n + j] = o;
+            atomicOr(&s_word, 1u << jl);
+        }
+        if (arrived) atomicAdd(&s_arrivals, arrived);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {  // the block's 32 neurons: one spike-bit word
+        const u32 b = s_word;
+        const int word = blockIdx.x;
+        if (word < p.words) {
+            p.bits[(size_t)(n & p.bit_mask) * p.words + word] = b;
+            const long long r = n - p.rec0;
+            if (p.raster && r >= 0 && r < p.raster_steps) p.raster[(size_t)r * p.words + word] = b;
+        }
+        if (b) atomicAdd(p.counters + 1, (u64)__popc(b));
+        if (s_arrivals) atomicAdd(p.counters, (u64)s_arrivals);
+    }
+""")
+    for a in attrs:
+        src.append(f"    if (live && own) p.s_{a}[j] = s_{a};\n")
+    src.append("}\n")
+    return "".join(src)
+
+
 def build_source(pop_name: str, attrs: dict, hooks: dict, incoming: list, exact: bool = False) -> tuple[str, list]:
     """(CUDA source, params fields [(name, C type, ctypes type)]) of one population.
 
@@ -118,6 +258,9 @@ __device__ __forceinline__ float n2_uniform(const Params &p, int j, long long n,
 }
 
 ''')
+    if not exact:
+        src.append(_clocked_kernel(pop_name, attrs, hooks, incoming))
+        return "".join(src), fields
     src.append(f'// population {pop_name}\nextern "C" __global__ void __launch_bounds__(128) n2b_user_step('
                "const __grid_constant__ Params p) {\n")
     src.append("    const int j = blockIdx.x * blockDim.x + threadIdx.x;\n")
