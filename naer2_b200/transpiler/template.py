@@ -10,8 +10,9 @@ per neuron.
      (clocked: the SCAN threads list the arrivals of their row segments first, the hooks then run over the
      lists in link order);
   2. update, then send (n2.spike() anywhere marks the neuron as firing at step n);
-  3. a ballot word per warp into the population's spike-bit ring slot n mod depth (and the raster), the
-     state back to memory, and the spike / arrival counters.
+  3. the spike-bit word of 32 neurons (clocked: one per block; exact-time: a ballot per warp) into the
+     population's spike-bit ring slot n mod depth (and the raster), the state back to memory, and the spike /
+     arrival counters.
 The source is self-contained (NVRTC compiles it with no includes); its one parameter is the `Params` block,
 mirrored field by field by the ctypes structure `params_type` builds, so that the host fills it directly.
 """
