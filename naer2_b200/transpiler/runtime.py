@@ -19,7 +19,7 @@ import torch
 
 from .. import _lib
 from ..topology import delay_steps, pull_form
-from .template import NPB_C, SCAN, build_source, ctype_of, edge_hook_context, hook_context, params_type
+from .template import NPB_C, build_source, ctype_of, edge_hook_context, hook_context, params_type, scan
 
 BLOCK = 128  # exact-time intake: one thread per neuron
 _CACHE: dict = {}  # (source hash, device) -> n2b_jit_kernel handle, for the process's lifetime
@@ -148,7 +148,7 @@ class JitRuntime:
             hooks = {"update": (node.update.ast, hook_context(p, node.update, site_base=site)),
                      "send": (node.send.ast, hook_context(p, node.send, site_base=site + 32))}
             src, fields = build_source(type(p.instance).__name__, dict(p.dynamic_attrs), hooks, incoming,
-                                       exact=self.exact)
+                                       exact=self.exact, n=len(p.shape))
             self.sources.append(src)
             self.kernels.append(compile_source(src, dindex))
             P = params_type(fields)()
@@ -210,7 +210,7 @@ class JitRuntime:
                 per = BLOCK if self.exact else NPB_C  # neurons per block (clocked: SCAN threads each)
                 grid = (len(p.shape) + per - 1) // per
                 if grid:
-                    threads = BLOCK if self.exact else SCAN * NPB_C
+                    threads = BLOCK if self.exact else scan(len(p.shape)) * NPB_C
                     _lib.check(lib.n2b_jit_launch(kern, grid, threads, ctypes.byref(P), ctypes.sizeof(P), self._s),
                                "n2b_jit_launch")
                     self.launches += 1

@@ -2,7 +2,7 @@
 85-371, the Gluon kernel it fills: pull -> deliver -> update/send -> emit).
 
 One launch per population per step n (time t = (n + 1) dt, the end of the step); clocked intake: 32 neurons
-per block, SCAN threads per neuron (the neuron's first thread runs its hooks); exact-time intake: one thread
+per block, scan(n) threads per neuron (the neuron's first thread runs its hooks); exact-time intake: one thread
 per neuron.
   1. intake and receive: for each incoming connection (in the network's order), the neuron's pull row (its
      incoming links, canonical order within the row); a link whose source spiked at step n - d (the source
@@ -77,17 +77,24 @@ def _arrival_body(pop_name: str, c: int, inc: dict) -> str:
     return body
 
 
-SCAN = 8    # clocked intake: threads scanning one neuron's incoming row
-NPB_C = 32  # clocked intake: neurons per block (one spike-bit word), SCAN * NPB_C threads
-CAP = 16    # arrivals a scanner lists per connection and step (more: its segment is walked again)
+NPB_C = 32  # clocked intake: neurons per block (one spike-bit word), scan(n) * NPB_C threads
+LIST_WORDS = 4096  # clocked intake: the block's arrival lists (u32), SCAN * CAP per neuron
 
 
-def _clocked_kernel(pop_name: str, attrs: dict, hooks: dict, incoming: list) -> str:
+def scan(n: int) -> int:
+    """Clocked intake: threads scanning one neuron's incoming row, for a population of n neurons (more for small
+    populations, so that their blocks still fill the GPU)."""
+    return 32 if n <= 4096 else 8
+
+
+def _clocked_kernel(pop_name: str, attrs: dict, hooks: dict, incoming: list, n: int) -> str:
     """The clocked step kernel: SCAN threads per neuron split each incoming row into SCAN contiguous segments
     and list the arrivals of their segment in shared memory (link words and spike bits of many links in
     flight); the neuron's first thread (the owner) then runs the hooks over the lists in segment order, i.e.
     in link order, with the same arrival numbers and draws as one link at a time. A segment with more than CAP
-    arrivals is walked again by the owner, link by link."""
+    arrivals is walked again by the owner, link by link. SCAN = scan(n), CAP = LIST_WORDS / (NPB_C * SCAN)."""
+    SCAN = scan(n)
+    CAP = LIST_WORDS // (NPB_C * SCAN)
     src = [f"constexpr int SCAN = {SCAN}, NPB_C = {NPB_C}, CAP = {CAP};\n\n"]
     src.append(f'// population {pop_name}\nextern "C" __global__ void __launch_bounds__({SCAN * NPB_C}) '
                "n2b_user_step(const __grid_constant__ Params p) {\n")
@@ -213,7 +220,8 @@ def _clocked_kernel(pop_name: str, attrs: dict, hooks: dict, incoming: list) -> 
     return "".join(src)
 
 
-def build_source(pop_name: str, attrs: dict, hooks: dict, incoming: list, exact: bool = False) -> tuple[str, list]:
+def build_source(pop_name: str, attrs: dict, hooks: dict, incoming: list, exact: bool = False,
+                 n: int = 1 << 30) -> tuple[str, list]:
     """(CUDA source, params fields [(name, C type, ctypes type)]) of one population.
 
     attrs: dynamic attr -> python type; hooks: {"update": (fn_ast, ctx), "send": (fn_ast, ctx)};
@@ -221,6 +229,8 @@ def build_source(pop_name: str, attrs: dict, hooks: dict, incoming: list, exact:
     arrays by the edge's own attribute names; "edge_written": those the edge hooks assign (stored back);
     "alias": {receive-facing name: edge name} where they differ; "forward" / "backward": (fn_ast, ctx) of the
     edge hooks or None.
+
+    n: the population's size (the clocked intake's threads per neuron, `scan(n)`).
 
     exact: event-driven intake at exact times. Every spike carries its time (its offset in its step, in the
     population's offset ring); a link of delay d delivers it at that time plus d steps. A neuron collects its
@@ -260,7 +270,7 @@ __device__ __forceinline__ float n2_uniform(const Params &p, int j, long long n,
 
 ''')
     if not exact:
-        src.append(_clocked_kernel(pop_name, attrs, hooks, incoming))
+        src.append(_clocked_kernel(pop_name, attrs, hooks, incoming, n))
         return "".join(src), fields
     src.append(f'// population {pop_name}\nextern "C" __global__ void __launch_bounds__(128) n2b_user_step('
                "const __grid_constant__ Params p) {\n")
