@@ -228,7 +228,10 @@ int n2b_bptt_forward(const n2b_bptt_desc *d, const float *u, const float *w_rec,
                      float *m, int32_t *tstar, void *workspace, size_t workspace_bytes, void *stream);
 
 /* Backward of the last taped forward: dm [B][R] = dL/dm, tstar as the forward
- * wrote it; writes du [T][B][H] = dL/du, dw_rec [nnz], dw_out [H][R]. */
+ * wrote it; writes du [T][B][H] = dL/du, dw_rec [nnz], dw_out [H][R]. The work
+ * runs on two streams of the library's own (made on a device's first call,
+ * kept): it starts after the work already on `stream`, and `stream` waits for
+ * its end, so the results are ordered on `stream` as if it ran there. */
 int n2b_bptt_backward(const n2b_bptt_desc *d, const float *u, const float *w_rec, const float *w_out,
                       const float *dm, const int32_t *tstar, float *du, float *dw_rec, float *dw_out,
                       void *workspace, size_t workspace_bytes, void *stream);
