@@ -2,6 +2,7 @@
 compiled by nvcc for sm_100a, and the DSL interpreter that checks the compiled kernels on the GPU."""
 
 import ast
+import math
 import shutil
 import subprocess
 
@@ -119,3 +120,39 @@ def test_edge_hooks_lower_and_refuse_the_source():
     ctx = HookContext(time_name="time", source_name="src", roots={}, random=False)
     with pytest.raises(NotImplementedError, match="sending neuron"):
         lower_hook(bad, ctx, "fwd")
+
+
+def test_clocked_kernel_geometry_by_population_size():
+    """The clocked intake's threads per neuron (scan(n)): 32 for populations of at most 4,096 neurons, else 8;
+    the block (32 neurons) stays within 1,024 threads and the arrival lists within LIST_WORDS, as the generated
+    source states them."""
+    from naer2_b200.transpiler.template import LIST_WORDS, NPB_C, scan
+
+    for n, want in ((1, 32), (4096, 32), (4097, 8), (10000, 8)):
+        assert scan(n) == want
+        pop = DecayLIF() * 8
+        node = pop.node
+        hooks = {"update": (node.update.ast, hook_context(pop, node.update)),
+                 "send": (node.send.ast, hook_context(pop, node.send))}
+        inc = [{"receive": (node.receive["receive"].ast, hook_context(pop, node.receive["receive"], ["weight"], {})),
+                "edge_dynamic": ["weight"]}]
+        src, _ = build_source("DecayLIF", dict(pop.dynamic_attrs), hooks, inc, exact=False, n=n)
+        cap = LIST_WORDS // (NPB_C * want)
+        assert f"__launch_bounds__({want * NPB_C})" in src and want * NPB_C <= 1024
+        assert f"constexpr int SCAN = {want}, NPB_C = {NPB_C}, CAP = {cap};" in src and cap >= 4
+
+
+def test_transpiled_lif_thresholds_are_the_poisson_cdf():
+    """TranspiledLIF counts external events by comparing one uniform with P(count <= k), k < 12: the counts of
+    many uniforms have the Poisson mean and variance of ext_rate dt."""
+    from naer2_b200.networks.brunel import POISSON_TERMS, TranspiledLIF
+
+    m = TranspiledLIF(ext_rate=20.0, ext_weight=0.1, dt=0.1)
+    c = np.array([getattr(m, f"c{k}") for k in range(POISSON_TERMS)])
+    lam = 2.0
+    k = np.arange(POISSON_TERMS)
+    cdf = np.cumsum(np.exp(-lam) * lam ** k / np.array([math.factorial(int(i)) for i in k]))
+    np.testing.assert_allclose(c, cdf, rtol=1e-6)
+    u = np.random.default_rng(1).random(400_000)
+    counts = (u[:, None] > c[None, :]).sum(1)
+    assert abs(counts.mean() - lam) < 0.01 and abs(counts.var() - lam) < 0.02
