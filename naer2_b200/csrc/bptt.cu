@@ -137,12 +137,6 @@ __host__ __device__ inline BwdSmem bwd_smem(int H, int HC, int R, int out_cta_ma
     return L;
 }
 
-// The two halves of a cluster barrier (every thread of every CTA of the cluster, the same number of times):
-// arrive orders this thread's earlier memory accesses (release), wait returns once every thread has arrived
-// and makes their earlier writes visible (acquire).
-__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
-__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
-
 // One CTA's arrival at a group step (thread 0, after a __syncthreads that follows the CTA's writes): a release
 // add on the group's counter; later (other work in between), a bounded acquire spin until `target` arrivals
 // (every CTA of the group at this step). A wait that gives up counts in err[3] and sets `aborted`, after which
