@@ -1,4 +1,4 @@
-"""Many independent Brunel networks of uneven size and parameters, stepped together:
+"""Many independent Brunel networks of uneven size and parameters, stepped together (the batched workload):
 instance b draws N_E log-uniform in [1,000, 20,000], N_I = N_E / 4, C_E = min(0.1 N_E, 1,000), C_I = C_E / 4,
 g uniform in [3, 6], eta uniform in [0.9, 4], per-link delays uniform in 1-20 steps, its own seed. All
 instances joined in one Network run as one persistent launch per window (each instance's populations are

@@ -1,6 +1,6 @@
 """The layered cortical microcircuit of Potjans & Diesmann (2014) at a fixed dt: 8 populations (E/I of layers
 2/3, 4, 5, 6) of PD14 LIF neurons with exponential current synapses, the reference's model
-(test/networks/PD14/net.py, neuron.py, connection.py) with the changes BASELINE's config 2 asks for: an
+(test/networks/PD14/net.py, neuron.py, connection.py) with the changes of the full-size PD14 workload: an
 explicit Poisson background of 8 Hz x K_bg events of weight J_E into every neuron (instead of the DC shift),
 the connection matrix given target rows x source columns, inhibitory delays 0.8 +- 0.4 ms, every delay
 clipped to >= dt and rounded to steps.
