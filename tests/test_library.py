@@ -118,3 +118,26 @@ def test_null_handle_is_an_error_not_a_crash():
     assert lib.n2b_step(None, 1, None) == -1
     assert lib.n2b_replay(None, 1, None) == -1
     assert lib.n2b_destroy(None) == 0
+
+
+def test_projection_and_bptt_entry_points_reject_bad_arguments():
+    """Host-side checks of n2b_project_* and n2b_bptt_workspace_bytes, made before any device work (the
+    pointers here are never dereferenced)."""
+    lib = _lib.load()
+    P = 0x1000
+    err = lambda: lib.n2b_last_error().decode()  # noqa: E731
+    assert lib.n2b_project_forward(P, P, 10, 5, 6, P, P, None) == -1 and "hidden" in err()
+    assert lib.n2b_project_forward(P, P, -1, 5, 8, P, P, None) == -1 and "rows" in err()
+    assert lib.n2b_project_forward(None, P, 10, 5, 8, P, P, None) == -1 and "missing" in err()
+    assert lib.n2b_project_forward(P, P, 10, 5, 8, 0x1004, P, None) == -1 and "aligned" in err()
+    assert lib.n2b_project_forward(None, None, 0, 5, 8, None, None, None) == 0  # nothing to do
+    assert lib.n2b_project_backward(P, 3, P, P, 5, 10, 2000, P, P, P, None) == -1 and "hidden" in err()
+    assert lib.n2b_project_backward(P, 3, None, P, 5, 10, 8, P, P, P, None) == -1 and "missing" in err()
+    d = _lib.BpttDesc(batch=12, steps=10, hidden=64, readouts=4, checkpoint=5)
+    d.in_ptr = d.out_grp = P
+    n = ctypes.c_size_t()
+    assert lib.n2b_bptt_workspace_bytes(ctypes.byref(d), ctypes.byref(n)) == -1 and "multiple of 8" in err()
+    d.batch, d.hidden = 16, 2048
+    assert lib.n2b_bptt_workspace_bytes(ctypes.byref(d), ctypes.byref(n)) == -1 and "hidden" in err()
+    d.hidden = 64
+    assert lib.n2b_bptt_workspace_bytes(ctypes.byref(d), ctypes.byref(n)) == 0 and n.value > 0
