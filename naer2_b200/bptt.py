@@ -1,8 +1,9 @@
 """A recurrent LIF layer trained by surrogate-gradient BPTT, on the library's forward and adjoint kernels.
 
-The layer: input spikes x [T, B, C] -> input current U = x @ w_in (`n2b_project_forward` over the input's spike
-events, `SpikeEvents`; its gradient to w_in by `n2b_project_backward`) -> H recurrent LIF neurons with sparse delayed recurrence (w_rec, delays 1..5 steps) -> R leaky
-non-spiking readouts; the output is the max over time of each readout, m [B, R], for a cross-entropy loss.
+The layer: input spikes x [T, B, C] -> input current U = x @ w_in (`n2b_project_forward` over the input's
+spike events, `SpikeEvents`; its gradient to w_in by `n2b_project_backward`) -> H recurrent LIF neurons with
+sparse delayed recurrence (w_rec, delays 1..5 steps) -> R leaky non-spiking readouts; the output is the max
+over time of each readout, m [B, R], for a cross-entropy loss.
 The recurrence and its adjoint run in `n2b_bptt_forward` / `n2b_bptt_backward` (naer2_b200/csrc/bptt.cu)
 behind `torch.autograd.Function`: the forward keeps the spikes of every step (one bit per neuron, sample and
 step) and the membrane every `checkpoint` steps; the backward recomputes each segment from its checkpoint and
