@@ -1,31 +1,32 @@
-"""Benchmark: synaptic events/s of Brunel's model A at config 1's size
-(N_E 10,000, N_I 2,500, C_E 1,000, C_I 250: 15.6M synapses, per-link delays
-of 1-20 steps, dt 0.1 ms), stepped by the fused CUDA step kernel.
+"""Benchmark: synaptic events/s of the fixed-dt hot path on one B200, headline workload the PD14 cortical
+microcircuit at full size (77,169 neurons, ~3e8 synapses, per-link normal delays, dt 0.1 ms).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl naer2_b200|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl naer2_b200|reference] [--config 1|2|3|4]
 
-One bench step = 1,000 simulation steps (100 ms of network time); the
-config's 10,000 steps are 10 bench steps (the default K). Printed: one JSON
-line (rank 0).
-  value   events delivered in the timed steps / device time (CUDA events on
-          the runtime's stream, L2 flushed before every timed step), summed
-          over ranks, time the max over ranks
-  e2e     the same metric through the public API with host buffers: every
-          step copies the network state in from pinned host memory, runs
-          Network.step, and reads the spike raster and state back
-  roofline  the step kernel's algorithmic bytes (9 B per synaptic event +
-          16 B per neuron per step) over its average launch time, against the
-          measured HBM copy bandwidth
-  cpu_baseline  the oracle (a C restatement of the reference's time-driven
-          loop, all host threads) on a bounded sample of the same network
---impl reference times that CPU implementation alone (rank 0; others exit).
-Multi-GPU: independent replicas (one network per rank, its own seed).
+One bench step = 1,000 simulation steps (100 ms of network time) stepped by the persistent step kernel (one
+cooperative launch per window of --window steps, replayed from a CUDA graph). Printed: one JSON line (rank 0).
+  value     events delivered in the timed steps / device time (CUDA events on the runtime's stream, L2 flushed
+            before every timed step), summed over ranks, time the max over ranks
+  e2e       the same metric through the public API with host buffers: every step copies the network state in
+            from pinned host memory, runs Network.step, and reads the spike raster and state back
+  roofline  the step kernel's algorithmic bytes (9 B per synaptic event + 32 B per PD14 neuron per simulation
+            step) per launch over its average launch time, against the measured HBM copy bandwidth; traffic:
+            the DRAM bytes of one launch of the same window from the committed ncu capture
+  cpu_baseline  the oracle (a C restatement of the reference's time-driven loop, all host threads) on a bounded
+            sample of the same network
+  workloads  at N=1 the other workloads, each measured the same way: Brunel's network at config 1's size,
+            the 64 batched uneven instances against the same instances one network at a time (autotuned),
+            and BPTT's training step against the plain forward
+--impl reference times the CPU implementation (the oracle port, all host threads) on the same workload and the
+same window of simulation steps (rank 0; other ranks exit). --config 1|3|4 prints one of the other workloads
+as the line instead. Multi-GPU: independent replicas (one network per rank, its own seed).
 """
 
 from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import pathlib
 import subprocess
@@ -37,11 +38,10 @@ sys.path.insert(0, str(ROOT))
 
 SIM_STEPS_PER_STEP = 1000
 BYTES_PER_EVENT = 9  # int32 target + int8 delay + fp32 weight
-BYTES_PER_NEURON_STEP = 16  # V read + write, arrival slot read + clear
+NEURON_BYTES = {"brunel": 16, "pd14": 32}  # per neuron and step: V (and I, refractory) read + write, slot read + clear
 METRIC = "synaptic events/s"
 UNIT = "events/s"
-WORKLOAD = "brunel_A_config1"
-MODE = "persistent"
+KERNEL = "n2b::persistent_kernel<256>"
 
 
 def measured_peaks() -> tuple[float, str]:
@@ -105,12 +105,6 @@ def l2_atomics(events_per_s: float, dev) -> dict | None:
             "peak_probe": pk["probe"]}
 
 
-def config(n_gpus: int) -> dict:
-    return {"workload": WORKLOAD, "neurons": 12500, "synapses": 15_625_000, "delays_steps": "U{1..20}", "dt_ms": 0.1,
-            "sim_steps_per_step": SIM_STEPS_PER_STEP, "l2": "flushed before every timed step (256 MiB write)",
-            "parallelism": f"replicas x{n_gpus}" if n_gpus > 1 else "single GPU", "launch": MODE}
-
-
 class Clocks:
     """nvidia-smi samples (200 ms) while the timed region runs."""
 
@@ -129,6 +123,7 @@ class Clocks:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+        time.sleep(0.3)  # the first sample lands inside the timed region
         return self
 
     def __exit__(self, *exc):
@@ -178,184 +173,233 @@ def reduce_over_ranks(times, counts, world: int, device):
     return [*t.tolist(), *c.tolist()]
 
 
-def cpu_sample(desc, states, target_s: float = 12.0, threads: int = 0) -> dict:
-    """The oracle on the host cores: a bounded sample of the same network (first steps from the same state)."""
+# ---------------------------------------------------------------------------------------------------- workloads
+
+def build_workload(name: str, seed: int, device=None):
+    """(network, populations list, neuron bytes per step, config dict) of a plain workload."""
+    if name == "pd14_config2":
+        from naer2_b200.networks import pd14
+
+        net, pops = pd14.build(scale=1.0, seed=seed, device=device)
+        cfg = {"workload": name, "neurons": sum(len(p.shape) for p in pops), "populations": 8,
+               "synapses_expected": pd14.expected_synapses(1.0), "delays": "normal per link, >= dt, in steps",
+               "dt_ms": 0.1}
+        return net, pops, NEURON_BYTES["pd14"], cfg
+    if name == "brunel_A_config1":
+        from naer2_b200.networks import brunel
+
+        net, pops = brunel.build(**brunel.CONFIG1, seed=seed, device=device)
+        cfg = {"workload": name, "neurons": 12500, "synapses": 15_625_000, "delays_steps": "U{1..20}", "dt_ms": 0.1}
+        return net, list(pops.values()), NEURON_BYTES["brunel"], cfg
+    raise ValueError(name)
+
+
+def workload_profile(name: str) -> dict | None:
+    """The committed ncu capture of the workload's step kernel (DRAM bytes of one launch), if any."""
+    p = ROOT / "profiles" / f"persistent_kernel_{name}.json"
+    return json.loads(p.read_text()) if p.exists() else None
+
+
+def state_tensors(net):
+    """(population, attribute) of every state tensor the kernels step."""
+    from naer2_b200.models import params_of
+
+    out = []
+    for p in net.populations:
+        for attr in params_of(p, net.resolution)["state"].values():
+            out.append((p, attr))
+    return out
+
+
+def measure(net, args, dev, world: int, sim: int, clocks: bool = True) -> dict:
+    """Warm-up, the timed region (device time of K bench steps, L2 flushed before each) and the end-to-end pass
+    through the public API with host buffers. Per rank; the caller reduces over ranks."""
+    import torch
+    import torch.distributed as dist
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    net.window = sim  # one persistent launch per bench step
+    net.record(sim)
+    rt = net.runtime
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(args.warmup):
+        net.run_steps(sim)
+    barrier()
+    ev0 = rt.counters()["events"]
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clk = Clocks(dev.index or 0) if clocks else None
+    if clk:
+        clk.__enter__()
+    try:
+        barrier()
+        for k in range(args.steps):
+            flush.zero_()
+            rt._enter()  # the runtime's stream after the flush
+            starts[k].record(rt.stream)
+            net.run_steps(sim)
+            ends[k].record(rt.stream)
+        barrier()
+    finally:
+        if clk:
+            clk.__exit__(None, None, None)
+    per_launch_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    dev_ms = sum(per_launch_ms)
+    events = rt.counters()["events"] - ev0
+    net.check()
+
+    # end to end through the public API, host buffers
+    hosts = []
+    for p, attr in state_tensors(net):
+        t = p.state_tensor(attr)
+        h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+        h.copy_(t)
+        hosts.append((p, attr, h))
+    raster_host = [torch.empty(r.shape, dtype=r.dtype, pin_memory=True) for r in rt.rasters if r is not None]
+    h2d = sum(h.numel() * h.element_size() for _, _, h in hosts)
+    d2h = h2d + sum(r.numel() * r.element_size() for r in raster_host)
+    barrier()
+    ev1 = rt.counters()["events"]
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for p, attr, h in hosts:  # inputs: the network state, from pinned host memory
+            p.state_tensor(attr).copy_(h, non_blocking=True)
+        net.record(sim)
+        net.step(sim * net.resolution)
+        for r, h in zip([r for r in rt.rasters if r is not None], raster_host):  # results: raster and state
+            h.copy_(r, non_blocking=True)
+        for p, attr, h in hosts:
+            h.copy_(p.state_tensor(attr), non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_events = rt.counters()["events"] - ev1
+    net.check()
+    windows = args.steps * math.ceil(sim / max(net.window, 1))
+    return {"dev_ms": dev_ms, "events": events, "e2e_s": e2e_s, "e2e_events": e2e_events, "h2d": h2d, "d2h": d2h,
+            "clocks": clk.summary() if clk else None, "launches": 2 * windows, "windows": windows,
+            "per_launch_ms": per_launch_ms, "n_links": rt.n_links, "grid": rt.opt.grid}
+
+
+def roofline(events: float, steps: int, neurons: int, neuron_bytes: int, dev_ms: float, windows: int,
+             profile: dict | None) -> dict:
+    """Algorithmic bytes per launch (one window of simulation steps) over the average launch time."""
+    ev_step = events / steps
+    per_step = ev_step * BYTES_PER_EVENT + neurons * neuron_bytes
+    steps_per_launch = steps / windows
+    launch_bytes = per_step * steps_per_launch
+    launch_s = dev_ms / 1e3 / windows
+    achieved = launch_bytes / launch_s / 1e9
+    peak, kind = measured_peaks()
+    traffic = None
+    if profile is not None and profile.get("steps_per_launch"):
+        traffic = profile["dram_bytes_per_launch"] * steps_per_launch / profile["steps_per_launch"]
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "peak_kind": kind, "kernel": KERNEL, "bytes_per_launch": launch_bytes,
+            "us_per_launch": launch_s * 1e6, "steps_per_launch": steps_per_launch,
+            "us_per_sim_step": launch_s * 1e6 / steps_per_launch,
+            "per_unit": f"{BYTES_PER_EVENT} B per synaptic event + {neuron_bytes} B per neuron per step",
+            "traffic_source": profile.get("source") if profile else None}
+
+
+def cpu_sample(prepared, states, dt: float, name: str, target_s: float = 12.0) -> dict:
+    """The oracle on all host cores: a bounded sample of the same network, from its initial state."""
     import oracle
 
-    used = oracle.set_threads(threads)
-    probe = 50
+    used = oracle.set_threads(0)
+    probe = 20
     t0 = time.perf_counter()
-    _, ev = oracle.run(desc, states, 0, probe, record=False)
+    _, ev = oracle.run(prepared, states, 0, probe, record=False)
     t_probe = time.perf_counter() - t0
-    steps = max(50, min(400_000, int(probe * target_s / max(t_probe, 1e-3))))
+    steps = max(20, min(400_000, int(probe * target_s / max(t_probe, 1e-3))))
     t0 = time.perf_counter()
-    _, ev2 = oracle.run(desc, states, probe, steps, record=False)
+    _, ev2 = oracle.run(prepared, states, probe, steps, record=False)
     el = time.perf_counter() - t0
     return {"value": ev2 / el, "unit": UNIT, "cores": used, "kind": "port",
-            "sample": f"{WORKLOAD}: simulation steps {probe}-{probe + steps} ({steps * 0.1:.0f} ms of network time, "
+            "sample": f"{name}: simulation steps {probe}-{probe + steps} ({steps * dt:.0f} ms of network time, "
                       f"{ev2} events) in {el:.1f} s, C oracle, {used} OpenMP threads, nproc {os.cpu_count()}",
-            "realtime_factor": el / (steps * 1e-4)}
+            "realtime_factor": el / (steps * dt * 1e-3)}
 
 
-def run_reference(args) -> None:
-    """The reference arm: the CPU implementation (the oracle port, all host threads) on the same workload."""
-    import oracle
-    from naer2_b200.networks import brunel
+def line_of(name: str, m: dict, args, world: int, sim: int, neurons: int, neuron_bytes: int, cfg: dict,
+            dev=None) -> dict:
+    steps = args.steps * sim
+    value = m["events"] / (m["dev_ms"] / 1e3)
+    rl = roofline(m["events_rank0"], steps, neurons, neuron_bytes, m["dev_ms_rank0"], m["windows"],
+                  workload_profile(name))
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": m["dev_ms"] / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (seeded draws: connectivity, weights, delays, initial state, Philox Poisson drive)",
+           "config": {**cfg, "sim_steps_per_step": sim, "window_steps": sim,
+                      "l2": "flushed before every timed step (256 MiB write)",
+                      "parallelism": f"replicas x{world}" if world > 1 else "single GPU", "launch": "persistent"},
+           "realtime_factor": (m["dev_ms"] / 1e3) / (steps * 1e-4),
+           "e2e": {"value": m["e2e_events"] / m["e2e_s"], "unit": UNIT, "h2d_bytes_per_step": m["h2d"],
+                   "d2h_bytes_per_step": m["d2h"]},
+           "roofline": rl,
+           "gpu_launches": m["launches"],
+           "clocks": m["clocks"],
+           "events_per_sim_step": m["events_rank0"] / steps,
+           "synapses": m["n_links"], "grid": m["grid"]}
+    if dev is not None:
+        out["l2_atomics"] = l2_atomics(m["events_rank0"] / (m["dev_ms_rank0"] / 1e3), dev)
+    return out
+
+
+def run_plain(name: str, args, dev, rank: int, world: int, cpu: bool) -> dict:
+    """A plain workload (PD14 or config 1) on every rank, reduced over ranks; rank 0 gets the line."""
+    import torch
+
     from naer2_b200.runtime import describe
+    from naer2_b200.stats import SpikeStats
 
-    net, _ = brunel.build(**brunel.CONFIG1, seed=1)
-    desc = describe(net)
-    states = oracle.states_of(net, desc)
-    used = oracle.set_threads(0)
-    per_step = 100  # simulation steps per bench step: a bounded sample of the 1,000 of ours
-    n = 0
-    for _ in range(args.warmup):
-        oracle.run(desc, states, n, per_step, record=False)
-        n += per_step
+    sim = SIM_STEPS_PER_STEP
     t0 = time.perf_counter()
-    events = 0
-    for _ in range(args.steps):
-        _, ev = oracle.run(desc, states, n, per_step, record=False)
-        events += ev
-        n += per_step
-    el = time.perf_counter() - t0
-    value = events / el
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox network)",
-            "config": {**config(1), "sim_steps_per_step": per_step}, "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "port",
-                             "sample": f"{args.steps} x {per_step} simulation steps of {WORKLOAD} after "
-                                       f"{args.warmup} x {per_step} warm-up, C oracle, {used} OpenMP threads"},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "realtime_factor": el / (args.steps * per_step * 1e-4)}
-    print(json.dumps(line))
+    net, pops, nb, cfg = build_workload(name, 1 + rank, device=dev)
+    neurons = sum(len(p.shape) for p in pops)
+    prepared = states = None
+    if cpu and rank == 0 and world == 1:
+        import oracle
 
-
-def run_transpiled(args, dev) -> dict:
-    """Config 1's network with TranspiledLIF neurons (the built-in LIF's dynamics, its Poisson drive drawn in its
-    own hook): the run-time compiled step kernels, launched from the host once per population and step (no
-    persistent window, no graph), events/s over the timed steps."""
-    import torch
-
-    from naer2_b200.networks import brunel
-
-    t0 = time.perf_counter()
-    net, pops = brunel.build(**brunel.CONFIG1, seed=1, device=dev, transpiled=True)
-    net.run_steps(1)  # builds the runtime: transpiles and compiles the hooks
-    rt = net.runtime
+        desc = describe(net, forms=False)
+        states = oracle.states_of(net, desc)
+        prepared = oracle.prepare(desc)
+        del desc
     build_s = time.perf_counter() - t0
-    for _ in range(args.warmup):
-        net.run_steps(SIM_STEPS_PER_STEP)
-    torch.cuda.synchronize(dev)
-    ev0, l0 = rt.counters()["events"], rt.launches
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    with Clocks(dev.index or 0) as clocks:
-        for k in range(args.steps):
-            flush.zero_()
-            rt.stream.wait_stream(torch.cuda.current_stream(dev))
-            starts[k].record(rt.stream)
-            net.run_steps(SIM_STEPS_PER_STEP)
-            ends[k].record(rt.stream)
-        torch.cuda.synchronize(dev)
-    dev_ms = sum(st.elapsed_time(e) for st, e in zip(starts, ends))
-    events = rt.counters()["events"] - ev0
-    net.check()
-    return {"metric": METRIC, "value": events / (dev_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded draws on the GPU, Brunel model A at config 1's size)",
-            "config": {"workload": "brunel_config1_transpiled", "neurons": sum(len(p.shape) for p in pops.values()),
-                       "sim_steps_per_step": SIM_STEPS_PER_STEP, "launch": "one per population and step, from the host",
-                       "l2": "flushed before every timed step (256 MiB write)"},
-            "us_per_sim_step": dev_ms * 1e3 / (args.steps * SIM_STEPS_PER_STEP),
-            "gpu_launches": rt.launches - l0, "build_s": build_s, "clocks": clocks.summary()}
+    m = measure(net, args, dev, world, sim)
+    stats = [SpikeStats(len(p.shape), net.resolution, t_skip_ms=0.0) for p in pops]
+    for p, s in zip(pops, stats):  # the last end-to-end step's raster
+        s.add_words(net.runtime.raster_words(p), 0)
+    m["dev_ms_rank0"], m["events_rank0"] = m["dev_ms"], m["events"]
+    m["dev_ms"], m["e2e_s"], m["events"], m["e2e_events"] = reduce_over_ranks(
+        [m["dev_ms"], m["e2e_s"]], [m["events"], m["e2e_events"]], world, dev)
+    line = line_of(name, m, args, world, sim, neurons, nb, cfg, dev)
+    if name == "pd14_config2":
+        from naer2_b200.networks import pd14
 
-
-def run_pd14(args, dev) -> dict:
-    """Config 2: the full PD14 microcircuit (77,169 neurons, ~3e8 synapses) built on the GPU; events/s over the
-    timed steps, population rates and CV-ISI over them."""
-    import numpy as np
-    import torch
-
-    from naer2_b200.networks import pd14
-
-    t0 = time.perf_counter()
-    net, pops = pd14.build(scale=args.scale, seed=1, device=dev)
-    net.persistent = args.mode == "persistent"
-    net.record(args.steps * SIM_STEPS_PER_STEP)
-    for p in pops:
-        p.state_tensor("potential", dev)
-    rt_build = time.perf_counter()
-    net.run_steps(1)  # builds the runtime
-    rt = net.runtime
-    build_s = time.perf_counter() - t0
-    for _ in range(args.warmup):
-        net.run_steps(SIM_STEPS_PER_STEP)
-    net.record(args.steps * SIM_STEPS_PER_STEP)
-    torch.cuda.synchronize(dev)
-    ev0 = rt.counters()["events"]
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    with Clocks(dev.index or 0) as clocks:
-        for k in range(args.steps):
-            flush.zero_()
-            rt._enter()
-            starts[k].record(rt.stream)
-            net.run_steps(SIM_STEPS_PER_STEP)
-            ends[k].record(rt.stream)
-        torch.cuda.synchronize(dev)
-    dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    events = rt.counters()["events"] - ev0
-    net.check()
-    steps = args.steps * SIM_STEPS_PER_STEP
-    rates, cvs = [], []
-    for p in pops:
-        r = torch.from_numpy(rt.raster(p))  # [steps, n]
-        n = r.shape[1]
-        rates.append(float(r.sum()) / n / (steps * 1e-4))
-        step_idx, nid = torch.nonzero(r, as_tuple=True)
-        order = torch.argsort(nid * (steps + 1) + step_idx)
-        nid, t = nid[order], step_idx[order].double()
-        same = nid[1:] == nid[:-1]
-        isi = (t[1:] - t[:-1])[same]
-        owner = nid[1:][same]
-        cnt = torch.bincount(owner, minlength=n).double()
-        s1 = torch.bincount(owner, weights=isi, minlength=n)
-        s2 = torch.bincount(owner, weights=isi * isi, minlength=n)
-        ok = cnt >= 3
-        mean = s1[ok] / cnt[ok]
-        var = (s2[ok] - cnt[ok] * mean * mean) / (cnt[ok] - 1)
-        cvs.append(float((var.clamp(min=0).sqrt() / mean).mean()) if int(ok.sum()) else float("nan"))
-    ev_step = events / steps
-    n_neurons = sum(len(p.shape) for p in pops)
-    alg = ev_step * BYTES_PER_EVENT + n_neurons * (BYTES_PER_NEURON_STEP + 16)
-    us = dev_ms * 1e3 / steps
-    peak, kind = measured_peaks()
-    return {"metric": METRIC, "value": events / (dev_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded draws on the GPU, PD14 microcircuit)",
-            "config": {"workload": "pd14_config2", "scale": args.scale, "neurons": n_neurons,
-                       "synapses": rt.n_links, "dt_ms": 0.1, "sim_steps_per_step": SIM_STEPS_PER_STEP,
-                       "launch": MODE, "l2": "flushed before every timed step (256 MiB write)"},
-            "realtime_factor": (dev_ms / 1e3) / (steps * 1e-4),
-            "roofline": {"bound": "hbm", "achieved": alg / (us * 1e-6) / 1e9, "peak": peak, "unit": "GB/s",
-                         "frac": alg / (us * 1e-6) / 1e9 / peak, "traffic": None, "peak_kind": kind,
-                         "bytes_per_launch": alg, "us_per_launch": us},
-            "l2_atomics": l2_atomics(events / (dev_ms / 1e3), dev),
-            "rates_hz": dict(zip(pd14.NAMES, [round(x, 3) for x in rates])),
-            "cv_isi": dict(zip(pd14.NAMES, [round(x, 3) for x in cvs])),
-            "events_per_sim_step": ev_step, "build_s": build_s, "clocks": clocks.summary()}
+        names = pd14.NAMES
+    else:
+        names = ["E", "I"]
+    line["rates_hz_last_step"] = {k: round(s.rate_hz(), 3) for k, s in zip(names, stats)}
+    line["cv_isi_last_step"] = {k: round(s.cv_isi(), 3) for k, s in zip(names, stats)}
+    line["build_s"] = build_s
+    net.close()
+    del net
+    torch.cuda.empty_cache()
+    if prepared is not None:
+        line["cpu_baseline"] = cpu_sample(prepared, states, 0.1, name)
+    return line
 
 
 def run_batched(args, dev) -> dict:
     """Config 3: B uneven Brunel instances in one network (one persistent launch per window), tuned by the
-    autotuner, against the same instances stepped one network at a time on the same GPU (same seeds: the same
-    spikes). Aggregate synaptic events/s of both, and per-instance rates."""
+    autotuner, against the same instances stepped one network at a time on the same GPU, each tuned by the
+    same autotuner over the same candidates (same seeds: the same spikes). Aggregate synaptic events/s of both,
+    and per-instance rates."""
     import torch
 
     from naer2_b200.networks import batched
@@ -382,6 +426,7 @@ def run_batched(args, dev) -> dict:
     net, parts = batched.build(B, seed=1, device=dev)
     build_s = time.perf_counter() - t0
     report = autotune(net, steps=200, warmup=50) if args.tune else None
+    net.window = sim
     net.run_steps(args.warmup * sim)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     ms_b, ev_b, spk_b = 0.0, 0, None
@@ -392,17 +437,18 @@ def run_batched(args, dev) -> dict:
         spk_b = spk if spk_b is None else [x + y for x, y in zip(spk_b, spk)]
     n_links = net.runtime.n_links
     neurons = sum(len(p.shape) for p in net.populations)
-    chosen = dict(block=net.block, grid=net.grid, persistent=net.persistent, tuned=dict(net.tuned))
+    chosen = dict(block=net.block, grid=net.grid, persistent=net.persistent, pull=len(net.tuned))
     net.close()
     del net, parts
     torch.cuda.empty_cache()
-    # the same instances, one network at a time, the tuned configuration
-    ms_p, ev_p, spk_p = 0.0, 0, []
+    # the same instances, one network at a time, each tuned the same way
+    ms_p, ev_p, spk_p, plain_choice = 0.0, 0, [], []
     for b in range(B):
         inst, _ = batched.build_instance(b, seed=1, device=dev)
-        # the single instances at two blocks per SM: measured faster for them than the persistent default
-        sms = torch.cuda.get_device_properties(dev).multi_processor_count
-        inst.block, inst.grid, inst.persistent = chosen["block"], 2 * sms, chosen["persistent"]
+        if args.tune:
+            r = autotune(inst, steps=200, warmup=50)
+            plain_choice.append(r["chosen"])
+        inst.window = sim
         inst.run_steps(args.warmup * sim)
         for _ in range(args.steps):
             flush.zero_()
@@ -426,15 +472,26 @@ def run_batched(args, dev) -> dict:
             "ms_per_step": ms_b / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded draws on the GPU, 64 uneven Brunel instances)",
             "config": {"workload": "batched_config3", "instances": B, "neurons": neurons, "synapses": n_links,
-                       "dt_ms": 0.1, "sim_steps_per_step": sim, "tuned": {k: v for k, v in chosen.items()
-                                                                             if k != "tuned"}},
+                       "dt_ms": 0.1, "sim_steps_per_step": sim, "tuned": chosen,
+                       "l2": "flushed before every timed step (256 MiB write)"},
             "l2_atomics": l2_atomics(value, dev),
-            "plain_one_at_a_time": {"value": plain, "ms_per_step": ms_p / args.steps},
+            "plain_one_at_a_time": {"value": plain, "ms_per_step": ms_p / args.steps,
+                                    "tuned": _summarise_choices(plain_choice)},
             "batched_over_plain": value / plain,
             "identical_spike_counts": spk_b == spk_p,
             "rates_hz_first4": [[round(x, 2) for x in r] for r in rates_b[:4]],
             "max_rate_difference_hz": max(abs(x - y) for rb, rp in zip(rates_b, rates_p) for x, y in zip(rb, rp)),
-            "tune": report["trials"] if report else None, "build_s": build_s}
+            "tune_trials": report["trials"] if report else None, "build_s": build_s}
+
+
+def _summarise_choices(choices: list) -> dict | None:
+    if not choices:
+        return None
+    out = {}
+    for c in choices:
+        key = f"block {c['block']}, {'persistent' if c['persistent'] else 'per-step'}, pull {c['pull']}"
+        out[key] = out.get(key, 0) + 1
+    return out
 
 
 def run_bptt(args, dev) -> dict:
@@ -507,6 +564,100 @@ def run_bptt(args, dev) -> dict:
             "realtime_factor": (ms_plain / 1e3) / (T * 1e-3), "build_s": build_s, "clocks": clocks.summary()}
 
 
+def run_transpiled(args, dev) -> dict:
+    """Config 1's network with TranspiledLIF neurons (the built-in LIF's dynamics, its Poisson drive drawn in its
+    own hook): the run-time compiled step kernels, events/s over the timed steps."""
+    import torch
+
+    from naer2_b200.networks import brunel
+
+    t0 = time.perf_counter()
+    net, pops = brunel.build(**brunel.CONFIG1, seed=1, device=dev, transpiled=True)
+    net.run_steps(1)  # builds the runtime: transpiles and compiles the hooks
+    rt = net.runtime
+    build_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        net.run_steps(SIM_STEPS_PER_STEP)
+    torch.cuda.synchronize(dev)
+    ev0, l0 = rt.counters()["events"], rt.launches
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with Clocks(dev.index or 0) as clocks:
+        for k in range(args.steps):
+            flush.zero_()
+            rt.stream.wait_stream(torch.cuda.current_stream(dev))
+            starts[k].record(rt.stream)
+            net.run_steps(SIM_STEPS_PER_STEP)
+            ends[k].record(rt.stream)
+        torch.cuda.synchronize(dev)
+    dev_ms = sum(st.elapsed_time(e) for st, e in zip(starts, ends))
+    events = rt.counters()["events"] - ev0
+    net.check()
+    return {"metric": METRIC, "value": events / (dev_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded draws on the GPU, Brunel model A at config 1's size)",
+            "config": {"workload": "brunel_config1_transpiled", "neurons": sum(len(p.shape) for p in pops.values()),
+                       "sim_steps_per_step": SIM_STEPS_PER_STEP, "launch": "one per population and step, from the host",
+                       "l2": "flushed before every timed step (256 MiB write)"},
+            "us_per_sim_step": dev_ms * 1e3 / (args.steps * SIM_STEPS_PER_STEP),
+            "gpu_launches": rt.launches - l0, "build_s": build_s, "clocks": clocks.summary()}
+
+
+def compact(line: dict) -> dict:
+    """A workload's line without the keys the headline line already states."""
+    drop = {"metric", "unit", "n_gpus", "higher_is_better", "scaling", "vs_baseline", "data", "warmup"}
+    return {k: v for k, v in line.items() if k not in drop}
+
+
+def run_reference(args) -> None:
+    """The reference arm: the CPU implementation (the oracle port, all host threads) on the same workload -- the
+    network built on the host from the same parameters -- over the same window of simulation steps (W bench
+    steps of warm-up, then K timed), rank 0 only."""
+    import oracle
+    from naer2_b200.runtime import describe
+
+    name = {1: "brunel_A_config1", 2: "pd14_config2"}.get(args.config, "pd14_config2")
+    sim = SIM_STEPS_PER_STEP
+    t0 = time.perf_counter()
+    net, pops, nb, cfg = build_workload(name, 1, device=None)
+    desc = describe(net, forms=False)
+    states = oracle.states_of(net, desc)
+    prepared = oracle.prepare(desc)
+    del desc
+    build_s = time.perf_counter() - t0
+    used = oracle.set_threads(0)
+    n = 0
+    for _ in range(args.warmup):
+        oracle.run(prepared, states, n, sim, record=False)
+        n += sim
+    t0 = time.perf_counter()
+    events = 0
+    for _ in range(args.steps):
+        _, ev = oracle.run(prepared, states, n, sim, record=False)
+        events += ev
+        n += sim
+    el = time.perf_counter() - t0
+    value = events / el
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded draws: connectivity, weights, delays, initial state, Philox Poisson drive)",
+            "config": {**cfg, "sim_steps_per_step": sim, "window_steps": sim,
+                       "l2": "flushed before every timed step (256 MiB write)",
+                       "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "single GPU",
+                       "launch": "persistent"},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "port",
+                             "sample": f"simulation steps {args.warmup * sim}-{n} of {name} (after {args.warmup} x "
+                                       f"{sim} warm-up steps), C oracle, {used} OpenMP threads, nproc "
+                                       f"{os.cpu_count()}; the network drawn on the host"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "realtime_factor": el / (args.steps * sim * 1e-4), "build_s": build_s}
+    print(json.dumps(line))
+
+
 def main() -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -514,23 +665,20 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="naer2_b200", choices=["naer2_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", type=int, default=1, choices=[1, 2, 3, 4],
-                    help="1: Brunel model A at config 1's size (the default workload); 2: the PD14 microcircuit; "
-                         "3: 64 uneven Brunel instances batched against one at a time; 4: BPTT of the "
-                         "recurrent LIF layer (training step against the plain forward)")
+    ap.add_argument("--no-workloads", action="store_true", help="the headline workload alone (no sub-objects)")
+    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4],
+                    help="2: the PD14 microcircuit (the headline, default); 1: Brunel model A at config 1's size; "
+                         "3: 64 uneven Brunel instances batched against one at a time; 4: BPTT of the recurrent "
+                         "LIF layer (training step against the plain forward)")
     ap.add_argument("--instances", type=int, default=64, help="config 3: instances")
-    ap.add_argument("--tune", action="store_true", help="config 3: run the autotuner first")
-    ap.add_argument("--scale", type=float, default=1.0, help="config 2: population sizes times this")
-    ap.add_argument("--mode", choices=["persistent", "per-step"], default="persistent",
-                    help="a window of steps per cooperative launch, or one launch per step")
+    ap.add_argument("--no-tune", dest="tune", action="store_false", help="config 3: skip the autotuner")
     ap.add_argument("--transpiled", action="store_true",
                     help="config 1 with the neurons' hooks transpiled and compiled at run time (TranspiledLIF)")
     ap.add_argument("--sim-steps", type=int, default=1000,
                     help="simulation steps per bench step (default 1000; small values for profiling runs)")
     args = ap.parse_args()
-    global SIM_STEPS_PER_STEP, MODE
+    global SIM_STEPS_PER_STEP
     SIM_STEPS_PER_STEP = args.sim_steps
-    MODE = args.mode
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -541,12 +689,8 @@ def main() -> int:
             run_reference(args)
         return 0
 
-    import numpy as np
     import torch
     import torch.distributed as dist
-
-    from naer2_b200.networks import brunel
-    from naer2_b200.runtime import describe
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -555,126 +699,25 @@ def main() -> int:
             raise SystemExit("--transpiled runs config 1 on one GPU")
         print(json.dumps(run_transpiled(args, dev)))
         return 0
-    if args.config in (2, 3, 4):
+    if args.config in (3, 4):
         if world > 1:
             raise SystemExit(f"config {args.config} runs on one GPU")
-        run = {2: run_pd14, 3: run_batched, 4: run_bptt}[args.config]
-        print(json.dumps(run(args, dev)))
+        print(json.dumps({3: run_batched, 4: run_bptt}[args.config](args, dev)))
         return 0
     if world > 1:
         import datetime
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize(dev)
-
-    net, pops = brunel.build(**brunel.CONFIG1, seed=1 + rank)
-    net.persistent = args.mode == "persistent"
-    desc = describe(net) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
-    import oracle as _oracle_for_baseline_only  # noqa: F401  (the CPU baseline leg below)
-
-    cpu_states = _oracle_for_baseline_only.states_of(net, desc) if desc is not None else None
-    net.record(SIM_STEPS_PER_STEP)
-    rt = net.runtime
-    n_neurons = sum(len(p.shape) for p in net.populations)
-
-    # ---- device-resident timing
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    for _ in range(args.warmup):
-        net.run_steps(SIM_STEPS_PER_STEP)
-    barrier()
-    ev0 = rt.counters()["events"]
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    with Clocks(local) as clocks:
-        barrier()
-        for k in range(args.steps):
-            flush.zero_()
-            rt._enter()  # the runtime's stream after the flush
-            starts[k].record(rt.stream)
-            net.run_steps(SIM_STEPS_PER_STEP)
-            ends[k].record(rt.stream)
-        barrier()
-    dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    events = rt.counters()["events"] - ev0
-    launches = args.steps * SIM_STEPS_PER_STEP  # simulation steps (one step kernel each, or one window iteration)
-    windows = args.steps * (SIM_STEPS_PER_STEP // max(net.window, 1) + (SIM_STEPS_PER_STEP % max(net.window, 1) > 0))
-    # kernels launched: per-step mode one per step; persistent mode one per window; + one counter advance per window
-    launches_all = (launches if MODE == "per-step" else windows) + windows
-    net.check()
-
-    # ---- end to end through the public API, host buffers
-    hosts = []
-    for p in net.populations:
-        for attr in ("V", "ref"):
-            t = p.state_tensor(attr)
-            hosts.append((p, attr, torch.empty(t.shape, dtype=t.dtype, pin_memory=True)))
-    for p, attr, h in hosts:
-        h.copy_(p.state_tensor(attr))
-    raster_host = [torch.empty(r.shape, dtype=r.dtype, pin_memory=True) for r in rt.rasters]
-    h2d = sum(h.numel() * h.element_size() for _, _, h in hosts)
-    d2h = h2d + sum(r.numel() * r.element_size() for r in raster_host)
-    barrier()
-    ev1 = rt.counters()["events"]
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        for p, attr, h in hosts:  # inputs: the network state, from pinned host memory
-            p.state_tensor(attr).copy_(h, non_blocking=True)
-        net.record(SIM_STEPS_PER_STEP)
-        net.step(SIM_STEPS_PER_STEP * net.resolution)
-        for r, h in zip(rt.rasters, raster_host):  # results: the spike raster and the state
-            h.copy_(r, non_blocking=True)
-        for p, attr, h in hosts:
-            h.copy_(p.state_tensor(attr), non_blocking=True)
-        torch.cuda.current_stream(dev).synchronize()
-    e2e_s = time.perf_counter() - t0
-    e2e_events = rt.counters()["events"] - ev1
-
-    # ---- max over ranks
-    dev_ms, e2e_s, events_all, e2e_events_all = reduce_over_ranks([dev_ms, e2e_s], [events, e2e_events], world, dev)
-
-    cpu = None
-    if desc is not None:
-        cpu = cpu_sample(desc, cpu_states)
-
-    if rank == 0:
-        value = events_all / (dev_ms / 1e3)
-        ms_per_launch = dev_ms / launches
-        ev_per_launch = events / launches
-        alg_bytes = ev_per_launch * BYTES_PER_EVENT + n_neurons * BYTES_PER_NEURON_STEP
-        achieved = alg_bytes / (ms_per_launch / 1e3) / 1e9
-        peak, peak_kind = measured_peaks()
-        traffic = None
-        prof = ROOT / "profiles" / "persistent_kernel_brunel_config1.json"
-        if prof.exists() and MODE == "persistent":  # one ncu capture, scaled to this run's events per step
-            pr = json.loads(prof.read_text())
-            traffic = pr["dram_bytes_per_step"] * ev_per_launch / pr["events_per_step"]
-        line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox network, Brunel model A)",
-            "config": config(world),
-            "realtime_factor": (dev_ms / 1e3) / (args.steps * SIM_STEPS_PER_STEP * 1e-4),
-            "e2e": {"value": e2e_events_all / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": ("n2b::persistent_kernel<256>" if MODE == "persistent" else "n2b::step_kernel<256>"),
-                         "bytes_per_launch": alg_bytes, "us_per_launch": ms_per_launch * 1e3,
-                         "note": "per simulation step: timed device time / steps (launch gaps and grid barriers "
-                                 "included)"},
-            "l2_atomics": l2_atomics(events / (dev_ms / 1e3), dev),
-            "gpu_launches": launches_all,
-            "clocks": clocks.summary(),
-            "events_per_sim_step": ev_per_launch,
+    name = "pd14_config2" if args.config == 2 else "brunel_A_config1"
+    line = run_plain(name, args, dev, rank, world, cpu=not args.no_cpu_baseline)
+    if world == 1 and args.config == 2 and not args.no_workloads:
+        line["workloads"] = {
+            "brunel_A_config1": compact(run_plain("brunel_A_config1", args, dev, 0, 1, cpu=False)),
+            "batched_config3": compact(run_batched(args, dev)),
+            "bptt_config4": compact(run_bptt(args, dev)),
         }
-        if cpu is not None:
-            line["cpu_baseline"] = cpu
+    if rank == 0:
         print(json.dumps(line))
-    net.close()
     if world > 1:
         dist.destroy_process_group()
     return 0

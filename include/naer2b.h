@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define N2B_ABI_VERSION 1
+#define N2B_ABI_VERSION 2
 
 /* return codes */
 #define N2B_OK 0
@@ -53,7 +53,9 @@ extern "C" {
 #define N2B_ERR_PULL_LINK 1 /* pull links with delay 0, delay >= bit depth, or source >= n */
 #define N2B_ERR_SPLIT 2     /* push links past a row's split with a delay below 2 steps (skipped) */
 #define N2B_ERR_ITEMS 3     /* work-list entries past its capacity (skipped; cannot happen for a valid split) */
-#define N2B_ERR_BARRIER 4   /* persistent windows: a grid barrier wait that gave up after 2 s (the window stopped) */
+#define N2B_ERR_BARRIER 4   /* persistent windows: a grid barrier wait that gave up (n2b_options.barrier_limit_ns,
+                               default 2 s): the window stopped, and later windows return at once until
+                               n2b_reset_counters */
 #define N2B_ERR_WORDS 8
 
 /* One population: the state arrays and rings of the reference's
@@ -116,6 +118,10 @@ typedef struct n2b_options {
                         blocks, each looping over its tiles) */
     int32_t persistent; /* 1: a window of steps is one cooperative launch, steps separated by a grid
                            barrier; 0: one launch per step */
+    int32_t reserved;
+    int64_t barrier_limit_ns; /* persistent windows: the longest a block waits at a grid barrier before the
+                                 window stops with N2B_ERR_BARRIER (0: 2 s). Tests set a few ns: the wait
+                                 then gives up at once although every block arrives, without a hang */
 } n2b_options;
 
 typedef struct n2b_net n2b_net;
@@ -214,6 +220,9 @@ typedef struct n2b_bptt_desc {
     const int32_t *out_grp;   /* [H][6] outgoing rows: start of the delay-1..5 links, then the row end */
     const uint16_t *out_code; /* [nnz] target | delay << 11, outgoing order */
     const int32_t *out_perm;  /* [nnz] incoming-order index of each outgoing link */
+    int32_t wait_polls;       /* polls before a backward exchange wait gives up with error word 3 (0: about a
+                                 second); tests set a few, so that the wait gives up without a hang */
+    int32_t reserved;
 } n2b_bptt_desc;
 
 /* Device workspace bytes of the layer (spike tape, checkpoints, one segment's
@@ -302,15 +311,18 @@ int n2b_jit_destroy(n2b_jit_kernel *k);
  * arrival slots before the call's work ends, so a later call from step
  * step0 + n_steps continues the run exactly. If `status` is not NULL, the call
  * waits for its work on `stream` and copies the N2B_ERR_WORDS error words
- * there.
+ * there; with status NULL no error word is reported (a grid barrier that gave
+ * up, or links out of range, pass unseen). Every call waits on `stream` for its
+ * own set-up (it copies the network's tables into the array first), and it
+ * makes `opt->device` current only for its own work: the caller's current
+ * device is the same after the call.
  *
  * Limits: a network whose workspace (n2b_workspace_bytes) exceeds
  * N2B_STATIC_SCRATCH_BYTES is rejected with N2B_ESPACE. Every device that
- * loads this library holds the array until the process exits. The first call
- * on a device looks the array's address up (with that device current); make
- * that first call before any stream capture. Every call on a device shares
- * the one array, and each call starts by resetting the counts, error words
- * and barrier in it: two calls whose work overlaps on the GPU (different
+ * loads this library holds the array until the process exits. Each call looks
+ * the array's address up on the device it runs on. Every call on a device
+ * shares the one array, and each call starts by resetting the counts, error
+ * words and barrier in it: two calls whose work overlaps on the GPU (different
  * streams, or threads) race and corrupt each other. */
 int n2b_run_static(const n2b_population *pops, int32_t n_pops, const n2b_connection *conns, int32_t n_conns,
                    const n2b_options *opt, int64_t step0, int64_t n_steps, int32_t *status, void *stream);

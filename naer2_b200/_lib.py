@@ -9,7 +9,7 @@ import pathlib
 
 LIB_PATH = pathlib.Path(__file__).resolve().parent / "libnaer2b.so"
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 MODEL_LIF_DELTA, MODEL_PD14, MODEL_POISSON_SOURCE = 1, 2, 3
 PUSH, PULL = 0, 1
 ERR_PUSH_LINK, ERR_PULL_LINK, ERR_SPLIT, ERR_ITEMS, ERR_BARRIER, ERR_WORDS = 0, 1, 2, 3, 4, 8
@@ -38,7 +38,7 @@ class Connection(ctypes.Structure):
 
 class Options(ctypes.Structure):
     _fields_ = [("block", ctypes.c_int32), ("device", ctypes.c_int32), ("grid", ctypes.c_int32),
-                ("persistent", ctypes.c_int32)]
+                ("persistent", ctypes.c_int32), ("reserved", ctypes.c_int32), ("barrier_limit_ns", ctypes.c_int64)]
 
 
 BPTT_ERR_WORDS = 4  # N2B_BPTT_ERR_WORDS
@@ -51,7 +51,8 @@ class BpttDesc(ctypes.Structure):
         ("nnz", ctypes.c_int32), ("in_cta_max", ctypes.c_int32), ("out_cta_max", ctypes.c_int32),
         ("alpha", ctypes.c_float), ("beta", ctypes.c_float), ("theta", ctypes.c_float), ("slope", ctypes.c_float),
         ("in_ptr", ctypes.c_void_p), ("in_code", ctypes.c_void_p), ("out_grp", ctypes.c_void_p),
-        ("out_code", ctypes.c_void_p), ("out_perm", ctypes.c_void_p),
+        ("out_code", ctypes.c_void_p), ("out_perm", ctypes.c_void_p), ("wait_polls", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 

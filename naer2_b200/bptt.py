@@ -243,6 +243,9 @@ class RecurrentLIF(torch.nn.Module):
         self._ws = None
         self._ws_key = None
         self.tape_id = 0
+        # polls before a wait of the backward's per-step exchange gives up (0: the library's default, about a
+        # second); tests set a few to make the wait give up without a hang
+        self.wait_polls = 0
 
     # ------------------------------------------------------------------ the kernels' view
 
@@ -255,6 +258,7 @@ class RecurrentLIF(torch.nn.Module):
         d.alpha, d.beta, d.theta, d.slope = self.alpha, self.beta, self.theta, self.slope
         d.in_ptr, d.in_code, d.out_grp = w.in_ptr.data_ptr(), w.in_code.data_ptr(), w.out_grp.data_ptr()
         d.out_code, d.out_perm = w.out_code.data_ptr(), w.out_perm.data_ptr()
+        d.wait_polls = int(self.wait_polls)
         return d
 
     def workspace(self, d: _lib.BpttDesc) -> torch.Tensor:

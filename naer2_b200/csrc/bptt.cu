@@ -81,6 +81,7 @@ struct Args {
     float *qx;          // [NC][2][H][8] the adjoint's q exchange ring (slot t & 1)
     uint32_t *xcnt;     // [NC] the adjoint's arrivals per group (zeroed before each launch)
     int32_t *err;       // [N2B_BPTT_ERR_WORDS]
+    int wait_polls;     // polls before an exchange wait gives up
 };
 
 __device__ __forceinline__ float surrogate(float x, float slope) {
@@ -141,18 +142,19 @@ __host__ __device__ inline BwdSmem bwd_smem(int H, int HC, int R, int out_cta_ma
 // add on the group's counter; later (other work in between), a bounded acquire spin until `target` arrivals
 // (every CTA of the group at this step). A wait that gives up counts in err[3] and sets `aborted`, after which
 // the CTA still arrives but no longer waits, so that neither it nor the CTAs that wait for its arrivals can hang.
-constexpr int XCHG_SPIN_LIMIT = 1 << 21;  // polls of an L2 round trip each: about a second
+constexpr int XCHG_SPIN_LIMIT = 1 << 21;  // default polls (n2b_bptt_desc.wait_polls = 0): about a second
 __device__ __forceinline__ void group_arrive(uint32_t *cnt) {
     __threadfence();
     asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(cnt) : "memory");
 }
-__device__ __forceinline__ void group_wait(const uint32_t *cnt, uint32_t target, int32_t *err, int &aborted) {
+__device__ __forceinline__ void group_wait(const uint32_t *cnt, uint32_t target, int32_t *err, int limit,
+                                           int &aborted) {
     if (aborted) return;
     for (int it = 0;; ++it) {
         uint32_t v;
         asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(cnt) : "memory");
         if (v >= target) return;
-        if (it >= XCHG_SPIN_LIMIT) {
+        if (it >= limit) {
             atomicAdd(err + 3, 1);
             aborted = 1;
             return;
@@ -732,7 +734,7 @@ __global__ void __launch_bounds__(512) bwd_kernel(const __grid_constant__ Args a
             for (int d = 2; d <= MAXD; ++d)
                 out_rows(t + 1, d, SMOOTH ? 0xffu : (uint32_t)((hist >> (8 * (d - 2))) & 0xffu), histf[d - 2]);
         }
-        if (tid == 0) group_wait(xcnt, target, a.err, aborted);
+        if (tid == 0) group_wait(xcnt, target, a.err, a.wait_polls, aborted);
         __syncthreads();  // every CTA's q[t] written, every read of q[t + 1] done: copy q[t] (past L1) into pnew
         for (int j = tid; j < H * (NS / 4); j += nthr)
             reinterpret_cast<float4 *>(pnew)[(size_t)(j >> 1) * (QROW / 4) + (j & 1)] =
@@ -903,6 +905,7 @@ int check_desc(const n2b_bptt_desc *d) {
         return bfail(N2B_EINVAL, "missing link arrays");
     if (!d->in_ptr || !d->out_grp) return bfail(N2B_EINVAL, "missing row arrays");
     if (d->in_cta_max < 0 || d->out_cta_max < 0) return bfail(N2B_EINVAL, "negative link counts");
+    if (d->wait_polls < 0) return bfail(N2B_EINVAL, "wait_polls < 0");
     return N2B_OK;
 }
 
@@ -964,6 +967,7 @@ Args args_of(const n2b_bptt_desc *d, char *ws, const WsLayout &L) {
     a.qx = reinterpret_cast<float *>(ws + L.qx);
     a.xcnt = reinterpret_cast<uint32_t *>(ws + L.xcnt);
     a.err = reinterpret_cast<int32_t *>(ws + L.err);
+    a.wait_polls = d->wait_polls > 0 ? d->wait_polls : XCHG_SPIN_LIMIT;
     return a;
 }
 

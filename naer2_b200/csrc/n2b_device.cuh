@@ -93,6 +93,7 @@ struct StepArgs {
     int32_t *tile_claim;   // per step n mod 3: tiles past the first gridDim.x claimed so far
     unsigned *barrier;     // persistent kernel: the arrival counter, the abort word
     unsigned long long *trace;  // N2B_TRACE builds: per step and block, %globaltimer at each phase (else unused)
+    unsigned long long bar_limit_ns;  // persistent windows: a grid barrier wait gives up after this long
     int32_t trace_steps;
     int32_t item_cap;
     int32_t n_tiles;
@@ -150,7 +151,7 @@ constexpr int BAR_COUNT = 0;      // persistent launches: arrivals of this launc
 constexpr int BAR_ABORT = 32;     // set when a barrier wait gave up (a line of its own)
 constexpr int BAR_WORDS = 64;
 constexpr int BAR_MAX_BLOCKS = 1 << 16;
-constexpr unsigned long long BAR_LIMIT_NS = 2000000000ull;  // a barrier wait gives up after 2 s
+constexpr unsigned long long BAR_LIMIT_NS = 2000000000ull;  // default: a barrier wait gives up after 2 s
 
 // ------------------------------------------------------------------ Philox
 
@@ -831,8 +832,10 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
 // Grid-wide barrier k (0, 1, ...) of a cooperative launch: every block adds 1 to one counter with release
 // semantics (its writes before its arrival) and waits, with acquire loads, until the counter holds
 // (k + 1) * gridDim.x -- the counter starts each launch at 0 (advance_kernel clears it after every launch).
-// Every wait is bounded (BAR_LIMIT_NS): a timeout sets error word 4 and the abort word, and the kernel winds
-// down instead of hanging. Returns false once aborted.
+// Every wait is bounded (a.bar_limit_ns, BAR_LIMIT_NS by default): a timeout sets error word 4 and the abort
+// word, and the kernel winds down instead of hanging. Returns false once aborted. A wait ends in every case:
+// its count is reached, another block's abort is seen, or its own time runs out (and it sets the abort word
+// before it leaves, so that a block still waiting at this or a later barrier sees it).
 __device__ __forceinline__ bool grid_sync(const StepArgs &a, unsigned k) {
     __shared__ int s_ok;
     __syncthreads();
@@ -846,7 +849,7 @@ __device__ __forceinline__ bool grid_sync(const StepArgs &a, unsigned k) {
             if ((int)(ld_acquire(bar + BAR_COUNT) - target) >= 0) break;
             if (*(volatile unsigned *)(bar + BAR_ABORT)) { ok = 0; break; }
             if (spin == 0) t0 = globaltimer();
-            else if (globaltimer() - t0 > BAR_LIMIT_NS) {
+            else if (globaltimer() - t0 > a.bar_limit_ns) {
                 atomicExch(bar + BAR_ABORT, 1u);
                 atomicAdd(a.err + 4, 1);
                 ok = 0;

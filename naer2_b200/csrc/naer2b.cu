@@ -11,7 +11,6 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -38,6 +37,18 @@ int cuda_fail(cudaError_t e, const char *what) {
     } while (0)
 
 bool pow2(int32_t x) { return x > 0 && (x & (x - 1)) == 0; }
+
+// The calling thread's current device, put back when an entry point returns (each one makes its handle's
+// device current for its work).
+struct DeviceGuard {
+    int prev = -1;
+    DeviceGuard() {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
 
 }  // namespace
 
@@ -94,6 +105,7 @@ int validate(const n2b_population *pops, int32_t n_pops, const n2b_connection *c
         return fail(N2B_EINVAL, "negative counts or missing arrays");
     const int32_t block = block_of(opt);
     if (block != 64 && block != 128 && block != 256) return fail(N2B_EINVAL, "block must be 64, 128 or 256");
+    if (opt && opt->barrier_limit_ns < 0) return fail(N2B_EINVAL, "barrier_limit_ns < 0");
     for (int32_t p = 0; p < n_pops; ++p) {
         const n2b_population &P = pops[p];
         const std::string at = "population " + std::to_string(p) + ": ";
@@ -237,6 +249,7 @@ int n2b_workspace_bytes(const n2b_population *pops, int32_t n_pops, const n2b_co
 
 int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection *conns, int32_t n_conns,
                const n2b_options *opt, void *workspace, size_t workspace_bytes, void *stream, n2b_net **out) {
+    DeviceGuard guard;
     if (!out) return fail(N2B_EINVAL, "out is NULL");
     *out = nullptr;
     int rc = validate(pops, n_pops, conns, n_conns, opt);
@@ -390,6 +403,8 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     a.n_tiles = L.n_tiles;
     a.offset = 0;
     a.barrier = reinterpret_cast<unsigned *>(ws + L.barrier);
+    a.bar_limit_ns = (opt && opt->barrier_limit_ns > 0) ? (unsigned long long)opt->barrier_limit_ns
+                                                         : n2b::BAR_LIMIT_NS;
     a.n_pops = n_pops;
     a.n_push = L.n_push;
     if (inl) {
@@ -409,6 +424,7 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
 }
 
 int n2b_step(n2b_net *net, int64_t n_steps, void *stream) {
+    DeviceGuard guard;
     if (!net) return fail(N2B_EINVAL, "net is NULL");
     if (n_steps < 0 || n_steps > (int64_t)1 << 30) return fail(N2B_EINVAL, "n_steps out of range");
     N2B_CUDA(cudaSetDevice(net->device));
@@ -418,6 +434,7 @@ int n2b_step(n2b_net *net, int64_t n_steps, void *stream) {
 }
 
 int n2b_capture(n2b_net *net, int32_t window_steps, void *stream) {
+    DeviceGuard guard;
     if (!net) return fail(N2B_EINVAL, "net is NULL");
     if (window_steps <= 0 || window_steps > (1 << 20)) return fail(N2B_EINVAL, "window_steps out of range");
     N2B_CUDA(cudaSetDevice(net->device));
@@ -445,6 +462,7 @@ int n2b_capture(n2b_net *net, int32_t window_steps, void *stream) {
 }
 
 int n2b_replay(n2b_net *net, int64_t n_windows, void *stream) {
+    DeviceGuard guard;
     if (!net) return fail(N2B_EINVAL, "net is NULL");
     if (!net->exec) return fail(N2B_ESTATE, "no captured window: call n2b_capture first");
     if (n_windows < 0) return fail(N2B_EINVAL, "n_windows < 0");
@@ -455,6 +473,7 @@ int n2b_replay(n2b_net *net, int64_t n_windows, void *stream) {
 }
 
 int n2b_set_step(n2b_net *net, int64_t step, void *stream) {
+    DeviceGuard guard;
     if (!net) return fail(N2B_EINVAL, "net is NULL");
     if (step < 0) return fail(N2B_EINVAL, "step < 0");
     N2B_CUDA(cudaSetDevice(net->device));
@@ -465,6 +484,7 @@ int n2b_set_step(n2b_net *net, int64_t step, void *stream) {
 }
 
 int n2b_record(n2b_net *net, int64_t step0, void *stream) {
+    DeviceGuard guard;
     if (!net) return fail(N2B_EINVAL, "net is NULL");
     N2B_CUDA(cudaSetDevice(net->device));
     n2b::set_kernel<<<1, 1, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
@@ -474,6 +494,7 @@ int n2b_record(n2b_net *net, int64_t step0, void *stream) {
 }
 
 int n2b_status(n2b_net *net, int32_t *words, int32_t n_words, void *stream) {
+    DeviceGuard guard;
     if (!net || !words || n_words < 0) return fail(N2B_EINVAL, "bad arguments");
     N2B_CUDA(cudaSetDevice(net->device));
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -485,6 +506,7 @@ int n2b_status(n2b_net *net, int32_t *words, int32_t n_words, void *stream) {
 }
 
 int n2b_counters(n2b_net *net, uint64_t *out, int32_t n_out, void *stream) {
+    DeviceGuard guard;
     if (!net || !out || n_out < 0) return fail(N2B_EINVAL, "bad arguments");
     N2B_CUDA(cudaSetDevice(net->device));
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -497,6 +519,7 @@ int n2b_counters(n2b_net *net, uint64_t *out, int32_t n_out, void *stream) {
 }
 
 int n2b_reset_counters(n2b_net *net, void *stream) {
+    DeviceGuard guard;
     if (!net) return fail(N2B_EINVAL, "net is NULL");
     N2B_CUDA(cudaSetDevice(net->device));
     n2b::zero_kernel<<<1, 64, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
@@ -521,6 +544,7 @@ int n2b_trace(n2b_net *net, unsigned long long *trace, int32_t steps, int32_t *g
 #endif
 
 int n2b_destroy(n2b_net *net) {
+    DeviceGuard guard;
     if (!net) return N2B_OK;
     cudaSetDevice(net->device);
     drop_graph(net);
@@ -541,22 +565,16 @@ static __device__ __align__(256) unsigned char g_static_scratch[N2B_STATIC_SCRAT
 
 namespace {
 
-constexpr int STATIC_MAX_DEVICES = 64;
-std::mutex g_static_mu;
-void *g_static_ptr[STATIC_MAX_DEVICES] = {};
-
-// The array's device address on `device` (which must be current): looked up once per device, on its first call.
-int static_scratch(int device, void **out) {
-    if (device < 0 || device >= STATIC_MAX_DEVICES) return fail(N2B_EINVAL, "device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_static_mu);
-    if (!g_static_ptr[device]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_static_scratch)");
-        if (!p || (reinterpret_cast<uintptr_t>(p) & 255) != 0) return fail(N2B_ECUDA, "static scratch misaligned");
-        g_static_ptr[device] = p;
-    }
-    *out = g_static_ptr[device];
+// The array's device address on the current device. In host code `g_static_scratch` names a host-side stand-in,
+// never the device copy, so the address is asked of the runtime -- on every call: the call is cheap next to
+// n2b_create's synchronisations, and an address kept from an earlier call would be stale after a
+// cudaDeviceReset (the next primary context maps the array elsewhere).
+int static_scratch(void **out) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_static_scratch)");
+    if (!p || (reinterpret_cast<uintptr_t>(p) & 255) != 0) return fail(N2B_ECUDA, "static scratch misaligned");
+    *out = p;
     return N2B_OK;
 }
 
@@ -564,6 +582,9 @@ int static_scratch(int device, void **out) {
 // what is left of a run that stops after step n - 1.
 template <int NPB, bool INL>
 __global__ void __launch_bounds__(NPB) drain_kernel(const __grid_constant__ n2b::StepArgs a) {
+    // a persistent window that gave up at a grid barrier may have left its last step's tiles undone: its work
+    // list is then incomplete, and nothing of it is delivered (error word 4 reports the stop)
+    if (*(volatile unsigned *)(a.barrier + n2b::BAR_ABORT)) return;
     __shared__ n2b::SConn s_tab[n2b::SMEM_CONNS];
     const n2b::SConn *s_conn = n2b::fill_conns<INL>(a, s_tab, a.n_push);
     __syncthreads();
@@ -596,10 +617,11 @@ extern "C" int n2b_run_static(const n2b_population *pops, int32_t n_pops, const 
                                     " bytes of workspace, the static scratch holds " +
                                     std::to_string((size_t)N2B_STATIC_SCRATCH_BYTES) +
                                     " (use n2b_create with a workspace of the caller's)");
+    DeviceGuard guard;
     const int device = opt ? opt->device : 0;
     N2B_CUDA(cudaSetDevice(device));
     void *ws = nullptr;
-    rc = static_scratch(device, &ws);
+    rc = static_scratch(&ws);
     if (rc) return rc;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     n2b_net *net = nullptr;

@@ -29,6 +29,9 @@ class Network:
         # a window of steps as one persistent cooperative launch (steps separated by a grid barrier), or one
         # launch per step
         self.persistent: bool = True
+        # persistent windows: how long a block may wait at a grid barrier before the window stops with an error
+        # word (0: the library's 2 s); tests set a few ns to make the wait give up without a hang
+        self.barrier_limit_ns: int = 0
         self.device = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else None
         self.record_steps: int = 0  # raster rows kept per population (Network.record)
         self.tuned: dict = {}  # per connection id: the push/pull choice the tuner measured (naer2_b200.tune)

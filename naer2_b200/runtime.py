@@ -125,11 +125,13 @@ class NetDesc:
     n_links: int
 
 
-def describe(net, modes: dict | None = None) -> NetDesc:
+def describe(net, modes: dict | None = None, forms: bool = True) -> NetDesc:
     """The network as the kernels see it: per population its model constants, ring depths, fixed-point
     shift and external-drive table; per connection its CSR form, built where its topology lives (a pattern
     drawn on the GPU is restructured there). modes: connection id -> "push" / "pull" (default: the
-    connection's own `mode`, else the network's tuned choice, else push)."""
+    connection's own `mode`, else the network's tuned choice, else push). forms=False: the canonical rows only
+    (ConnDesc.canonical), no device form (ptr, link, w and split None) -- a description for a host-side
+    checker of a large network, without the form's sort."""
     dt = float(net.resolution)
     pops, conns = list(net.populations), list(net.connections)
     index = {id(p): k for k, p in enumerate(pops)}
@@ -191,6 +193,11 @@ def describe(net, modes: dict | None = None) -> NetDesc:
     for s, t, topo, steps, wscalar, warr, mode in cinfo:
         n_tgt = len(pops[t].shape)
         split = None
+        if not forms:
+            cdesc.append(ConnDesc(src=s, tgt=t, mode=mode, n_links=len(topo), ptr=None, link=None,
+                                  weight=wscalar if wscalar is not None else 0.0, w=None, split=None, topo=topo,
+                                  steps=steps, warr=warr))
+            continue
         if mode == "pull":
             ptr, link, perm = pull_form(topo, steps, n_tgt)
         elif mode == "push":
@@ -272,7 +279,8 @@ class NetworkRuntime:
         block = net.block or min([p.group_size for p in pops] + [256])
         block = 64 if block <= 64 else 128 if block <= 128 else 256
         self.opt = _lib.Options(block=block, device=dev.index if dev.index is not None else 0, grid=int(net.grid or 0),
-                                persistent=int(bool(net.persistent)))
+                                persistent=int(bool(net.persistent)),
+                                barrier_limit_ns=int(getattr(net, "barrier_limit_ns", 0) or 0))
         nbytes = ctypes.c_size_t()
         _lib.check(lib.n2b_workspace_bytes(self.cpop, len(pops), self.cconn, len(desc.conns), ctypes.byref(self.opt),
                                            ctypes.byref(nbytes)), "n2b_workspace_bytes")
@@ -355,6 +363,12 @@ class NetworkRuntime:
         if words[_lib.ERR_PUSH_LINK] or words[_lib.ERR_PULL_LINK]:
             raise RuntimeError(f"links out of range: {words[_lib.ERR_PUSH_LINK]} push, "
                                f"{words[_lib.ERR_PULL_LINK]} pull")
+        if words[_lib.ERR_SPLIT] or words[_lib.ERR_ITEMS]:
+            raise RuntimeError(f"deferred links dropped: {words[_lib.ERR_SPLIT]} below 2 steps past a row's split, "
+                               f"{words[_lib.ERR_ITEMS]} past the work list's capacity")
+        if words[_lib.ERR_BARRIER]:
+            raise RuntimeError(f"a persistent window stopped: {words[_lib.ERR_BARRIER]} grid barrier wait(s) gave up "
+                               "(the run is incomplete; reset_counters clears the stop)")
 
     def counters(self) -> dict:
         out = (ctypes.c_uint64 * (2 + len(self.pops)))()

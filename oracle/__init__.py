@@ -112,10 +112,30 @@ def _ptr(a):
     return a.ctypes.data if a is not None else None
 
 
-def run(desc, states: list, step0: int, n_steps: int, record: bool = True, ext_counts: dict | None = None):
-    """Run the description's network from step0 for n_steps in place on `states` (one State per population).
-    Returns (rasters: list of bool [n_steps, n] or None, events). ext_counts: population index -> int32
-    [n_steps, n] external counts to use instead of the Philox draws."""
+class Prepared:
+    """A description with its connections' canonical rows converted to host arrays once (for networks whose
+    rows are large, run in many chunks): pass it to run() in place of the description."""
+
+    def __init__(self, desc):
+        self.dt, self.pops = desc.dt, desc.pops
+        self.rows = []
+        for c in desc.conns:
+            ptr, link, w = c.canonical()
+            self.rows.append((c.src, c.tgt, c.weight, np.ascontiguousarray(ptr, dtype=np.int32),
+                              np.ascontiguousarray(link, dtype=np.uint32),
+                              None if w is None else np.ascontiguousarray(w, dtype=np.float32)))
+
+
+def prepare(desc) -> Prepared:
+    return Prepared(desc)
+
+
+def run(desc, states: list, step0: int, n_steps: int, record: bool = True, ext_counts: dict | None = None,
+        packed: bool = False):
+    """Run the description's network (or a Prepared one) from step0 for n_steps in place on `states` (one State
+    per population). Returns (rasters: list of bool [n_steps, n] -- packed: uint32 words [n_steps, ceil(n/32)],
+    bit j of word w neuron 32 w + j -- or None, events). ext_counts: population index -> int32 [n_steps, n]
+    external counts to use instead of the Philox draws."""
     lib = load()
     pops = (OrPop * max(len(desc.pops), 1))()
     keep = []
@@ -144,21 +164,26 @@ def run(desc, states: list, step0: int, n_steps: int, record: bool = True, ext_c
             rasters.append((r, words))
         else:
             rasters.append(None)
-    conns = (OrConn * max(len(desc.conns), 1))()
-    for k, c in enumerate(desc.conns):
+    if isinstance(desc, Prepared):
+        rows = desc.rows
+    else:  # rows per source, canonical order
+        rows = []
+        for c in desc.conns:
+            ptr, link, w = c.canonical()
+            rows.append((c.src, c.tgt, c.weight, np.ascontiguousarray(ptr, dtype=np.int32),
+                         np.ascontiguousarray(link, dtype=np.uint32),
+                         None if w is None else np.ascontiguousarray(w, dtype=np.float32)))
+    conns = (OrConn * max(len(rows), 1))()
+    for k, (src, tgt, weight, ptr, link, w) in enumerate(rows):
         oc = conns[k]
-        ptr, link, w = c.canonical()  # rows per source, canonical order
-        ptr = np.ascontiguousarray(ptr, dtype=np.int32)
-        link = np.ascontiguousarray(link, dtype=np.uint32)
         keep += [ptr, link]
-        oc.src, oc.tgt, oc.ptr, oc.link = c.src, c.tgt, _ptr(ptr), _ptr(link)
+        oc.src, oc.tgt, oc.ptr, oc.link = src, tgt, _ptr(ptr), _ptr(link)
         if w is not None:
-            w = np.ascontiguousarray(w, dtype=np.float32)
             keep.append(w)
             oc.w = _ptr(w)
-        oc.weight = c.weight
+        oc.weight = weight
     events = ctypes.c_uint64(0)
-    rc = lib.or_run(pops, len(desc.pops), conns, len(desc.conns), step0, n_steps, ctypes.byref(events))
+    rc = lib.or_run(pops, len(desc.pops), conns, len(rows), step0, n_steps, ctypes.byref(events))
     if rc != 0:
         raise RuntimeError(f"oracle run failed ({rc})")
     out = []
@@ -167,6 +192,9 @@ def run(desc, states: list, step0: int, n_steps: int, record: bool = True, ext_c
             out.append(None)
             continue
         r, words = rr
+        if packed:
+            out.append(r.reshape(n_steps, words))
+            continue
         bits = np.unpackbits(r.view(np.uint8).reshape(n_steps, words, 4), axis=2, bitorder="little")
         out.append(bits.reshape(n_steps, words * 32)[:, :d.n].astype(bool))
     return out, int(events.value)

@@ -143,6 +143,30 @@ static int pd14(or_pop *p, int32_t j, float input) {
 
 /* ---------------------------------------------------------------- the step loop */
 
+/* One neuron's intake, update and send at step n; returns its spike (or -1 for a bad description). */
+static int neuron_step(or_pop *p, int32_t j, int64_t n, int64_t *slot) {
+    if (p->model == OR_MODEL_POISSON_SOURCE) return draw(p, j, n, 1u) < p->fire_threshold;
+    int64_t a = slot ? slot[j] : 0;
+    if (slot) slot[j] = 0;
+    if (p->ext_counts) {
+        if (n < p->ext_step0 || n >= p->ext_step0 + p->ext_steps) return -1;
+        a += (int64_t)p->ext_counts[(size_t)(n - p->ext_step0) * (size_t)p->n + (size_t)j] * p->ext_wfx;
+    } else if (p->ext_table && p->ext_len > 0) {
+        a += (int64_t)poisson_count(p->ext_table, p->ext_len, draw(p, j, n, 0u)) * p->ext_wfx;
+    }
+    float input = fx_to_float(a, p->shift);
+    if (p->model == OR_MODEL_LIF_DELTA) return lif_delta(p, j, input);
+    if (p->model == OR_MODEL_PD14) return pd14(p, j, input);
+    return -1;
+}
+
+/* A run of at most RUN links of one spike's outgoing row in one connection: the unit of the parallel
+ * delivery (the sums are exact integers, so the units may run in any order). */
+#define RUN 512
+typedef struct {
+    int32_t conn, first, end;
+} or_unit;
+
 int or_run(or_pop *pops, int32_t n_pops, const or_conn *conns, int32_t n_conns,
            int64_t step0, int64_t n_steps, uint64_t *events) {
     for (int32_t c = 0; c < n_conns; ++c) {
@@ -150,102 +174,115 @@ int or_run(or_pop *pops, int32_t n_pops, const or_conn *conns, int32_t n_conns,
             return -1;
     }
     if (n_pops < 0 || n_conns < 0) return -1;
-    int32_t total = 0;
+    int32_t total = 0, total_words = 0;
     for (int32_t q = 0; q < n_pops; ++q) {
         if (pops[q].n < 0 || (pops[q].acc_depth & (pops[q].acc_depth - 1)) != 0) return -1;
         total += pops[q].n;
+        total_words += (pops[q].n + 31) / 32;
     }
     int32_t *spk = (int32_t *)malloc(sizeof(int32_t) * (size_t)(total > 0 ? total : 1));
     int32_t *first = (int32_t *)calloc((size_t)n_pops + 1, sizeof(int32_t));
     int32_t *count = (int32_t *)calloc((size_t)n_pops + 1, sizeof(int32_t));
-    if (!spk || !first || !count) { free(spk); free(first); free(count); return -3; }
-    for (int32_t q = 0; q < n_pops; ++q) first[q + 1] = first[q] + pops[q].n;
-    /* per population its spike words of the step: population q's at first[q] / 32 + q */
-    uint32_t *mark = (uint32_t *)calloc((size_t)total / 32 + 2 * (size_t)n_pops + 2, sizeof(uint32_t));
-    if (!mark) { free(spk); free(first); free(count); return -3; }
+    /* per population its first word in the step's flat word list (every population's words in one loop) */
+    int32_t *wfirst = (int32_t *)calloc((size_t)n_pops + 1, sizeof(int32_t));
+    int32_t *wpop = (int32_t *)malloc(sizeof(int32_t) * (size_t)(total_words > 0 ? total_words : 1));
+    uint32_t *mark = (uint32_t *)calloc((size_t)(total_words > 0 ? total_words : 1), sizeof(uint32_t));
+    int64_t *wfx_const = (int64_t *)calloc((size_t)n_conns + 1, sizeof(int64_t));
+    size_t cap = 1024;
+    or_unit *units = (or_unit *)malloc(sizeof(or_unit) * cap);
+    if (!spk || !first || !count || !wfirst || !wpop || !mark || !wfx_const || !units) {
+        free(spk); free(first); free(count); free(wfirst); free(wpop); free(mark); free(wfx_const); free(units);
+        return -3;
+    }
+    for (int32_t q = 0; q < n_pops; ++q) {
+        first[q + 1] = first[q] + pops[q].n;
+        wfirst[q + 1] = wfirst[q] + (pops[q].n + 31) / 32;
+        for (int32_t w = wfirst[q]; w < wfirst[q + 1]; ++w) wpop[w] = q;
+    }
+    for (int32_t c = 0; c < n_conns; ++c) wfx_const[c] = or_wfx(conns[c].weight, pops[conns[c].tgt].shift);
     uint64_t ev = 0;
     int rc = 0;
 
     for (int64_t s = 0; s < n_steps && rc == 0; ++s) {
         int64_t n = step0 + s;
-        /* update every population from its due arrival slot (neurons are independent) */
-        for (int32_t q = 0; q < n_pops && rc == 0; ++q) {
-            or_pop *p = &pops[q];
-            int32_t words = (p->n + 31) / 32;
-            uint32_t *row = NULL;
-            if (p->raster && n >= p->raster_step0 && n < p->raster_step0 + p->raster_steps) {
-                row = p->raster + (size_t)(n - p->raster_step0) * (size_t)words;
-                memset(row, 0, sizeof(uint32_t) * (size_t)words);
-            }
-            int64_t *slot = p->acc ? p->acc + (size_t)(n & (p->acc_depth - 1)) * (size_t)p->n : NULL;
-            int bad = 0;
-            /* one word of 32 neurons per iteration: the raster word and the spike marks are the thread's own */
+        /* update every neuron of every population from its due arrival slot (neurons are independent); one word
+         * of 32 neurons per iteration: the raster word and the spike marks are the iteration's own */
+        int bad = 0;
 #pragma omp parallel for schedule(static) num_threads(g_threads) reduction(|:bad)
-            for (int32_t w = 0; w < words; ++w) {
-                uint32_t bits = 0;
-                int32_t j1 = (w + 1) * 32 < p->n ? (w + 1) * 32 : p->n;
-                for (int32_t j = w * 32; j < j1; ++j) {
-                    int fire = 0;
-                    if (p->model == OR_MODEL_POISSON_SOURCE) {
-                        fire = draw(p, j, n, 1u) < p->fire_threshold;
-                    } else {
-                        int64_t a = slot ? slot[j] : 0;
-                        if (slot) slot[j] = 0;
-                        if (p->ext_counts) {
-                            if (n < p->ext_step0 || n >= p->ext_step0 + p->ext_steps) { bad = 1; continue; }
-                            a += (int64_t)p->ext_counts[(size_t)(n - p->ext_step0) * (size_t)p->n + (size_t)j] * p->ext_wfx;
-                        } else if (p->ext_table && p->ext_len > 0) {
-                            a += (int64_t)poisson_count(p->ext_table, p->ext_len, draw(p, j, n, 0u)) * p->ext_wfx;
-                        }
-                        float input = fx_to_float(a, p->shift);
-                        if (p->model == OR_MODEL_LIF_DELTA) fire = lif_delta(p, j, input);
-                        else if (p->model == OR_MODEL_PD14) fire = pd14(p, j, input);
-                        else { bad = 1; continue; }
-                    }
-                    if (fire) bits |= 1u << (j & 31);
-                }
-                if (row) row[w] = bits;
-                mark[first[q] / 32 + q + w] = bits;
+        for (int32_t gw = 0; gw < total_words; ++gw) {
+            const int32_t q = wpop[gw], w = gw - wfirst[q];
+            or_pop *p = &pops[q];
+            int64_t *slot = p->acc ? p->acc + (size_t)(n & (p->acc_depth - 1)) * (size_t)p->n : NULL;
+            uint32_t bits = 0;
+            int32_t j1 = (w + 1) * 32 < p->n ? (w + 1) * 32 : p->n;
+            for (int32_t j = w * 32; j < j1; ++j) {
+                int fire = neuron_step(p, j, n, slot);
+                if (fire < 0) { bad = 1; break; }
+                if (fire) bits |= 1u << (j & 31);
             }
-            if (bad) { rc = -4; break; }
-            /* the spikes of this step, in index order */
+            mark[gw] = bits;
+            if (p->raster && n >= p->raster_step0 && n < p->raster_step0 + p->raster_steps)
+                p->raster[(size_t)(n - p->raster_step0) * (size_t)((p->n + 31) / 32) + (size_t)w] = bits;
+        }
+        if (bad) { rc = -4; break; }
+        /* the spikes of this step, per population in index order */
+        for (int32_t q = 0; q < n_pops; ++q) {
             count[q] = 0;
-            for (int32_t w = 0; w < words; ++w) {
-                uint32_t bits = mark[first[q] / 32 + q + w];
+            for (int32_t gw = wfirst[q]; gw < wfirst[q + 1]; ++gw) {
+                uint32_t bits = mark[gw];
                 while (bits) {
                     int b = __builtin_ctz(bits);
                     bits &= bits - 1;
-                    spk[first[q] + count[q]++] = w * 32 + b;
+                    spk[first[q] + count[q]++] = (gw - wfirst[q]) * 32 + b;
                 }
             }
         }
-        /* deliver every spike of this step along its outgoing links (exact integer adds: any order) */
-        for (int32_t c = 0; c < n_conns && rc == 0; ++c) {
+        /* the step's deliveries as runs of links: every spike's row in every outgoing connection */
+        size_t nu = 0;
+        for (int32_t c = 0; c < n_conns; ++c) {
             const or_conn *cn = &conns[c];
-            or_pop *tgt = &pops[cn->tgt];
-            int64_t wfx_const = or_wfx(cn->weight, tgt->shift);
-            int bad = 0;
-            uint64_t ev_c = 0;
-#pragma omp parallel for schedule(dynamic, 4) num_threads(g_threads) reduction(|:bad) reduction(+:ev_c)
             for (int32_t k = 0; k < count[cn->src]; ++k) {
                 int32_t s_id = spk[first[cn->src] + k];
-                for (int32_t l = cn->ptr[s_id]; l < cn->ptr[s_id + 1]; ++l) {
-                    uint32_t rec = cn->link[l];
-                    int32_t d = (int32_t)(rec >> 24), t = (int32_t)(rec & 0xFFFFFFu);
-                    if (d < 1 || d >= tgt->acc_depth || t >= tgt->n || !tgt->acc) { bad = 1; break; }
-                    int64_t wfx = cn->w ? or_wfx(cn->w[l], tgt->shift) : wfx_const;
-                    int64_t *cell = &tgt->acc[(size_t)((n + d) & (tgt->acc_depth - 1)) * (size_t)tgt->n + (size_t)t];
-                    if (g_threads > 1) __atomic_fetch_add(cell, wfx, __ATOMIC_RELAXED);
-                    else *cell += wfx;
-                    ++ev_c;
+                for (int32_t l = cn->ptr[s_id]; l < cn->ptr[s_id + 1]; l += RUN) {
+                    if (nu == cap) {
+                        or_unit *grown = (or_unit *)realloc(units, sizeof(or_unit) * cap * 2);
+                        if (!grown) { rc = -3; break; }
+                        units = grown;
+                        cap *= 2;
+                    }
+                    int32_t e = cn->ptr[s_id + 1] - l > RUN ? l + RUN : cn->ptr[s_id + 1];
+                    units[nu].conn = c;
+                    units[nu].first = l;
+                    units[nu].end = e;
+                    ++nu;
                 }
+                if (rc) break;
             }
-            ev += ev_c;
-            if (bad) rc = -2;
+            if (rc) break;
         }
+        if (rc) break;
+        /* deliver: exact integer adds into the arrival slots, any order */
+        uint64_t ev_s = 0;
+#pragma omp parallel for schedule(dynamic, 4) num_threads(g_threads) reduction(|:bad) reduction(+:ev_s)
+        for (size_t u = 0; u < nu; ++u) {
+            const or_conn *cn = &conns[units[u].conn];
+            or_pop *tgt = &pops[cn->tgt];
+            for (int32_t l = units[u].first; l < units[u].end; ++l) {
+                uint32_t rec = cn->link[l];
+                int32_t d = (int32_t)(rec >> 24), t = (int32_t)(rec & 0xFFFFFFu);
+                if (d < 1 || d >= tgt->acc_depth || t >= tgt->n || !tgt->acc) { bad = 1; break; }
+                int64_t wfx = cn->w ? or_wfx(cn->w[l], tgt->shift) : wfx_const[units[u].conn];
+                int64_t *cell = &tgt->acc[(size_t)((n + d) & (tgt->acc_depth - 1)) * (size_t)tgt->n + (size_t)t];
+                if (g_threads > 1) __atomic_fetch_add(cell, wfx, __ATOMIC_RELAXED);
+                else *cell += wfx;
+                ++ev_s;
+            }
+        }
+        ev += ev_s;
+        if (bad) rc = -2;
     }
     if (events) *events += ev;
-    free(spk); free(first); free(count); free(mark);
+    free(spk); free(first); free(count); free(wfirst); free(wpop); free(mark); free(wfx_const); free(units);
     return rc;
 }
 

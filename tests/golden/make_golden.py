@@ -1,10 +1,10 @@
 """Regenerate the golden fixtures of this directory from the reference itself.
 
-    python tests/golden/make_golden.py [--reference PATH]
+    python tests/golden/make_golden.py --reference PATH   (or NAER2_REFERENCE=PATH)
 
-Runs only where the reference source tree is available (default
-/root/reference); the fixtures it writes are committed, and the tests read
-only them. What each fixture pins:
+Runs only where the reference source tree is available (PATH: the root of
+its checkout); the fixtures it writes are committed, and the tests read only
+them. What each fixture pins:
 
 brunel_reference_c0.npz
     The reference's time-driven Brunel loop, tools/brunel_reference.py:34-48,
@@ -24,6 +24,17 @@ pd14_neuron.npz
     extracted from its source and run here on CPU step by step over a fixed
     dt of 0.1 ms, with a per-step input current (count * J) injected as
     `received`. Outputs: the raster and the state after every 10th step.
+
+brunel_longrun_c1.json
+    The same loop at config 1's size (N_E/N_I 10,000/2,500, C_E/C_I
+    1,000/250) over 10,000 steps of 0.1 ms (1 s), with the reference's own
+    connectivity rule (with replacement, autapses kept; drawn here so that the
+    oracle can run the same network: longrun_network), its one delay of
+    1.5 ms, V0 drawn here, and its own Poisson drive (torch.poisson, torch's
+    generator seeded). Its statistics are computed by its own code
+    (lines 50-62: rate after 50 ms, CV-ISI over the first 2,000 neurons with
+    at least 4 spikes, activity std/mean in 1 ms bins), captured instead of
+    printed; plus the loop's wall time on this machine's cores.
 
 philox_triton.json
     tl.randint4x / tl.rand of Triton (the reference's random lowering calls
@@ -107,6 +118,55 @@ def brunel_c0(reference: pathlib.Path, steps: int = 1000):
     print(f"brunel_reference_c0: {raster.sum()} spikes in {steps} steps")
 
 
+LONGRUN_KEY = 23
+LONGRUN = dict(NE=10000, NI=2500, CE=1000, CI=250, delay_steps=15, steps=10000)
+
+
+def longrun_network(NE: int, NI: int, CE: int, CI: int, key: int = LONGRUN_KEY):
+    """(src int64 [N, C_E + C_I], V0 fp32 [N]) of the long-run fixture: per target C_E sources from E and C_I from
+    I, uniform with replacement, autapses kept (the reference's rule, tools/brunel_reference.py:20-21);
+    V0 uniform in [0, 20) mV. Numpy's Philox under `key`: the test draws the same network."""
+    rng = np.random.Generator(np.random.Philox(key=key))
+    N = NE + NI
+    src = np.concatenate([rng.integers(0, NE, size=(N, CE)), NE + rng.integers(0, NI, size=(N, CI))], axis=1)
+    V0 = (rng.random(N, dtype=np.float32) * np.float32(20.0)).astype(np.float32)
+    return src.astype(np.int64), V0
+
+
+def brunel_longrun(reference: pathlib.Path):
+    import time
+
+    import torch
+
+    P = LONGRUN
+    NE, NI, CE, CI, steps = P["NE"], P["NI"], P["CE"], P["CI"], P["steps"]
+    src, V0 = longrun_network(NE, NI, CE, CI)
+    text = (reference / "tools" / "brunel_reference.py").read_text()
+    text = _sub(text, 'dt = float(sys.argv[1]) if len(sys.argv) > 1 else 0.05', "dt = 0.1")
+    text = _sub(text, "T = 400.0", f"T = {steps * 0.1!r}")
+    text = _sub(text, 'dev = "cuda"', 'dev = "cpu"')
+    text = _sub(text, "src = torch.cat([torch.randint(0, NE, (N, CE), generator=gen), NE + torch.randint(0, NI, "
+                      "(N, CI), generator=gen)], 1).flatten()", "src = _golden_src.flatten()")
+    text = _sub(text, "V = torch.rand(N, generator=gen).to(dev) * theta", "V = _golden_V0.clone()")
+    text = _sub(text, "torch.cuda.synchronize()", "_golden_wall.append(time.time() - t0)")
+    text = _sub(text, '    print(f"{name}: rate {rate:.2f} Hz, CV(ISI) {sum(cvs)/len(cvs):.2f}, activity std/mean '
+                      '{float(act.std()/act.mean()):.2f}")',
+                '    _golden_stats[name] = dict(rate_hz=rate, cv_isi=sum(cvs) / len(cvs), '
+                'activity_std_over_mean=float(act.std() / act.mean()), spikes=int(m.sum()))')
+    torch.manual_seed(LONGRUN_KEY)  # the reference's torch.poisson draws from torch's default generator
+    ns = {"_golden_src": torch.from_numpy(src), "_golden_V0": torch.from_numpy(V0), "_golden_stats": {},
+          "_golden_wall": [], "__name__": "golden"}
+    exec(compile(text, str(reference / "tools" / "brunel_reference.py"), "exec"), ns)
+    spikes = int(sum(len(i) for i in ns["spk_i"]))
+    wall = ns["_golden_wall"][0]
+    out = {"network": dict(P, key=LONGRUN_KEY, J=0.1, g=5.0, eta=2.0, dt_ms=0.1, autapses=True),
+           "stats": ns["_golden_stats"], "loop_wall_s": wall, "spikes": spikes,
+           "events_per_s": spikes * (CE + CI) / wall, "torch_threads": torch.get_num_threads(),
+           "nproc": os.cpu_count(), "torch": torch.__version__}
+    (HERE / "brunel_longrun_c1.json").write_text(json.dumps(out, indent=1))
+    print(f"brunel_longrun_c1: {spikes} spikes, {ns['_golden_stats']}, loop {wall:.1f} s")
+
+
 def _reference_function(path: pathlib.Path, name: str):
     """A top-level function of a reference module, compiled from its source alone (its imports not run)."""
     tree = ast.parse(path.read_text())
@@ -184,9 +244,12 @@ def philox_triton():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
-    ap.add_argument("--only", choices=["brunel", "pd14", "philox"])
+    ap.add_argument("--reference", default=os.environ.get("NAER2_REFERENCE"),
+                    help="root of the reference checkout (or the NAER2_REFERENCE environment variable)")
+    ap.add_argument("--only", choices=["brunel", "pd14", "philox", "longrun"])
     args = ap.parse_args()
+    if not args.reference:
+        raise SystemExit("give --reference PATH (or NAER2_REFERENCE): the root of the reference checkout")
     ref = pathlib.Path(args.reference)
     if not ref.exists():
         raise SystemExit(f"the reference tree is not at {ref}: the committed fixtures stand")
@@ -196,6 +259,8 @@ def main():
         brunel_c0(ref)
     if args.only in (None, "pd14"):
         pd14_neuron(ref)
+    if args.only in (None, "longrun"):
+        brunel_longrun(ref)
 
 
 if __name__ == "__main__":
