@@ -81,6 +81,17 @@ int load_nvrtc(Nvrtc **out) {
 
 }  // namespace
 
+// The calling thread's current device, put back when an entry point returns.
+struct JitDeviceGuard {
+    int prev = -1;
+    JitDeviceGuard() {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    }
+    ~JitDeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 extern "C" {
 
 int n2b_jit_compile(const char *source, const char *kernel_name, const char *const *options, int32_t n_options,
@@ -91,6 +102,7 @@ int n2b_jit_compile(const char *source, const char *kernel_name, const char *con
     Nvrtc *nv = nullptr;
     int rc = load_nvrtc(&nv);
     if (rc) return rc;
+    JitDeviceGuard guard;
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return n2b_host::set_error(N2B_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
     int major = 0, minor = 0;
@@ -135,6 +147,7 @@ int n2b_jit_launch(n2b_jit_kernel *k, uint32_t grid, uint32_t block, const void 
                    void *stream) {
     if (!k || !params || params_bytes == 0 || grid == 0 || block == 0 || block > 1024)
         return n2b_host::set_error(N2B_EINVAL, "bad arguments");
+    JitDeviceGuard guard;
     cudaError_t e = cudaSetDevice(k->device);
     if (e == cudaSuccess) {
         void *args[] = {const_cast<void *>(params)};
@@ -147,6 +160,7 @@ int n2b_jit_launch(n2b_jit_kernel *k, uint32_t grid, uint32_t block, const void 
 
 int n2b_jit_destroy(n2b_jit_kernel *k) {
     if (!k) return N2B_OK;
+    JitDeviceGuard guard;
     cudaSetDevice(k->device);
     if (k->lib) cudaLibraryUnload(k->lib);
     delete k;
