@@ -56,6 +56,8 @@ extern "C" {
 #define N2B_ERR_BARRIER 4   /* persistent windows: a grid barrier wait that gave up (n2b_options.barrier_limit_ns,
                                default 2 s): the window stopped, and later windows return at once until
                                n2b_reset_counters */
+#define N2B_ERR_PULL_STAGE 5 /* staged pull chunks that did not land within the wait limit (loaded directly
+                                 instead; the launch stops staging) */
 #define N2B_ERR_WORDS 8
 
 /* One population: the state arrays and rings of the reference's

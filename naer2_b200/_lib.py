@@ -12,7 +12,7 @@ LIB_PATH = pathlib.Path(__file__).resolve().parent / "libnaer2b.so"
 ABI_VERSION = 2
 MODEL_LIF_DELTA, MODEL_PD14, MODEL_POISSON_SOURCE = 1, 2, 3
 PUSH, PULL = 0, 1
-ERR_PUSH_LINK, ERR_PULL_LINK, ERR_SPLIT, ERR_ITEMS, ERR_BARRIER, ERR_WORDS = 0, 1, 2, 3, 4, 8
+ERR_PUSH_LINK, ERR_PULL_LINK, ERR_SPLIT, ERR_ITEMS, ERR_BARRIER, ERR_PULL_STAGE, ERR_WORDS = 0, 1, 2, 3, 4, 5, 8
 STATIC_SCRATCH_BYTES = 32 << 20  # N2B_STATIC_SCRATCH_BYTES: the workspace limit of n2b_run_static
 
 

@@ -67,7 +67,7 @@ struct alignas(16) PopDev {
 
 struct alignas(16) ConnDev {
     int32_t homogeneous, src_n, tgt_n, tgt_acc_mask;
-    int32_t src_bit_mask, src_words, has_split, pad1;
+    int32_t src_bit_mask, src_words, has_split, staged;  // staged (pull): link (and w) 16-byte aligned
     long long wfx;        // homogeneous weight, fixed point of the target
     float wscale;         // 2^shift of the target (exact)
     float pad2;
@@ -95,6 +95,7 @@ struct StepArgs {
     unsigned long long *trace;  // N2B_TRACE builds: per step and block, %globaltimer at each phase (else unused)
     unsigned long long bar_limit_ns;  // persistent windows: a grid barrier wait gives up after this long
     int32_t trace_steps;
+    int32_t pull_staged;   // the launch has a PullStage per warp in dynamic shared memory
     int32_t item_cap;
     int32_t n_tiles;
     int32_t offset;        // this launch's step = *step + offset (per-step launches)
@@ -305,35 +306,191 @@ __device__ __forceinline__ bool pd14(const PopDev &P, float in, float &v, float 
 // Every pull connection into the population: each warp walks the incoming
 // rows of its 32 neurons one after another, the lanes striding a row
 // (coalesced link loads), testing each link's source bit in the ring row of
-// step n - delay; the warp's sum lands in the row's owner lane.
+// step n - delay; the warp's sum lands in the row's owner lane. The plain walk:
+// used for connections whose rows are not 16-byte aligned, and where the launch
+// has no staging memory.
 template <bool INL>
-__device__ __forceinline__ long long pull_intake(const StepArgs &a, const PopDev &P, int first, int count,
+__device__ __forceinline__ long long pull_walk(const ConnDev &C, int32_t *err, int wbase, int nq, long long n) {
+    const int lane = threadIdx.x & 31;
+    long long mine = 0;
+    for (int q = 0; q < nq; ++q) {
+        const int jq = wbase + q;
+        const int r0 = __ldg(C.ptr + jq), r1 = __ldg(C.ptr + jq + 1);
+        long long part = 0;
+        for (int l = r0 + lane; l < r1; l += 32) {
+            const uint32_t rec = __ldg(C.link + l);
+            const int d = (int)(rec >> 24), s = (int)(rec & 0xFFFFFFu);
+            if (d >= 1 && d <= C.src_bit_mask && s < C.src_n) {
+                const uint32_t word =
+                    __ldcg(C.src_bits + (size_t)((n - d) & C.src_bit_mask) * C.src_words + (s >> 5));
+                if ((word >> (s & 31)) & 1u) part += C.homogeneous ? C.wfx : weight_fx(__ldg(C.w + l), C.wscale);
+            } else {
+                atomicAdd(err + 1, 1);
+            }
+        }
+        part = warp_sum64(part);
+        if (lane == q) mine += part;
+    }
+    return mine;
+}
+
+// The staged pull (the reference's pull intake, fused.py:1626-1965, with its link runs staged through shared
+// memory): the warp's incoming links -- one contiguous range of the pull CSR, rows of its 32 neurons -- stream
+// into shared memory by 1-D bulk copies (cp.async.bulk, completion counted on an mbarrier), PULL_CH links per
+// chunk, two chunks in flight; the lanes gather the staged links against the source's spike-bit ring. Only
+// this GPU's own memory is read, and no copy is multicast. The range's 16-byte aligned interior is copied;
+// its ragged head and tail (fewer than 4 links each) are loaded directly. Each lane sweeps its links in
+// increasing order, following the rows by their offsets (kept in shared memory), and adds a row's partial sum
+// into the row's shared slot when it leaves the row.
+constexpr int PULL_CH = 512;                        // links per staging chunk
+constexpr unsigned PULL_WAIT_POLLS = 1u << 22;      // polls of a chunk's mbarrier before it counts as lost
+
+struct alignas(16) PullStage {  // one per warp, in dynamic shared memory
+    uint32_t link[2][PULL_CH];
+    float w[2][PULL_CH];
+    unsigned long long bar[2];
+    long long sum[32];
+    int32_t ptr[33];
+    uint32_t uses[2];   // completions of each buffer's mbarrier so far (its next parity)
+    int32_t broken;     // a chunk was lost: the rest of the launch walks instead of staging
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void pull_stage_init(PullStage *st) {
+    if ((threadIdx.x & 31) == 0) {
+        for (int b = 0; b < 2; ++b) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&st->bar[b])) : "memory");
+            st->uses[b] = 0;
+        }
+        st->broken = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+}
+
+// Lane 0: chunk k of the aligned range [a0, a1) into buffer k & 1.
+__device__ __forceinline__ void pull_issue(PullStage *st, const ConnDev &C, int a0, int a1, int k) {
+    const int b = k & 1;
+    const int c0 = a0 + k * PULL_CH, c1 = min(a1, c0 + PULL_CH);
+    const uint32_t bytes = (uint32_t)(c1 - c0) * 4u;  // a multiple of 16: a0, a1 and PULL_CH are multiples of 4
+    const uint32_t bar = smem_u32(&st->bar[b]);
+    const uint32_t total = C.homogeneous ? bytes : 2u * bytes;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(total) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(st->link[b])),
+                 "l"(__cvta_generic_to_global(C.link + c0)), "r"(bytes), "r"(bar)
+                 : "memory");
+    if (!C.homogeneous)
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_u32(st->w[b])),
+                     "l"(__cvta_generic_to_global(C.w + c0)), "r"(bytes), "r"(bar)
+                     : "memory");
+}
+
+// Every lane: wait (bounded) until buffer b's chunk has landed; false if it did not within the limit (twice).
+__device__ __forceinline__ bool pull_wait(PullStage *st, int b) {
+    const uint32_t bar = smem_u32(&st->bar[b]);
+    const uint32_t parity = st->uses[b] & 1u;
+    for (unsigned it = 0; it < 2 * PULL_WAIT_POLLS; ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+struct PullSweep {
+    int q;          // the lane's current row (warp-relative)
+    long long part; // its partial sum in that row
+};
+
+__device__ __forceinline__ void pull_link(const ConnDev &C, PullStage *st, int32_t *err, PullSweep &sw, int l,
+                                          uint32_t rec, float w, long long n) {
+    while (l >= st->ptr[sw.q + 1]) {  // left the row (rows may be empty)
+        if (sw.part) atomicAdd(reinterpret_cast<unsigned long long *>(&st->sum[sw.q]), (unsigned long long)sw.part);
+        sw.part = 0;
+        ++sw.q;
+    }
+    const int d = (int)(rec >> 24), s = (int)(rec & 0xFFFFFFu);
+    if (d >= 1 && d <= C.src_bit_mask && s < C.src_n) {
+        const uint32_t word = __ldcg(C.src_bits + (size_t)((n - d) & C.src_bit_mask) * C.src_words + (s >> 5));
+        if ((word >> (s & 31)) & 1u) sw.part += C.homogeneous ? C.wfx : weight_fx(w, C.wscale);
+    } else {
+        atomicAdd(err + 1, 1);
+    }
+}
+
+// One connection's intake of the warp's nq rows (from neuron wbase); returns the lane's own row sum.
+template <bool INL>
+__device__ __forceinline__ long long pull_staged(const ConnDev &C, PullStage *st, int32_t *err, int wbase, int nq,
                                                  long long n) {
     const int lane = threadIdx.x & 31;
+    if (lane <= nq) st->ptr[lane] = __ldg(C.ptr + wbase + lane);
+    if (lane == 0 && nq == 32) st->ptr[32] = __ldg(C.ptr + wbase + 32);
+    st->sum[lane] = 0;
+    __syncwarp();
+    const int L0 = st->ptr[0], L1 = st->ptr[nq];
+    int a0 = (L0 + 3) & ~3, a1 = L1 & ~3;
+    if (a1 <= a0) a0 = a1 = L1;  // too short to stage: every link loaded directly
+    const int n_chunks = (a1 - a0 + PULL_CH - 1) / PULL_CH;
+    if (lane == 0) {
+        if (n_chunks > 0) pull_issue(st, C, a0, a1, 0);
+        if (n_chunks > 1) pull_issue(st, C, a0, a1, 1);
+    }
+    PullSweep sw{0, 0};
+    for (int l = L0 + lane; l < a0; l += 32)  // the head
+        pull_link(C, st, err, sw, l, __ldg(C.link + l), C.homogeneous ? 0.f : __ldg(C.w + l), n);
+    bool lost = false;
+    for (int k = 0; k < n_chunks; ++k) {
+        const int b = k & 1;
+        const int c0 = a0 + k * PULL_CH, c1 = min(a1, c0 + PULL_CH);
+        if (!lost && !pull_wait(st, b)) lost = true;
+        __syncwarp();
+        if (lane == 0) st->uses[b] += 1;
+        if (lost) {  // the chunk did not land in time: its links (and the rest) loaded directly
+            for (int l = c0 + lane; l < c1; l += 32)
+                pull_link(C, st, err, sw, l, __ldg(C.link + l), C.homogeneous ? 0.f : __ldg(C.w + l), n);
+            continue;
+        }
+        for (int l = c0 + lane; l < c1; l += 32)
+            pull_link(C, st, err, sw, l, st->link[b][l - c0], C.homogeneous ? 0.f : st->w[b][l - c0], n);
+        __syncwarp();  // every lane done with buffer b before it is refilled
+        if (lane == 0 && k + 2 < n_chunks) pull_issue(st, C, a0, a1, k + 2);
+    }
+    if (lost) {
+        if (lane == 0) {
+            atomicAdd(err + 5, 1);
+            st->broken = 1;
+        }
+    }
+    for (int l = max(a1, L0) + lane; l < L1; l += 32)  // the tail
+        pull_link(C, st, err, sw, l, __ldg(C.link + l), C.homogeneous ? 0.f : __ldg(C.w + l), n);
+    if (sw.part) atomicAdd(reinterpret_cast<unsigned long long *>(&st->sum[sw.q]), (unsigned long long)sw.part);
+    __syncwarp();
+    const long long mine = lane < nq ? st->sum[lane] : 0;
+    __syncwarp();
+    return mine;
+}
+
+template <bool INL>
+__device__ __forceinline__ long long pull_intake(const StepArgs &a, const PopDev &P, int first, int count,
+                                                 long long n, PullStage *stage) {
     const int wbase = first + (threadIdx.x & ~31);
     const int nq = min(32, first + count - wbase);
+    if (nq <= 0) return 0;
     long long mine = 0;
     for (int c = P.pull_first; c < P.pull_first + P.n_pull; ++c) {
         const ConnDev &C = pull_at<INL>(a, c);
-        for (int q = 0; q < nq; ++q) {
-            const int jq = wbase + q;
-            const int r0 = __ldg(C.ptr + jq), r1 = __ldg(C.ptr + jq + 1);
-            long long part = 0;
-            for (int l = r0 + lane; l < r1; l += 32) {
-                const uint32_t rec = __ldg(C.link + l);
-                const int d = (int)(rec >> 24), s = (int)(rec & 0xFFFFFFu);
-                if (d >= 1 && d <= C.src_bit_mask && s < C.src_n) {
-                    const uint32_t word =
-                        __ldcg(C.src_bits + (size_t)((n - d) & C.src_bit_mask) * C.src_words + (s >> 5));
-                    if ((word >> (s & 31)) & 1u)
-                        part += C.homogeneous ? C.wfx : weight_fx(__ldg(C.w + l), C.wscale);
-                } else {
-                    atomicAdd(a.err + 1, 1);
-                }
-            }
-            part = warp_sum64(part);
-            if (lane == q) mine += part;
-        }
+        if (stage != nullptr && C.staged && !stage->broken)
+            mine += pull_staged<INL>(C, stage, a.err, wbase, nq, n);
+        else
+            mine += pull_walk<INL>(C, a.err, wbase, nq, n);
     }
     return mine;
 }
@@ -611,7 +768,8 @@ __device__ __forceinline__ void cache_rows(const StepArgs &a, const PopDev &P, i
 // before the window, stored after it) and its row bounds are in s_cache; otherwise both come from memory.
 template <int NPB, bool INL, bool CACHED>
 __device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n, const int4 tile, int k, Neuron &nr,
-                                           const int *s_cache, Scratch<NPB> &sc, const SConn *s_conn) {
+                                           const int *s_cache, Scratch<NPB> &sc, const SConn *s_conn,
+                                           PullStage *stage) {
     int &s_cnt = sc.cnt;
     int *s_row = sc.row, *s_off = sc.off, *s_wsum = sc.wsum;
 
@@ -640,7 +798,7 @@ __device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n,
     if (model == 3) {  // N2B_MODEL_POISSON_SOURCE
         fire = live && draw(P, j, n, 1u) < P.fire_threshold;
     } else {
-        if (P.n_pull > 0) acc += pull_intake<INL>(a, P, tile.y, tile.z, n);
+        if (P.n_pull > 0) acc += pull_intake<INL>(a, P, tile.y, tile.z, n, stage);
         if (live) {
             *slot = 0;
             if (P.ext_len > 0) acc += (long long)poisson_count(P, draw(P, j, n, 0u)) * P.ext_wfx;
@@ -765,7 +923,7 @@ __device__ __forceinline__ void far_phase(const StepArgs &a, const long long n, 
 
 template <int NPB, bool INL>
 __device__ __forceinline__ void step_body(const StepArgs &a, const long long n, int k, Neuron *cached,
-                                          const int *s_cache, const SConn *s_conn) {
+                                          const int *s_cache, const SConn *s_conn, PullStage *stage) {
     __shared__ Scratch<NPB> sc;
     N2B_STAMP(a, k, 0);
     if (blockIdx.x == 0 && threadIdx.x == 0) {  // step n + 1's list and tile counter, list n's chunk counter
@@ -784,9 +942,9 @@ __device__ __forceinline__ void step_body(const StepArgs &a, const long long n, 
     const int t = blockIdx.x;
     if (t < a.n_tiles) {
         if (cached != nullptr)
-            tile_phase<NPB, INL, true>(a, n, tile_at<INL, NPB>(a, t), k, *cached, s_cache, sc, s_conn);
+            tile_phase<NPB, INL, true>(a, n, tile_at<INL, NPB>(a, t), k, *cached, s_cache, sc, s_conn, stage);
         else
-            tile_phase<NPB, INL, false>(a, n, tile_at<INL, NPB>(a, t), k, nr, nullptr, sc, s_conn);
+            tile_phase<NPB, INL, false>(a, n, tile_at<INL, NPB>(a, t), k, nr, nullptr, sc, s_conn, stage);
     }
     if (dyn) {
         __shared__ int s_tile;
@@ -796,7 +954,7 @@ __device__ __forceinline__ void step_body(const StepArgs &a, const long long n, 
             const int u = (int)gridDim.x + s_tile;  // every thread reads it before the tile's first barrier
             if (u >= a.n_tiles) break;
             if (threadIdx.x == 0) next = atomicAdd(claim, 1);
-            tile_phase<NPB, INL, false>(a, n, tile_at<INL, NPB>(a, u), k, nr, nullptr, sc, s_conn);
+            tile_phase<NPB, INL, false>(a, n, tile_at<INL, NPB>(a, u), k, nr, nullptr, sc, s_conn, stage);
         }
     }
     N2B_STAMP(a, k, 2);
@@ -804,13 +962,23 @@ __device__ __forceinline__ void step_body(const StepArgs &a, const long long n, 
     N2B_STAMP(a, k, 3);
 }
 
+// The warp's PullStage in the launch's dynamic shared memory (none without pull connections), initialised.
+__device__ __forceinline__ PullStage *warp_stage(const StepArgs &a) {
+    extern __shared__ __align__(128) unsigned char n2b_dyn_smem[];
+    if (!a.pull_staged) return nullptr;
+    PullStage *st = reinterpret_cast<PullStage *>(n2b_dyn_smem) + (threadIdx.x >> 5);
+    pull_stage_init(st);
+    return st;
+}
+
 // One step per launch: the launch boundary is the step's barrier.
 template <int NPB, bool INL>
-__global__ void __launch_bounds__(NPB) step_kernel(const __grid_constant__ StepArgs a) {
+__global__ void __launch_bounds__(NPB, 2) step_kernel(const __grid_constant__ StepArgs a) {
     __shared__ SConn s_tab[SMEM_CONNS];
     const SConn *s_conn = fill_conns<INL>(a, s_tab, a.n_push);
+    PullStage *stage = warp_stage(a);
     __syncthreads();
-    step_body<NPB, INL>(a, *a.step + a.offset, 0, nullptr, nullptr, s_conn);
+    step_body<NPB, INL>(a, *a.step + a.offset, 0, nullptr, nullptr, s_conn, stage);
 }
 
 __device__ __forceinline__ unsigned long long globaltimer() {
@@ -865,7 +1033,7 @@ __device__ __forceinline__ bool grid_sync(const StepArgs &a, unsigned k) {
 
 // A window of n_steps steps in one cooperative launch (every block resident), steps separated by grid_sync.
 template <int NPB, bool INL>
-__global__ void __launch_bounds__(NPB, 768 / NPB) persistent_kernel(const __grid_constant__ StepArgs a, const int n_steps) {
+__global__ void __launch_bounds__(NPB, 2) persistent_kernel(const __grid_constant__ StepArgs a, const int n_steps) {
     if (*(volatile unsigned *)(a.barrier + BAR_ABORT)) return;  // an earlier window gave up: nothing runs
     const long long n0 = *a.step;
     // the block's first tile stays in registers for the whole window
@@ -880,9 +1048,10 @@ __global__ void __launch_bounds__(NPB, 768 / NPB) persistent_kernel(const __grid
     cache_rows<NPB, INL>(a, P, j, live, s_cache);
     __shared__ SConn s_tab[SMEM_CONNS];
     const SConn *s_conn = fill_conns<INL>(a, s_tab, a.n_push);
+    PullStage *stage = warp_stage(a);
     __syncthreads();
     for (int k = 0; k < n_steps; ++k) {
-        step_body<NPB, INL>(a, n0 + k, k, &mine, s_cache, s_conn);
+        step_body<NPB, INL>(a, n0 + k, k, &mine, s_cache, s_conn, stage);
         if (!grid_sync(a, (unsigned)k)) break;
         N2B_STAMP(a, k, 4);
     }

@@ -156,6 +156,7 @@ struct n2b_net {
     int32_t persistent = 0;
     int32_t inl = 0;  // tables in the kernel parameters
     int32_t n_pops = 0;
+    size_t dyn_smem = 0;  // dynamic shared memory of the step kernels (the staged pull's buffers)
     Layout L{};
     char *ws = nullptr;
     n2b::StepArgs args{};
@@ -172,12 +173,12 @@ cudaError_t launch_one(n2b_net *net, int64_t n_steps, cudaStream_t s) {
         int32_t k = (int32_t)n_steps;
         void *args[] = {(void *)&net->args, (void *)&k};
         return cudaLaunchCooperativeKernel((const void *)n2b::persistent_kernel<NPB, INL>, dim3(net->grid), dim3(NPB),
-                                           args, 0, s);
+                                           args, net->dyn_smem, s);
     }
     n2b::StepArgs &a = net->args;
     for (int64_t k = 0; k < n_steps; ++k) {
         a.offset = (int32_t)k;
-        n2b::step_kernel<NPB, INL><<<net->grid, NPB, 0, s>>>(a);
+        n2b::step_kernel<NPB, INL><<<net->grid, NPB, net->dyn_smem, s>>>(a);
     }
     a.offset = 0;
     return cudaGetLastError();
@@ -202,18 +203,26 @@ cudaError_t launch_steps(n2b_net *net, int64_t n_steps, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// The step kernels' dynamic shared memory limit raised to `dyn` (the staged pull's buffers), and the persistent
+// kernel's resident blocks per SM with it.
 template <int NPB, bool INL>
-cudaError_t occupancy(int *per_sm) {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, n2b::persistent_kernel<NPB, INL>, NPB, 0);
+cudaError_t occupancy(int *per_sm, size_t dyn) {
+    cudaError_t e = cudaFuncSetAttribute((const void *)n2b::persistent_kernel<NPB, INL>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute((const void *)n2b::step_kernel<NPB, INL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)dyn);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, n2b::persistent_kernel<NPB, INL>, NPB, dyn);
 }
 
-int coresident_blocks(int32_t block, bool inl, int device, int *out) {
+int coresident_blocks(int32_t block, bool inl, int device, size_t dyn, int *out) {
     int per_sm = 0, sms = 0;
     cudaError_t e = cudaSuccess;
     switch (block) {
-        case 64: e = inl ? occupancy<64, true>(&per_sm) : occupancy<64, false>(&per_sm); break;
-        case 256: e = inl ? occupancy<256, true>(&per_sm) : occupancy<256, false>(&per_sm); break;
-        default: e = inl ? occupancy<128, true>(&per_sm) : occupancy<128, false>(&per_sm); break;
+        case 64: e = inl ? occupancy<64, true>(&per_sm, dyn) : occupancy<64, false>(&per_sm, dyn); break;
+        case 256: e = inl ? occupancy<256, true>(&per_sm, dyn) : occupancy<256, false>(&per_sm, dyn); break;
+        default: e = inl ? occupancy<128, true>(&per_sm, dyn) : occupancy<128, false>(&per_sm, dyn); break;
     }
     if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -314,6 +323,9 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
         D.src_bits = S.bits;
         D.has_split = C.mode == N2B_PUSH && C.split != nullptr;
         D.split = C.mode == N2B_PUSH ? C.split : nullptr;
+        // pull rows stream through shared memory by bulk copies, which need 16-byte aligned sources
+        D.staged = C.mode == N2B_PULL && (reinterpret_cast<uintptr_t>(C.link) & 15) == 0 &&
+                   (C.w == nullptr || (reinterpret_cast<uintptr_t>(C.w) & 15) == 0);
         return D;
     };
     for (int32_t p = 0; p < n_pops; ++p) {
@@ -370,10 +382,12 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     int want = (opt && opt->grid > 0) ? opt->grid
                                       : (persistent ? std::max(sms, L.n_tiles + sms / 2) : 2 * sms);
     int grid = std::max(L.n_tiles, want);
+    // the staged pull: a PullStage per warp in dynamic shared memory, when the network has pull connections
+    const size_t dyn = pull.empty() ? 0 : sizeof(n2b::PullStage) * (size_t)(block / 32);
+    int most = 0;
+    int rc2 = coresident_blocks(block, inl, device, dyn, &most);  // also raises the kernels' dynamic limit
+    if (rc2) return rc2;
     if (persistent) {
-        int most = 0;
-        int rc2 = coresident_blocks(block, inl, device, &most);
-        if (rc2) return rc2;
         if (most < 1) return fail(N2B_ECUDA, "the persistent kernel cannot be resident");
         grid = std::min(std::min(want, most), n2b::BAR_MAX_BLOCKS);
         grid = std::max(grid, 1);
@@ -385,6 +399,7 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     net->inl = inl;
     net->grid = grid;
     net->n_pops = n_pops;
+    net->dyn_smem = dyn;
     net->L = L;
     net->ws = ws;
     n2b::StepArgs &a = net->args;
@@ -405,6 +420,7 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     a.barrier = reinterpret_cast<unsigned *>(ws + L.barrier);
     a.bar_limit_ns = (opt && opt->barrier_limit_ns > 0) ? (unsigned long long)opt->barrier_limit_ns
                                                          : n2b::BAR_LIMIT_NS;
+    a.pull_staged = dyn > 0;
     a.n_pops = n_pops;
     a.n_push = L.n_push;
     if (inl) {
@@ -581,7 +597,7 @@ int static_scratch(void **out) {
 // The far links of step n - 1 (the work list the step kernel of step n would deliver), with no neuron update:
 // what is left of a run that stops after step n - 1.
 template <int NPB, bool INL>
-__global__ void __launch_bounds__(NPB) drain_kernel(const __grid_constant__ n2b::StepArgs a) {
+__global__ void __launch_bounds__(NPB, 2) drain_kernel(const __grid_constant__ n2b::StepArgs a) {
     // a persistent window that gave up at a grid barrier may have left its last step's tiles undone: its work
     // list is then incomplete, and nothing of it is delivered (error word 4 reports the stop)
     if (*(volatile unsigned *)(a.barrier + n2b::BAR_ABORT)) return;
