@@ -484,6 +484,61 @@ def run_batched(args, dev) -> dict:
             "tune_trials": report["trials"] if report else None, "build_s": build_s}
 
 
+def run_driven(args, dev) -> dict:
+    """A densely driven LIF population (naer2_b200.networks.driven: 2,000 Poisson inputs at 5 spikes/ms, 5M input
+    links into 10,000 neurons, a sparse recurrent part): the autotuner's push/pull choice per connection, and
+    events/s of the tuned configuration against the same network with every connection pushed."""
+    import torch
+
+    from naer2_b200.networks import driven
+    from naer2_b200.tune import autotune
+
+    sim = SIM_STEPS_PER_STEP
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def timed(modes: dict | None):
+        net, _ = driven.build(**driven.CONFIG, seed=1, device=dev)
+        chosen = None
+        if modes is None:
+            report = autotune(net, steps=200, warmup=50)
+            chosen = report["chosen"]
+        else:
+            net.tuned = modes
+        net.window = sim
+        net.run_steps(args.warmup * sim)
+        rt = net.runtime
+        ev0 = rt.counters()["events"]
+        ms = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            rt._enter()
+            e0.record(rt.stream)
+            net.run_steps(sim)
+            e1.record(rt.stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+        events = rt.counters()["events"] - ev0
+        spikes = rt.counters()["per_population"]
+        net.check()
+        out = {"value": events / (ms / 1e3), "us_per_sim_step": ms * 1e3 / (args.steps * sim),
+               "modes": list(rt.modes), "events_per_sim_step": events / (args.steps * sim),
+               "block": rt.opt.block, "persistent": bool(rt.opt.persistent), "tuned": chosen,
+               "pull_staged_error_words": rt.status()[5], "spikes": spikes}
+        net.close()
+        torch.cuda.empty_cache()
+        return out
+
+    tuned = timed(None)
+    push = timed({})
+    return {"metric": METRIC, "value": tuned["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded draws on the GPU)",
+            "config": {"workload": "driven_dense_input", **driven.CONFIG, "sim_steps_per_step": sim,
+                       "l2": "flushed before every timed step (256 MiB write)"},
+            "tuned": tuned, "all_push": push, "tuned_over_all_push": tuned["value"] / push["value"]}
+
+
 def _summarise_choices(choices: list) -> dict | None:
     if not choices:
         return None
@@ -666,10 +721,11 @@ def main() -> int:
     ap.add_argument("--impl", default="naer2_b200", choices=["naer2_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-workloads", action="store_true", help="the headline workload alone (no sub-objects)")
-    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4],
+    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5],
                     help="2: the PD14 microcircuit (the headline, default); 1: Brunel model A at config 1's size; "
                          "3: 64 uneven Brunel instances batched against one at a time; 4: BPTT of the recurrent "
-                         "LIF layer (training step against the plain forward)")
+                         "LIF layer (training step against the plain forward); 5: a densely driven population "
+                         "(the autotuner's push/pull choice against all push)")
     ap.add_argument("--instances", type=int, default=64, help="config 3: instances")
     ap.add_argument("--no-tune", dest="tune", action="store_false", help="config 3: skip the autotuner")
     ap.add_argument("--transpiled", action="store_true",
@@ -699,10 +755,10 @@ def main() -> int:
             raise SystemExit("--transpiled runs config 1 on one GPU")
         print(json.dumps(run_transpiled(args, dev)))
         return 0
-    if args.config in (3, 4):
+    if args.config in (3, 4, 5):
         if world > 1:
             raise SystemExit(f"config {args.config} runs on one GPU")
-        print(json.dumps({3: run_batched, 4: run_bptt}[args.config](args, dev)))
+        print(json.dumps({3: run_batched, 4: run_bptt, 5: run_driven}[args.config](args, dev)))
         return 0
     if world > 1:
         import datetime
@@ -715,6 +771,7 @@ def main() -> int:
             "brunel_A_config1": compact(run_plain("brunel_A_config1", args, dev, 0, 1, cpu=False)),
             "batched_config3": compact(run_batched(args, dev)),
             "bptt_config4": compact(run_bptt(args, dev)),
+            "driven_dense_input": compact(run_driven(args, dev)),
         }
     if rank == 0:
         print(json.dumps(line))

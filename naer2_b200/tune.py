@@ -58,8 +58,10 @@ def _trial(net, steps: int, warmup: int) -> tuple[float, dict]:
     return ms * 1e3 / steps, {"events": c1["events"] - c0["events"], "spikes": spikes}
 
 
-def pull_candidates(net, spikes_per_step: list, pull_factor: float = 0.25) -> dict:
-    """Connection id -> "pull" where streaming all its links costs fewer bytes than push's scatter x factor."""
+def pull_candidates(net, spikes_per_step: list, pull_factor: float = 4.0) -> dict:
+    """Connection id -> "pull" where streaming all its links (5 B each) costs fewer bytes than push's scatter
+    (9 B per event) x factor: a scattered event costs an L2 reduction, several times a streamed byte's share,
+    so pull is worth measuring up to a few times push's bytes; the trials decide."""
     index = {id(p): k for k, p in enumerate(net.populations)}
     out = {}
     for c in net.connections:
@@ -76,7 +78,7 @@ def pull_candidates(net, spikes_per_step: list, pull_factor: float = 0.25) -> di
 
 
 def autotune(net, steps: int = 300, warmup: int = 100, blocks=(128, 256), persistent=(True, False),
-             grids=(None,), pull_factor: float = 0.25, verbose: bool = False) -> dict:
+             grids=(None,), pull_factor: float = 4.0, verbose: bool = False) -> dict:
     """Measure the candidates, keep the fastest; returns the report (every trial's us per step)."""
     if net.device is None or net.device.type != "cuda":
         raise RuntimeError("autotune needs the network on a CUDA device")

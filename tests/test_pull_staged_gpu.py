@@ -92,3 +92,22 @@ def test_unaligned_rows_walk_and_match_the_staged_path(cuda):
         assert np.array_equal(x, y)
     for x, y in zip(va, vb):
         assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
+
+
+def test_autotuner_pulls_the_dense_input_and_matches_oracle(cuda):
+    """The densely driven population (5M input links, ~39% of the inputs spiking per step): the autotuner's
+    measured choice pulls the input connections and pushes the sparse recurrent ones; the tuned network
+    equals the oracle bit for bit."""
+    from naer2_b200.networks import driven
+    from naer2_b200.tune import autotune
+
+    net, pops = driven.build(**driven.CONFIG, seed=3, device=cuda)
+    report = autotune(net, steps=200, warmup=50)
+    inputs = [c for c in net.connections if c._source is pops["in"]]
+    assert report["chosen"]["pull"] > 0, report
+    assert all(net.tuned.get(id(c)) == "pull" for c in inputs), report
+    assert all(net.tuned.get(id(c), "push") == "push" for c in net.connections if c._source is not pops["in"])
+    gr, orr, gs, os_, cnt, ev = run_both(net, 300, persistent=net.persistent)
+    assert sum(r.sum() for r in gr[1:]) > 1000  # the driven neurons fire
+    assert_identical(gr, orr, gs, os_)
+    assert cnt["events"] == ev
