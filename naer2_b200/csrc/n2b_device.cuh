@@ -842,33 +842,37 @@ __device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n,
     }
 }
 
-// Two items of step m's work list, one link of each per thread: both link loads in flight before the reductions.
-// it0 is a listed item; it1 is one only if `two` (otherwise it may be anything past the list's end, never
-// dereferenced: it is replaced by an empty item of connection 0 before its connection is looked up).
-template <bool INL>
-__device__ __forceinline__ void far_pair(const StepArgs &a, const SConn *s_conn, const int4 it0, const int4 it1_in,
-                                         const bool two, const long long m) {
-    const int4 it1 = two ? it1_in : make_int4(0, 0, 0, 0);
-    const int l0 = it0.y + (int)threadIdx.x, l1 = it1.y + (int)threadIdx.x;
-    const SConn C0 = conn_view(a, s_conn, it0.x);
-    const SConn C1 = conn_view(a, s_conn, it1.x);
-    const bool h0 = l0 < it0.z, h1 = two && l1 < it1.z;
-    const uint32_t rec0 = h0 ? __ldg(C0.link + l0) : 0u;
-    const uint32_t rec1 = h1 ? __ldg(C1.link + l1) : 0u;
-    const float w0 = h0 ? link_weight(C0, l0) : 0.f;
-    const float w1 = h1 ? link_weight(C1, l1) : 0.f;
-    if (h0) deliver_rec(a, C0, rec0, w0, m, 2);
-    if (h1) deliver_rec(a, C1, rec1, w1, m, 2);
+// FG items of step m's work list, one link of each per thread: every link load in flight before the reductions.
+// it[0] is a listed item; it[g] is one only if g < valid (otherwise it may be anything past the list's end,
+// never dereferenced: it is replaced by an empty item of connection 0 before its connection is looked up).
+template <bool INL, int FG>
+__device__ __forceinline__ void far_group(const StepArgs &a, const SConn *s_conn, const int4 (&it_in)[FG],
+                                          const int valid, const long long m) {
+    uint32_t rec[FG];
+    float w[FG];
+    bool h[FG];
+#pragma unroll
+    for (int g = 0; g < FG; ++g) {
+        const int4 it = g < valid ? it_in[g] : make_int4(0, 0, 0, 0);
+        const int l = it.y + (int)threadIdx.x;
+        const SConn C = conn_view(a, s_conn, it.x);
+        h[g] = g < valid && l < it.z;
+        rec[g] = h[g] ? __ldg(C.link + l) : 0u;
+        w[g] = h[g] ? link_weight(C, l) : 0.f;
+    }
+#pragma unroll
+    for (int g = 0; g < FG; ++g)
+        if (h[g]) deliver_rec(a, conn_view(a, s_conn, it_in[g].x), rec[g], w[g], m, 2);
 }
 
-// 5. the far links of step n - 1: items of NPB links, one link per thread, two items at a time. With every
-// block holding tiles (no tile-free blocks), the first ~80% of the list is split statically (the next pair's
-// items loaded under this pair's links) and, for long lists, the rest is taken in chunks of FAR_CHUNK pairs by whichever
-// blocks get there first (one claim per chunk on the step's counter), so that blocks whose tiles ran late
-// take less of it. With tile-free blocks, those split the whole list statically.
+// 5. the far links of step n - 1: items of NPB links, one link per thread, FG items at a time (the next
+// round's items loaded under this round's links). With every block holding tiles (no tile-free blocks), the
+// first ~80% of the list is split statically and, for long lists, the rest is taken in chunks of FAR_CHUNK
+// rounds by whichever blocks get there first (one claim per chunk on the step's counter), so that blocks whose
+// tiles ran late take less of it. With tile-free blocks, those split the whole list statically.
 constexpr int FAR_CHUNK = 4;
 
-template <int NPB, bool INL>
+template <int NPB, bool INL, int FG>
 __device__ __forceinline__ void far_phase(const StepArgs &a, const long long n, const SConn *s_conn) {
     const long long m = n - 1;
     const int lst = (int)(((m % 3) + 3) % 3);
@@ -880,22 +884,31 @@ __device__ __forceinline__ void far_phase(const StepArgs &a, const long long n, 
     if (split && (int)blockIdx.x < a.n_tiles) return;
     const int G = split ? free_blocks : (int)gridDim.x;
     const int me = split ? (int)blockIdx.x - a.n_tiles : (int)blockIdx.x;
-    // the first two items loaded with the count, not after it (an item past the count is read, then ignored)
+    // the first round's items loaded with the count, not after it (an item past the count is read, then ignored)
     int i = G - 1 - me;
-    int4 pre0 = i < a.item_cap ? __ldcg(list + i) : make_int4(0, 0, 0, 0);
-    int4 pre1 = i + G < a.item_cap ? __ldcg(list + i + G) : make_int4(0, 0, 0, 0);
+    int4 pre[FG];
+#pragma unroll
+    for (int g = 0; g < FG; ++g) pre[g] = i + g * G < a.item_cap ? __ldcg(list + i + g * G) : make_int4(0, 0, 0, 0);
     const int count = min(__ldcg(a.item_count + lst), a.item_cap);  // final: appended before the last barrier
-    // the static part: whole rounds of 2G items covering ~80% of the list; all of it for tile-free blocks and
+    // the static part: whole rounds of FG G items covering ~80% of the list; all of it for tile-free blocks and
     // for lists under 16 items per block, where the chunk claims would cost more than the imbalance
-    const int stat = (split || count < 16 * G) ? count : (count * 4 / 5) / (2 * G) * (2 * G);
-    for (; i < stat; i += 2 * G) {
-        const int4 it0 = pre0, it1 = pre1;
-        const bool two = i + G < stat;
-        if (i + 2 * G < stat) {
-            pre0 = __ldcg(list + i + 2 * G);
-            pre1 = i + 3 * G < stat ? __ldcg(list + i + 3 * G) : make_int4(0, 0, 0, 0);
+    const int stat = (split || count < 16 * G) ? count : (count * 4 / 5) / (FG * G) * (FG * G);
+    for (; i < stat; i += FG * G) {
+        int4 it[FG];
+        int valid = 0;
+#pragma unroll
+        for (int g = 0; g < FG; ++g) {
+            it[g] = pre[g];
+            valid += i + g * G < stat;
         }
-        far_pair<INL>(a, s_conn, it0, it1, two, m);
+        if (i + FG * G < stat) {
+#pragma unroll
+            for (int g = 0; g < FG; ++g) {
+                const int q = i + (FG + g) * G;
+                pre[g] = q < stat ? __ldcg(list + q) : make_int4(0, 0, 0, 0);
+            }
+        }
+        far_group<INL, FG>(a, s_conn, it, valid, m);
     }
     if (stat >= count) return;  // the same for every thread of the block
     __shared__ int s_chunk;
@@ -903,25 +916,28 @@ __device__ __forceinline__ void far_phase(const StepArgs &a, const long long n, 
     for (;;) {
         if (threadIdx.x == 0) s_chunk = atomicAdd(claim, 1);
         __syncthreads();
-        const int c0 = stat + s_chunk * (2 * FAR_CHUNK);
+        const int c0 = stat + s_chunk * (FG * FAR_CHUNK);
         __syncthreads();  // every thread has read s_chunk before the next claim overwrites it
         if (c0 >= count) break;
-        const int c1 = min(count, c0 + 2 * FAR_CHUNK);
-        int4 p0 = __ldcg(list + c0);
-        int4 p1 = c0 + 1 < c1 ? __ldcg(list + c0 + 1) : make_int4(0, 0, 0, 0);
-        for (int b = c0; b < c1; b += 2) {
-            const int4 it0 = p0, it1 = p1;
-            const bool two = b + 1 < c1;
-            if (b + 2 < c1) {
-                p0 = __ldcg(list + b + 2);
-                p1 = b + 3 < c1 ? __ldcg(list + b + 3) : make_int4(0, 0, 0, 0);
+        const int c1 = min(count, c0 + FG * FAR_CHUNK);
+        int4 p[FG];
+#pragma unroll
+        for (int g = 0; g < FG; ++g) p[g] = c0 + g < c1 ? __ldcg(list + c0 + g) : make_int4(0, 0, 0, 0);
+        for (int b = c0; b < c1; b += FG) {
+            int4 it[FG];
+#pragma unroll
+            for (int g = 0; g < FG; ++g) it[g] = p[g];
+            const int valid = min(FG, c1 - b);
+            if (b + FG < c1) {
+#pragma unroll
+                for (int g = 0; g < FG; ++g) p[g] = b + FG + g < c1 ? __ldcg(list + b + FG + g) : make_int4(0, 0, 0, 0);
             }
-            far_pair<INL>(a, s_conn, it0, it1, two, m);
+            far_group<INL, FG>(a, s_conn, it, valid, m);
         }
     }
 }
 
-template <int NPB, bool INL>
+template <int NPB, bool INL, int FG>
 __device__ __forceinline__ void step_body(const StepArgs &a, const long long n, int k, Neuron *cached,
                                           const int *s_cache, const SConn *s_conn, PullStage *stage) {
     __shared__ Scratch<NPB> sc;
@@ -958,7 +974,7 @@ __device__ __forceinline__ void step_body(const StepArgs &a, const long long n, 
         }
     }
     N2B_STAMP(a, k, 2);
-    far_phase<NPB, INL>(a, n, s_conn);
+    far_phase<NPB, INL, FG>(a, n, s_conn);
     N2B_STAMP(a, k, 3);
 }
 
@@ -978,7 +994,7 @@ __global__ void __launch_bounds__(NPB, 2) step_kernel(const __grid_constant__ St
     const SConn *s_conn = fill_conns<INL>(a, s_tab, a.n_push);
     PullStage *stage = warp_stage(a);
     __syncthreads();
-    step_body<NPB, INL>(a, *a.step + a.offset, 0, nullptr, nullptr, s_conn, stage);
+    step_body<NPB, INL, 2>(a, *a.step + a.offset, 0, nullptr, nullptr, s_conn, stage);
 }
 
 __device__ __forceinline__ unsigned long long globaltimer() {
@@ -991,14 +1007,18 @@ __device__ __forceinline__ void red_release_add(unsigned *p, unsigned v) {
     asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned *p) {
     unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
 
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+
 // Grid-wide barrier k (0, 1, ...) of a cooperative launch: every block adds 1 to one counter with release
-// semantics (its writes before its arrival) and waits, with acquire loads, until the counter holds
+// semantics (its writes before its arrival) and polls, with relaxed loads and one acquire fence at the end,
+// until the counter holds
 // (k + 1) * gridDim.x -- the counter starts each launch at 0 (advance_kernel clears it after every launch).
 // Every wait is bounded (a.bar_limit_ns, BAR_LIMIT_NS by default): a timeout sets error word 4 and the abort
 // word, and the kernel winds down instead of hanging. Returns false once aborted. A wait ends in every case:
@@ -1014,7 +1034,12 @@ __device__ __forceinline__ bool grid_sync(const StepArgs &a, unsigned k) {
         int ok = 1;
         unsigned long long t0 = 0;
         for (int spin = 0;; ++spin) {
-            if ((int)(ld_acquire(bar + BAR_COUNT) - target) >= 0) break;
+            // relaxed polls, one acquire fence once the count is there (a fence-based acquire pattern: cheaper
+            // than an acquire load per poll)
+            if ((int)(ld_relaxed(bar + BAR_COUNT) - target) >= 0) {
+                fence_acq_rel();
+                break;
+            }
             if (*(volatile unsigned *)(bar + BAR_ABORT)) { ok = 0; break; }
             if (spin == 0) t0 = globaltimer();
             else if (globaltimer() - t0 > a.bar_limit_ns) {
@@ -1032,8 +1057,12 @@ __device__ __forceinline__ bool grid_sync(const StepArgs &a, unsigned k) {
 }
 
 // A window of n_steps steps in one cooperative launch (every block resident), steps separated by grid_sync.
-template <int NPB, bool INL>
-__global__ void __launch_bounds__(NPB, 2) persistent_kernel(const __grid_constant__ StepArgs a, const int n_steps) {
+// DENSE: three blocks per SM (registers capped for it; far items two at a time), for networks with more tiles
+// than two blocks per SM hold -- every tile then keeps a block of its own; otherwise two blocks per SM and far
+// items four at a time.
+template <int NPB, bool INL, bool DENSE>
+__global__ void __launch_bounds__(NPB, DENSE ? 3 : 2)
+    persistent_kernel(const __grid_constant__ StepArgs a, const int n_steps) {
     if (*(volatile unsigned *)(a.barrier + BAR_ABORT)) return;  // an earlier window gave up: nothing runs
     const long long n0 = *a.step;
     // the block's first tile stays in registers for the whole window
@@ -1051,7 +1080,7 @@ __global__ void __launch_bounds__(NPB, 2) persistent_kernel(const __grid_constan
     PullStage *stage = warp_stage(a);
     __syncthreads();
     for (int k = 0; k < n_steps; ++k) {
-        step_body<NPB, INL>(a, n0 + k, k, &mine, s_cache, s_conn, stage);
+        step_body<NPB, INL, DENSE ? 2 : 4>(a, n0 + k, k, &mine, s_cache, s_conn, stage);
         if (!grid_sync(a, (unsigned)k)) break;
         N2B_STAMP(a, k, 4);
     }

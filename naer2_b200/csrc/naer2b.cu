@@ -155,6 +155,7 @@ struct n2b_net {
     int32_t grid = 0;
     int32_t persistent = 0;
     int32_t inl = 0;  // tables in the kernel parameters
+    int32_t dense = 0;  // persistent windows: the three-blocks-per-SM kernel (more tiles than two per SM hold)
     int32_t n_pops = 0;
     size_t dyn_smem = 0;  // dynamic shared memory of the step kernels (the staged pull's buffers)
     Layout L{};
@@ -172,8 +173,9 @@ cudaError_t launch_one(n2b_net *net, int64_t n_steps, cudaStream_t s) {
     if (net->persistent) {
         int32_t k = (int32_t)n_steps;
         void *args[] = {(void *)&net->args, (void *)&k};
-        return cudaLaunchCooperativeKernel((const void *)n2b::persistent_kernel<NPB, INL>, dim3(net->grid), dim3(NPB),
-                                           args, net->dyn_smem, s);
+        const void *kern = net->dense ? (const void *)n2b::persistent_kernel<NPB, INL, true>
+                                      : (const void *)n2b::persistent_kernel<NPB, INL, false>;
+        return cudaLaunchCooperativeKernel(kern, dim3(net->grid), dim3(NPB), args, net->dyn_smem, s);
     }
     n2b::StepArgs &a = net->args;
     for (int64_t k = 0; k < n_steps; ++k) {
@@ -205,25 +207,29 @@ cudaError_t launch_steps(n2b_net *net, int64_t n_steps, cudaStream_t s) {
 
 // The step kernels' dynamic shared memory limit raised to `dyn` (the staged pull's buffers), and the persistent
 // kernel's resident blocks per SM with it.
-template <int NPB, bool INL>
+template <int NPB, bool INL, bool DENSE>
 cudaError_t occupancy(int *per_sm, size_t dyn) {
-    cudaError_t e = cudaFuncSetAttribute((const void *)n2b::persistent_kernel<NPB, INL>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    const void *pk = (const void *)n2b::persistent_kernel<NPB, INL, DENSE>;
+    cudaError_t e = cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute((const void *)n2b::step_kernel<NPB, INL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)dyn);
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, n2b::persistent_kernel<NPB, INL>, NPB, dyn);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, pk, NPB, dyn);
 }
 
-int coresident_blocks(int32_t block, bool inl, int device, size_t dyn, int *out) {
-    int per_sm = 0, sms = 0;
-    cudaError_t e = cudaSuccess;
+template <bool DENSE>
+cudaError_t occupancy_of(int32_t block, bool inl, size_t dyn, int *per_sm) {
     switch (block) {
-        case 64: e = inl ? occupancy<64, true>(&per_sm, dyn) : occupancy<64, false>(&per_sm, dyn); break;
-        case 256: e = inl ? occupancy<256, true>(&per_sm, dyn) : occupancy<256, false>(&per_sm, dyn); break;
-        default: e = inl ? occupancy<128, true>(&per_sm, dyn) : occupancy<128, false>(&per_sm, dyn); break;
+        case 64: return inl ? occupancy<64, true, DENSE>(per_sm, dyn) : occupancy<64, false, DENSE>(per_sm, dyn);
+        case 256: return inl ? occupancy<256, true, DENSE>(per_sm, dyn) : occupancy<256, false, DENSE>(per_sm, dyn);
+        default: return inl ? occupancy<128, true, DENSE>(per_sm, dyn) : occupancy<128, false, DENSE>(per_sm, dyn);
     }
+}
+
+int coresident_blocks(int32_t block, bool inl, bool dense, int device, size_t dyn, int *out) {
+    int per_sm = 0, sms = 0;
+    cudaError_t e = dense ? occupancy_of<true>(block, inl, dyn, &per_sm) : occupancy_of<false>(block, inl, dyn, &per_sm);
     if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
@@ -385,8 +391,18 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     // the staged pull: a PullStage per warp in dynamic shared memory, when the network has pull connections
     const size_t dyn = pull.empty() ? 0 : sizeof(n2b::PullStage) * (size_t)(block / 32);
     int most = 0;
-    int rc2 = coresident_blocks(block, inl, device, dyn, &most);  // also raises the kernels' dynamic limit
+    int rc2 = coresident_blocks(block, inl, false, device, dyn, &most);  // also raises the kernels' dynamic limit
     if (rc2) return rc2;
+    bool dense = false;
+    if (persistent && L.n_tiles > most) {  // more tiles than blocks: the denser kernel, if it holds more
+        int most3 = 0;
+        rc2 = coresident_blocks(block, inl, true, device, dyn, &most3);
+        if (rc2) return rc2;
+        if (most3 > most) {
+            dense = true;
+            most = most3;
+        }
+    }
     if (persistent) {
         if (most < 1) return fail(N2B_ECUDA, "the persistent kernel cannot be resident");
         grid = std::min(std::min(want, most), n2b::BAR_MAX_BLOCKS);
@@ -400,6 +416,7 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     net->grid = grid;
     net->n_pops = n_pops;
     net->dyn_smem = dyn;
+    net->dense = dense;
     net->L = L;
     net->ws = ws;
     n2b::StepArgs &a = net->args;
@@ -604,7 +621,7 @@ __global__ void __launch_bounds__(NPB, 2) drain_kernel(const __grid_constant__ n
     __shared__ n2b::SConn s_tab[n2b::SMEM_CONNS];
     const n2b::SConn *s_conn = n2b::fill_conns<INL>(a, s_tab, a.n_push);
     __syncthreads();
-    n2b::far_phase<NPB, INL>(a, *a.step, s_conn);
+    n2b::far_phase<NPB, INL, 2>(a, *a.step, s_conn);
 }
 
 template <bool INL>
