@@ -872,15 +872,26 @@ __device__ __forceinline__ void far_group(const StepArgs &a, const SConn *s_conn
 // tiles ran late take less of it. With tile-free blocks, those split the whole list statically.
 constexpr int FAR_CHUNK = 4;
 
+constexpr int FAR_SPLIT_ROUNDS = 2;  // tile-free blocks take a list alone when it is at most this many rounds
+
+// The length of step m's work list (final once step m's barrier has passed).
+__device__ __forceinline__ int far_count(const StepArgs &a, const long long m) {
+    return min(__ldcg(a.item_count + (int)(((m % 3) + 3) % 3)), a.item_cap);
+}
+
 template <int NPB, bool INL, int FG>
-__device__ __forceinline__ void far_phase(const StepArgs &a, const long long n, const SConn *s_conn) {
+__device__ __forceinline__ void far_phase(const StepArgs &a, const long long n, const SConn *s_conn,
+                                          const int count) {
     const long long m = n - 1;
     const int lst = (int)(((m % 3) + 3) % 3);
     const int4 *list = a.items + (size_t)lst * (size_t)a.item_cap;
-    // the items go to the blocks without a tile when there are enough of them (a quarter of the grid), else to
-    // every block, the tile-free ones first
+    // the items go to the blocks without a tile when there are enough of them (a quarter of the grid) or when
+    // they take them in at most FAR_SPLIT_ROUNDS rounds -- the tile blocks' step then ends with its tile --,
+    // else to every block, the tile-free ones first. `count` was loaded at the step's start (under the tile's
+    // loads), so every block decides alike without a load in its tile's chain.
     const int free_blocks = (int)gridDim.x - a.n_tiles;
-    const bool split = free_blocks >= (int)gridDim.x / 4 && free_blocks > 0;
+    const bool split = free_blocks > 0 &&
+                       (free_blocks >= (int)gridDim.x / 4 || count <= free_blocks * FG * FAR_SPLIT_ROUNDS);
     if (split && (int)blockIdx.x < a.n_tiles) return;
     const int G = split ? free_blocks : (int)gridDim.x;
     const int me = split ? (int)blockIdx.x - a.n_tiles : (int)blockIdx.x;
@@ -889,7 +900,6 @@ __device__ __forceinline__ void far_phase(const StepArgs &a, const long long n, 
     int4 pre[FG];
 #pragma unroll
     for (int g = 0; g < FG; ++g) pre[g] = i + g * G < a.item_cap ? __ldcg(list + i + g * G) : make_int4(0, 0, 0, 0);
-    const int count = min(__ldcg(a.item_count + lst), a.item_cap);  // final: appended before the last barrier
     // the static part: whole rounds of FG G items covering ~80% of the list; all of it for tile-free blocks and
     // for lists under 16 items per block, where the chunk claims would cost more than the imbalance
     const int stat = (split || count < 16 * G) ? count : (count * 4 / 5) / (FG * G) * (FG * G);
@@ -942,6 +952,7 @@ __device__ __forceinline__ void step_body(const StepArgs &a, const long long n, 
                                           const int *s_cache, const SConn *s_conn, PullStage *stage) {
     __shared__ Scratch<NPB> sc;
     N2B_STAMP(a, k, 0);
+    const int far_n = far_count(a, n - 1);  // in flight under the tile
     if (blockIdx.x == 0 && threadIdx.x == 0) {  // step n + 1's list and tile counter, list n's chunk counter
         atomicExch(a.item_count + (int)((n + 1) % 3), 0);
         atomicExch(a.tile_claim + (int)((n + 1) % 3), 0);
@@ -974,7 +985,7 @@ __device__ __forceinline__ void step_body(const StepArgs &a, const long long n, 
         }
     }
     N2B_STAMP(a, k, 2);
-    far_phase<NPB, INL, FG>(a, n, s_conn);
+    far_phase<NPB, INL, FG>(a, n, s_conn, far_n);
     N2B_STAMP(a, k, 3);
 }
 

@@ -621,7 +621,7 @@ __global__ void __launch_bounds__(NPB, 2) drain_kernel(const __grid_constant__ n
     __shared__ n2b::SConn s_tab[n2b::SMEM_CONNS];
     const n2b::SConn *s_conn = n2b::fill_conns<INL>(a, s_tab, a.n_push);
     __syncthreads();
-    n2b::far_phase<NPB, INL, 2>(a, *a.step, s_conn);
+    n2b::far_phase<NPB, INL, 2>(a, *a.step, s_conn, n2b::far_count(a, *a.step - 1));
 }
 
 template <bool INL>

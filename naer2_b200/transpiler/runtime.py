@@ -86,79 +86,166 @@ class EdgePlan:
         return torch.full((n_links,), float(v.item() if isinstance(v, torch.Tensor) else v), dtype=torch.float32)
 
 
+def plan_of(net) -> dict:
+    """The transpiled form of a network, everything its step kernels need and nothing of its Python model classes:
+    per population its CUDA source, the Params fields with the values of the scalar ones, its state attributes
+    (name -> "float" / "int" / "bool"), size, seed and spike-ring depth; per incoming connection (in order) its
+    source population, pull CSR (int32 ptr, uint32 link words) and per-link edge arrays (pull order) with the
+    pull permutation. JitRuntime builds from it; save_plan / load_plan keep it in a file, so that a network can
+    be transpiled where its model classes are and stepped where only the plan is."""
+    dev = net.device if net.device is not None else torch.device("cpu")
+    dt = float(net.resolution)
+    pops = list(net.populations)
+    index = {id(p): k for k, p in enumerate(pops)}
+    words = [(len(p.shape) + 31) // 32 for p in pops]
+    # spike-bit ring depth of each population: above every delay of its outgoing connections
+    steps_of, max_out = {}, [1] * len(pops)
+    for c in net.connections:
+        topo = c.fabric.topology
+        steps = delay_steps(c.fabric.value("delay"), len(topo), dt, device=topo.target_indices.device)
+        steps_of[id(c)] = steps
+        if len(topo):
+            s = index[id(c._source)]
+            max_out[s] = max(max_out[s], int(steps.max()))
+    depth = [max(2, 1 << int(np.ceil(np.log2(m + 1)))) for m in max_out]
+    exact = bool(getattr(net, "exact", False))
+    plan = {"dt": dt, "exact": exact, "pops": []}
+    for k, p in enumerate(pops):
+        node = p.node
+        incoming = []
+        conns = [c for c in net.connections if c._target is p]
+        site = 0
+        for c in conns:
+            port = c._target_port or "receive"
+            hook = node.receive.get(port)
+            if hook is None:
+                raise ValueError(f"{p!r} has no receive port {port!r}")
+            ep = EdgePlan(c, hook)
+            dyn = [h for h, real in ep.recv.items() if real in ep.per_link]
+            stat = {h: ep.static[real] for h, real in ep.recv.items() if real not in ep.per_link}
+            ctx = hook_context(p, hook, dyn, stat, site_base=site)
+            site += 32
+            inc = {"receive": (hook.ast, ctx), "edge_dynamic": ep.per_link, "edge_written": ep.written,
+                   "alias": {h: real for h, real in ep.recv.items() if real in ep.per_link and h != real},
+                   "forward": None, "backward": None, "conn": c, "plan": ep}
+            for kind in ("forward", "backward"):
+                eh = getattr(ep, kind)
+                if eh is not None:
+                    inc[kind] = (eh.ast, edge_hook_context(p, eh, ep.per_link, ep.static))
+            incoming.append(inc)
+        hooks = {"update": (node.update.ast, hook_context(p, node.update, site_base=site)),
+                 "send": (node.send.ast, hook_context(p, node.send, site_base=site + 32))}
+        src, fields = build_source(type(p.instance).__name__, dict(p.dynamic_attrs), hooks, incoming,
+                                   exact=exact, n=len(p.shape))
+        attrs = {a: ("bool" if py is bool else "int" if py is int else "float") for a, py in p.dynamic_attrs.items()}
+        entry = {"name": type(p.instance).__name__, "n": len(p.shape), "words": words[k], "depth": depth[k],
+                 "seed": int(p.seed) & 0xFFFFFFFFFFFFFFFF, "source": src,
+                 "fields": [(name, ctype) for name, ctype, _ in fields], "attrs": attrs, "conns": []}
+        for inc in incoming:
+            c = inc["conn"]
+            topo = c.fabric.topology
+            ptr, link, perm = pull_form(topo, steps_of[id(c)], len(p.shape))
+            ep = inc["plan"]
+            per_link = {}
+            for e in ep.per_link:
+                v = ep.initial(c, e, len(topo))
+                per_link[e] = (v[perm.cpu()] if v.numel() else torch.zeros(0)).to(torch.float32)
+            entry["conns"].append({"src": index[id(c._source)], "ptr": ptr.to(torch.int32).cpu(),
+                                   "link": link.to(torch.int32).cpu(), "perm": perm.cpu(), "per_link": per_link,
+                                   "written": list(ep.written), "conn_id": id(c)})
+        plan["pops"].append(entry)
+    plan["device"] = dev
+    return plan
+
+
+def save_plan(plan: dict, path) -> None:
+    """A plan in one .npz file: its structure as JSON, its arrays beside it."""
+    import json
+
+    arrays, meta = {}, {"dt": plan["dt"], "exact": plan["exact"], "pops": []}
+    for k, p in enumerate(plan["pops"]):
+        m = {key: p[key] for key in ("name", "n", "words", "depth", "seed", "source", "fields", "attrs")}
+        m["conns"] = []
+        for ci, c in enumerate(p["conns"]):
+            for key in ("ptr", "link", "perm"):
+                arrays[f"p{k}_c{ci}_{key}"] = c[key].numpy()
+            for e, v in c["per_link"].items():
+                arrays[f"p{k}_c{ci}_e_{e}"] = v.numpy()
+            m["conns"].append({"src": c["src"], "per_link": list(c["per_link"]), "written": c["written"]})
+        meta["pops"].append(m)
+    arrays["plan_json"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
+    np.savez_compressed(path, **arrays)
+
+
+def load_plan(path) -> dict:
+    import json
+
+    z = np.load(path)
+    meta = json.loads(bytes(z["plan_json"]).decode())
+    plan = {"dt": meta["dt"], "exact": meta["exact"], "pops": []}
+    for k, m in enumerate(meta["pops"]):
+        p = dict(m)
+        p["fields"] = [tuple(f) for f in m["fields"]]
+        p["conns"] = []
+        for ci, c in enumerate(m["conns"]):
+            p["conns"].append({"src": c["src"], "written": c["written"], "conn_id": None,
+                               "ptr": torch.from_numpy(z[f"p{k}_c{ci}_ptr"]),
+                               "link": torch.from_numpy(z[f"p{k}_c{ci}_link"]),
+                               "perm": torch.from_numpy(z[f"p{k}_c{ci}_perm"]),
+                               "per_link": {e: torch.from_numpy(z[f"p{k}_c{ci}_e_{e}"]) for e in c["per_link"]}})
+        plan["pops"].append(p)
+    return plan
+
+
+_CTYPES = {"long long": ctypes.c_int64, "float": ctypes.c_float, "int": ctypes.c_int32, "u32": ctypes.c_uint32}
+
+
+def _params_struct(fields: list):
+    """The ctypes Params structure of a plan's fields (pointers as void *)."""
+    return params_type([(name, ct, ctypes.c_void_p if ct.endswith("*") else _CTYPES[ct]) for name, ct in fields])
+
+
 class JitRuntime:
-    def __init__(self, net):
+    """The step kernels of a transpiled network: built from `net` (its plan made on the spot), or from a saved
+    plan (`plan`; `net` then a PlannedNetwork holding the plan's state)."""
+
+    def __init__(self, net, plan: dict | None = None):
         self.net = net
         dev = self.device = net.device
         dindex = dev.index if dev.index is not None else 0
-        dt = self.dt = float(net.resolution)
+        if plan is None:
+            plan = plan_of(net)
+        self.plan = plan
+        dt = self.dt = float(plan["dt"])
         pops = self.pops = list(net.populations)
-        index = {id(p): k for k, p in enumerate(pops)}
         self.keep = []
-        words = [(len(p.shape) + 31) // 32 for p in pops]
-        self.words = words
-        # spike-bit ring depth of each population: above every delay of its outgoing connections
-        steps_of, max_out = {}, [1] * len(pops)
-        for c in net.connections:
-            topo = c.fabric.topology
-            steps = delay_steps(c.fabric.value("delay"), len(topo), dt, device=topo.target_indices.device)
-            steps_of[id(c)] = steps
-            if len(topo):
-                s = index[id(c._source)]
-                max_out[s] = max(max_out[s], int(steps.max()))
-        depth = [max(2, 1 << int(np.ceil(np.log2(m + 1)))) for m in max_out]
-        self.depth = depth
+        words = self.words = [p["words"] for p in plan["pops"]]
+        depth = self.depth = [p["depth"] for p in plan["pops"]]
         self.bits = [torch.zeros(d * w, dtype=torch.int32, device=dev) for d, w in zip(depth, words)]
         # each spike's time within its step (event-driven intake reads it; the clocked one ignores it)
-        self.offs = [torch.zeros(d * max(1, len(p.shape)), dtype=torch.float32, device=dev)
-                     for d, p in zip(depth, pops)]
-        self.exact = bool(getattr(net, "exact", False))
+        self.offs = [torch.zeros(d * max(1, p["n"]), dtype=torch.float32, device=dev)
+                     for d, p in zip(depth, plan["pops"])]
+        self.exact = bool(plan["exact"])
         self.err = torch.zeros(len(pops), dtype=torch.int32, device=dev)
         self.counters_t = torch.zeros(len(pops), 2, dtype=torch.int64, device=dev)
         self.record_rows = int(net.record_steps)
         self.rec_step0 = net.step_count
         self.rasters = [torch.zeros(max(1, self.record_rows) * w, dtype=torch.int32, device=dev) for w in words]
-        self.raster_offs = [torch.zeros(max(1, self.record_rows) * max(1, len(p.shape)), dtype=torch.float32,
-                                        device=dev) for p in pops]
+        self.raster_offs = [torch.zeros(max(1, self.record_rows) * max(1, p["n"]), dtype=torch.float32,
+                                        device=dev) for p in plan["pops"]]
         self.kernels, self.params, self.sources = [], [], []
         self.edge_arrays = {}  # (connection id, edge name) -> (per-link values in pull order, pull permutation)
-        for k, p in enumerate(pops):
-            node = p.node
-            incoming, ctx_in = [], []
-            conns = [c for c in net.connections if c._target is p]
-            site = 0
-            for c in conns:
-                port = c._target_port or "receive"
-                hook = node.receive.get(port)
-                if hook is None:
-                    raise ValueError(f"{p!r} has no receive port {port!r}")
-                plan = EdgePlan(c, hook)
-                dyn = [h for h, real in plan.recv.items() if real in plan.per_link]
-                stat = {h: plan.static[real] for h, real in plan.recv.items() if real not in plan.per_link}
-                ctx = hook_context(p, hook, dyn, stat, site_base=site)
-                site += 32
-                inc = {"receive": (hook.ast, ctx), "edge_dynamic": plan.per_link, "edge_written": plan.written,
-                       "alias": {h: real for h, real in plan.recv.items() if real in plan.per_link and h != real},
-                       "forward": None, "backward": None, "conn": c, "plan": plan}
-                for kind in ("forward", "backward"):
-                    eh = getattr(plan, kind)
-                    if eh is not None:
-                        inc[kind] = (eh.ast, edge_hook_context(p, eh, plan.per_link, plan.static))
-                incoming.append(inc)
-            hooks = {"update": (node.update.ast, hook_context(p, node.update, site_base=site)),
-                     "send": (node.send.ast, hook_context(p, node.send, site_base=site + 32))}
-            src, fields = build_source(type(p.instance).__name__, dict(p.dynamic_attrs), hooks, incoming,
-                                       exact=self.exact, n=len(p.shape))
-            self.sources.append(src)
-            self.kernels.append(compile_source(src, dindex))
-            P = params_type(fields)()
-            P.n, P.words, P.bit_mask = len(p.shape), words[k], depth[k] - 1
-            P.seed_lo, P.seed_hi = int(p.seed) & 0xFFFFFFFF, (int(p.seed) >> 32) & 0xFFFFFFFF
-            for a, py in p.dynamic_attrs.items():
-                _, _, tdt = ctype_of(py)
+        tdtype = {"bool": torch.bool, "int": torch.int32, "float": torch.float32}
+        for k, (p, pp) in enumerate(zip(pops, plan["pops"])):
+            self.sources.append(pp["source"])
+            self.kernels.append(compile_source(pp["source"], dindex))
+            P = _params_struct(pp["fields"])()
+            P.n, P.words, P.bit_mask = pp["n"], words[k], depth[k] - 1
+            P.seed_lo, P.seed_hi = pp["seed"] & 0xFFFFFFFF, (pp["seed"] >> 32) & 0xFFFFFFFF
+            for a, ty in pp["attrs"].items():
                 t = p.state_tensor(a, dev)
-                if t.dtype != tdt:
-                    t = t.to(tdt)
+                if t.dtype != tdtype[ty]:
+                    t = t.to(tdtype[ty])
                 if not t.is_contiguous():
                     t = t.contiguous()
                 p._state[a] = t
@@ -168,24 +255,20 @@ class JitRuntime:
             P.raster_steps, P.rec0 = self.record_rows, self.rec_step0
             P.err = self.err[k:].data_ptr()
             P.counters = self.counters_t[k].data_ptr()
-            for ci, inc in enumerate(incoming):
-                c = inc["conn"]
-                s = index[id(c._source)]
-                topo = c.fabric.topology
-                ptr, link, perm = pull_form(topo, steps_of[id(c)], len(p.shape))
-                ptr, link = self._dev(ptr), self._dev(link if link.numel() else torch.zeros(1, dtype=torch.int32))
+            for ci, c in enumerate(pp["conns"]):
+                s = c["src"]
+                ptr = self._dev(c["ptr"])
+                link = self._dev(c["link"] if c["link"].numel() else torch.zeros(1, dtype=torch.int32))
                 setattr(P, f"c{ci}_ptr", ptr.data_ptr())
                 setattr(P, f"c{ci}_link", link.data_ptr())
                 setattr(P, f"c{ci}_src_bits", self.bits[s].data_ptr())
                 setattr(P, f"c{ci}_src_words", words[s])
                 setattr(P, f"c{ci}_src_mask", depth[s] - 1)
                 setattr(P, f"c{ci}_src_off", self.offs[s].data_ptr())
-                setattr(P, f"c{ci}_src_n", len(pops[s].shape))
-                plan = inc["plan"]
-                for e in plan.per_link:
-                    v = plan.initial(c, e, len(topo))
-                    v = self._dev(v[perm.cpu()] if v.numel() else torch.zeros(1))
-                    self.edge_arrays[(id(c), e)] = (v, perm.cpu())
+                setattr(P, f"c{ci}_src_n", plan["pops"][s]["n"])
+                for e, v in c["per_link"].items():
+                    v = self._dev(v if v.numel() else torch.zeros(1))
+                    self.edge_arrays[(c["conn_id"], e)] = (v, c["perm"])
                     setattr(P, f"c{ci}_e_{e}", v.data_ptr())
             self.params.append(P)
         self.stream = torch.cuda.Stream(device=dev)
@@ -208,9 +291,10 @@ class JitRuntime:
             for kern, P, p in zip(self.kernels, self.params, self.pops):
                 P.step, P.t, P.t0 = n, (n + 1) * self.dt, n * self.dt
                 per = BLOCK if self.exact else NPB_C  # neurons per block (clocked: SCAN threads each)
-                grid = (len(p.shape) + per - 1) // per
+                size = len(p.shape)
+                grid = (size + per - 1) // per
                 if grid:
-                    threads = BLOCK if self.exact else scan(len(p.shape)) * NPB_C
+                    threads = BLOCK if self.exact else scan(size) * NPB_C
                     _lib.check(lib.n2b_jit_launch(kern, grid, threads, ctypes.byref(P), ctypes.sizeof(P), self._s),
                                "n2b_jit_launch")
                     self.launches += 1
@@ -291,3 +375,43 @@ class JitRuntime:
     def close(self) -> None:
         self.stream.synchronize()
         self.kernels = []
+
+
+class PlannedPopulation:
+    """A population as a plan describes it: its size, seed and state tensors, no model class."""
+
+    def __init__(self, entry: dict, state: dict):
+        self.name = entry["name"]
+        self.shape = range(entry["n"])
+        self.seed = entry["seed"]
+        self._state = dict(state)
+
+    def state_tensor(self, attr: str, device=None) -> torch.Tensor:
+        t = self._state[attr]
+        if device is not None and t.device != torch.device(device):
+            t = self._state[attr] = t.to(device)
+        return t
+
+    def __repr__(self):
+        return f"PlannedPopulation({self.name} x {len(self.shape)})"
+
+
+class PlannedNetwork:
+    """Steps a saved plan (plan_of / save_plan / load_plan): the step kernels of a transpiled network, run where
+    its Python model classes are not. states: per population {attribute: tensor [n]} (the initial state)."""
+
+    def __init__(self, plan: dict, states: list, device, record_steps: int = 0):
+        self.device = torch.device(device)
+        self.resolution = float(plan["dt"])
+        self.exact = bool(plan["exact"])
+        self.step_count = 0
+        self.record_steps = int(record_steps)
+        self.populations = [PlannedPopulation(p, st) for p, st in zip(plan["pops"], states)]
+        self.runtime = JitRuntime(self, plan)
+
+    def run_steps(self, n_steps: int) -> None:
+        self.runtime.advance(n_steps)
+        self.step_count += int(n_steps)
+
+    def close(self) -> None:
+        self.runtime.close()

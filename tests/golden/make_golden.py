@@ -36,6 +36,17 @@ brunel_longrun_c1.json
     at least 4 spikes, activity std/mean in 1 ms bins), captured instead of
     printed; plus the loop's wall time on this machine's cores.
 
+refmodel_pd14.npz, refmodel_brunel.npz
+    The reference's own neuron models -- PD14_neuron (test/networks/PD14/neuron.py) and Brunel_neuron
+    (test/networks/Brunel/neuron.py), imported from their files with `naer2` resolving to this package's DSL
+    -- in small networks built here, lowered by this package's transpiler: the plan (naer2_b200.transpiler.
+    plan_of: the generated CUDA sources, Params fields and values, pull CSR), the initial state, and the
+    rasters and final state of the same networks run by the DSL interpreter (oracle/dsl_interpreter.py,
+    which calls the models' own hook functions). PD14_neuron clocked (its DC background, two populations,
+    per-link normal weights and delays); Brunel_neuron event-driven at exact spike times (net.exact), driven
+    by jittered pacemakers (tests/dsl_models.py) and recurrent links. The GPU test steps the plan where the
+    models' files are not, and compares.
+
 philox_triton.json
     tl.randint4x / tl.rand of Triton (the reference's random lowering calls
     tl.rand, naer2/transpiler/transformers/random_lowering_transformer.py:
@@ -167,6 +178,84 @@ def brunel_longrun(reference: pathlib.Path):
     print(f"brunel_longrun_c1: {spikes} spikes, {ns['_golden_stats']}, loop {wall:.1f} s")
 
 
+def _import_reference_model(reference: pathlib.Path, rel: str, cls: str):
+    """A model class of the reference, loaded from its file with `import naer2` resolving to this package."""
+    import importlib.util
+
+    import naer2_b200
+
+    sys.modules.setdefault("naer2", naer2_b200)
+    spec = importlib.util.spec_from_file_location(f"refmodel_{cls}", reference / rel)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return getattr(mod, cls)
+
+
+def reference_models(reference: pathlib.Path, steps: int = 300):
+    import torch
+
+    from naer2_b200.patterns import fixed_indegree
+    from naer2_b200.transpiler import plan_of, save_plan
+    from oracle import dsl_interpreter
+    from tests.dsl_models import JitterPacemaker, Syn
+
+    PD14 = _import_reference_model(reference, "test/networks/PD14/neuron.py", "PD14_neuron")
+    Brunel = _import_reference_model(reference, "test/networks/Brunel/neuron.py", "Brunel_neuron")
+    g = torch.Generator().manual_seed(31)
+
+    def pd14_net():
+        E = PD14(K_cortical=1600) * 240
+        I = PD14(K_cortical=1500) * 60
+        E.potential = (torch.randn(240, generator=g) * 4.0 - 58.0).float()
+        I.potential = (torch.randn(60, generator=g) * 4.0 - 58.0).float()
+        for s_, t_, k, w in ((E, E, 40, 0.08781), (E, I, 40, 0.08781), (I, E, 10, -0.35124), (I, I, 10, -0.35124)):
+            c = s_ >> fixed_indegree(k, seed=int(torch.randint(0, 1 << 30, (1,), generator=g))) >> t_
+            c.weight = (torch.randn(c.shape, generator=g) * abs(w) * 0.1 + w).float()
+            c.delay = torch.clamp(torch.randn(c.shape, generator=g) * 0.4 + 1.0, min=0.1).double()
+        net = E.network
+        net.resolution = 0.1
+        return net
+
+    def brunel_net():
+        src = JitterPacemaker(period=3) * 80
+        tgt = Brunel(tau=10.0, theta=1.0, V_r=0.0, t_ref=0.5) * 120
+        c1 = src >> Syn() @ fixed_indegree(8, seed=41) >> tgt
+        c1.weight = (0.1 + 0.25 * torch.rand(c1.shape, generator=g)).float()
+        c1.delay = (torch.randint(1, 5, c1.shape, generator=g) * 0.1).double()
+        c2 = tgt >> Syn() @ fixed_indegree(4, seed=42) >> tgt
+        c2.weight = (0.2 * torch.rand(c2.shape, generator=g) - 0.05).float()
+        c2.delay = 0.3
+        src.phase = torch.randint(0, 3, (80,), generator=g, dtype=torch.int32)
+        src.jitter = (0.1 * torch.rand(80, generator=g)).float()
+        net = src.network
+        net.resolution = 0.1
+        net.exact = True
+        return net
+
+    for name, make in (("pd14", pd14_net), ("brunel", brunel_net)):
+        net = make()
+        pops = list(net.populations)
+        init = {}
+        for k, p in enumerate(pops):
+            for a in p.dynamic_attrs:
+                init[f"p{k}_{a}_0"] = p.state_tensor(a).detach().cpu().numpy().copy()
+        plan = plan_of(net)
+        out = dsl_interpreter.run(net, steps)
+        rasters, state = out[0], out[1]
+        arrays = dict(init)
+        for k, p in enumerate(pops):
+            arrays[f"p{k}_raster"] = np.packbits(rasters[k], axis=1)
+            for a, v in state[k].items():
+                arrays[f"p{k}_{a}_end"] = v
+        if len(out) > 3:  # exact times: each spike's offset within its step
+            for k in range(len(pops)):
+                arrays[f"p{k}_offsets"] = out[3][k]
+        arrays["steps"] = np.int64(steps)
+        save_plan(plan, HERE / f"refmodel_{name}_plan.npz")
+        np.savez_compressed(HERE / f"refmodel_{name}.npz", **arrays)
+        print(f"refmodel_{name}: spikes per population {[int(r.sum()) for r in rasters]} in {steps} steps")
+
+
 def _reference_function(path: pathlib.Path, name: str):
     """A top-level function of a reference module, compiled from its source alone (its imports not run)."""
     tree = ast.parse(path.read_text())
@@ -246,7 +335,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("NAER2_REFERENCE"),
                     help="root of the reference checkout (or the NAER2_REFERENCE environment variable)")
-    ap.add_argument("--only", choices=["brunel", "pd14", "philox", "longrun"])
+    ap.add_argument("--only", choices=["brunel", "pd14", "philox", "longrun", "refmodels"])
     args = ap.parse_args()
     if not args.reference:
         raise SystemExit("give --reference PATH (or NAER2_REFERENCE): the root of the reference checkout")
@@ -261,6 +350,8 @@ def main():
         pd14_neuron(ref)
     if args.only in (None, "longrun"):
         brunel_longrun(ref)
+    if args.only in (None, "refmodels"):
+        reference_models(ref)
 
 
 if __name__ == "__main__":
