@@ -410,19 +410,67 @@ struct PullSweep {
     long long part; // its partial sum in that row
 };
 
-__device__ __forceinline__ void pull_link(const ConnDev &C, PullStage *st, int32_t *err, PullSweep &sw, int l,
-                                          uint32_t rec, float w, long long n) {
+constexpr int PULL_BATCH = 4;  // staged links per lane whose spike-bit words are loaded together
+
+// Whether a link word is in range, and its source's spike-bit word of step n - delay. A plain load (cached in
+// L1): the ring rows a pull reads were written before the last grid barrier or launch boundary, whose acquire
+// makes them visible to the block, and a source's ring is small, so its rows stay in L1 across a warp's links.
+__device__ __forceinline__ uint32_t pull_bits(const ConnDev &C, uint32_t rec, long long n, bool &ok) {
+    const int d = (int)(rec >> 24), s = (int)(rec & 0xFFFFFFu);
+    ok = d >= 1 && d <= C.src_bit_mask && s < C.src_n;
+    return ok ? C.src_bits[(size_t)((n - d) & C.src_bit_mask) * C.src_words + (s >> 5)] : 0u;
+}
+
+// Link l (the lane's links in increasing order) into the lane's row sums: leave the rows l is past, then add.
+__device__ __forceinline__ void pull_apply(const ConnDev &C, PullStage *st, int32_t *err, PullSweep &sw, int l,
+                                           uint32_t rec, uint32_t word, bool ok, float w) {
     while (l >= st->ptr[sw.q + 1]) {  // left the row (rows may be empty)
         if (sw.part) atomicAdd(reinterpret_cast<unsigned long long *>(&st->sum[sw.q]), (unsigned long long)sw.part);
         sw.part = 0;
         ++sw.q;
     }
-    const int d = (int)(rec >> 24), s = (int)(rec & 0xFFFFFFu);
-    if (d >= 1 && d <= C.src_bit_mask && s < C.src_n) {
-        const uint32_t word = __ldcg(C.src_bits + (size_t)((n - d) & C.src_bit_mask) * C.src_words + (s >> 5));
-        if ((word >> (s & 31)) & 1u) sw.part += C.homogeneous ? C.wfx : weight_fx(w, C.wscale);
-    } else {
+    if (!ok) {
         atomicAdd(err + 1, 1);
+        return;
+    }
+    const int s = (int)(rec & 0xFFFFFFu);
+    if ((word >> (s & 31)) & 1u) sw.part += C.homogeneous ? C.wfx : weight_fx(w, C.wscale);
+}
+
+__device__ __forceinline__ void pull_link(const ConnDev &C, PullStage *st, int32_t *err, PullSweep &sw, int l,
+                                          uint32_t rec, float w, long long n) {
+    bool ok;
+    const uint32_t word = pull_bits(C, rec, n, ok);
+    pull_apply(C, st, err, sw, l, rec, word, ok, w);
+}
+
+// The links [c0, c1) of a landed chunk in buffer b, PULL_BATCH per lane at a time: their bit words all in
+// flight before any is used.
+__device__ __forceinline__ void pull_chunk(const ConnDev &C, PullStage *st, int32_t *err, PullSweep &sw, int b,
+                                           int c0, int c1, long long n) {
+    const int lane = threadIdx.x & 31;
+    for (int base = c0 + lane; base < c1; base += 32 * PULL_BATCH) {
+        uint32_t rec[PULL_BATCH], word[PULL_BATCH];
+        float w[PULL_BATCH];
+        bool ok[PULL_BATCH];
+#pragma unroll
+        for (int q = 0; q < PULL_BATCH; ++q) {
+            const int l = base + 32 * q;
+            rec[q] = 0u;
+            w[q] = 0.f;
+            word[q] = 0u;
+            ok[q] = false;
+            if (l < c1) {
+                rec[q] = st->link[b][l - c0];
+                w[q] = C.homogeneous ? 0.f : st->w[b][l - c0];
+                word[q] = pull_bits(C, rec[q], n, ok[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < PULL_BATCH; ++q) {
+            const int l = base + 32 * q;
+            if (l < c1) pull_apply(C, st, err, sw, l, rec[q], word[q], ok[q], w[q]);
+        }
     }
 }
 
@@ -458,8 +506,7 @@ __device__ __forceinline__ long long pull_staged(const ConnDev &C, PullStage *st
                 pull_link(C, st, err, sw, l, __ldg(C.link + l), C.homogeneous ? 0.f : __ldg(C.w + l), n);
             continue;
         }
-        for (int l = c0 + lane; l < c1; l += 32)
-            pull_link(C, st, err, sw, l, st->link[b][l - c0], C.homogeneous ? 0.f : st->w[b][l - c0], n);
+        pull_chunk(C, st, err, sw, b, c0, c1, n);
         __syncwarp();  // every lane done with buffer b before it is refilled
         if (lane == 0 && k + 2 < n_chunks) pull_issue(st, C, a0, a1, k + 2);
     }
