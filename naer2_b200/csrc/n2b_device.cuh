@@ -96,6 +96,7 @@ struct StepArgs {
     unsigned long long bar_limit_ns;  // persistent windows: a grid barrier wait gives up after this long
     int32_t trace_steps;
     int32_t pull_staged;   // the launch has a PullStage per warp in dynamic shared memory
+    int32_t ring_cache_words;  // ... and after them a copy of a pull source's spike-bit ring of at most this size
     int32_t item_cap;
     int32_t n_tiles;
     int32_t offset;        // this launch's step = *step + offset (per-step launches)
@@ -310,9 +311,11 @@ __device__ __forceinline__ bool pd14(const PopDev &P, float in, float &v, float 
 // used for connections whose rows are not 16-byte aligned, and where the launch
 // has no staging memory.
 template <bool INL>
-__device__ __forceinline__ long long pull_walk(const ConnDev &C, int32_t *err, int wbase, int nq, long long n) {
+__device__ __forceinline__ long long pull_walk(const ConnDev &C, const uint32_t *ring, int32_t *err,
+                                               unsigned long long *events, int wbase, int nq, long long n) {
     const int lane = threadIdx.x & 31;
     long long mine = 0;
+    unsigned hits = 0;
     for (int q = 0; q < nq; ++q) {
         const int jq = wbase + q;
         const int r0 = __ldg(C.ptr + jq), r1 = __ldg(C.ptr + jq + 1);
@@ -321,9 +324,12 @@ __device__ __forceinline__ long long pull_walk(const ConnDev &C, int32_t *err, i
             const uint32_t rec = __ldg(C.link + l);
             const int d = (int)(rec >> 24), s = (int)(rec & 0xFFFFFFu);
             if (d >= 1 && d <= C.src_bit_mask && s < C.src_n) {
-                const uint32_t word =
-                    __ldcg(C.src_bits + (size_t)((n - d) & C.src_bit_mask) * C.src_words + (s >> 5));
-                if ((word >> (s & 31)) & 1u) part += C.homogeneous ? C.wfx : weight_fx(__ldg(C.w + l), C.wscale);
+                const size_t at = (size_t)((n - d) & C.src_bit_mask) * C.src_words + (s >> 5);
+                const uint32_t word = ring ? ring[at] : __ldcg(C.src_bits + at);
+                if ((word >> (s & 31)) & 1u) {
+                    part += C.homogeneous ? C.wfx : weight_fx(__ldg(C.w + l), C.wscale);
+                    ++hits;
+                }
             } else {
                 atomicAdd(err + 1, 1);
             }
@@ -331,6 +337,8 @@ __device__ __forceinline__ long long pull_walk(const ConnDev &C, int32_t *err, i
         part = warp_sum64(part);
         if (lane == q) mine += part;
     }
+    hits = __reduce_add_sync(FULL, hits);
+    if (lane == 0 && hits) atomicAdd(events, (unsigned long long)hits);
     return mine;
 }
 
@@ -342,7 +350,8 @@ __device__ __forceinline__ long long pull_walk(const ConnDev &C, int32_t *err, i
 // its ragged head and tail (fewer than 4 links each) are loaded directly. Each lane sweeps its links in
 // increasing order, following the rows by their offsets (kept in shared memory), and adds a row's partial sum
 // into the row's shared slot when it leaves the row.
-constexpr int PULL_CH = 512;                        // links per staging chunk
+constexpr int PULL_CH = 256;                        // links per staging chunk
+constexpr int RING_CACHE_MAX = 8192;                // words of a pull source's ring copied to shared memory, at most
 constexpr unsigned PULL_WAIT_POLLS = 1u << 22;      // polls of a chunk's mbarrier before it counts as lost
 
 struct alignas(16) PullStage {  // one per warp, in dynamic shared memory
@@ -408,6 +417,7 @@ __device__ __forceinline__ bool pull_wait(PullStage *st, int b) {
 struct PullSweep {
     int q;          // the lane's current row (warp-relative)
     long long part; // its partial sum in that row
+    unsigned hits;  // links whose source spiked (the synaptic events of the pull)
 };
 
 constexpr int PULL_BATCH = 4;  // staged links per lane whose spike-bit words are loaded together
@@ -415,10 +425,14 @@ constexpr int PULL_BATCH = 4;  // staged links per lane whose spike-bit words ar
 // Whether a link word is in range, and its source's spike-bit word of step n - delay. A plain load (cached in
 // L1): the ring rows a pull reads were written before the last grid barrier or launch boundary, whose acquire
 // makes them visible to the block, and a source's ring is small, so its rows stay in L1 across a warp's links.
-__device__ __forceinline__ uint32_t pull_bits(const ConnDev &C, uint32_t rec, long long n, bool &ok) {
+// ring: the source's ring copied into shared memory for this connection (small rings), else null.
+__device__ __forceinline__ uint32_t pull_bits(const ConnDev &C, const uint32_t *ring, uint32_t rec, long long n,
+                                              bool &ok) {
     const int d = (int)(rec >> 24), s = (int)(rec & 0xFFFFFFu);
     ok = d >= 1 && d <= C.src_bit_mask && s < C.src_n;
-    return ok ? C.src_bits[(size_t)((n - d) & C.src_bit_mask) * C.src_words + (s >> 5)] : 0u;
+    if (!ok) return 0u;
+    const size_t at = (size_t)((n - d) & C.src_bit_mask) * C.src_words + (s >> 5);
+    return ring ? ring[at] : C.src_bits[at];
 }
 
 // Link l (the lane's links in increasing order) into the lane's row sums: leave the rows l is past, then add.
@@ -434,20 +448,23 @@ __device__ __forceinline__ void pull_apply(const ConnDev &C, PullStage *st, int3
         return;
     }
     const int s = (int)(rec & 0xFFFFFFu);
-    if ((word >> (s & 31)) & 1u) sw.part += C.homogeneous ? C.wfx : weight_fx(w, C.wscale);
+    if ((word >> (s & 31)) & 1u) {
+        sw.part += C.homogeneous ? C.wfx : weight_fx(w, C.wscale);
+        ++sw.hits;
+    }
 }
 
-__device__ __forceinline__ void pull_link(const ConnDev &C, PullStage *st, int32_t *err, PullSweep &sw, int l,
-                                          uint32_t rec, float w, long long n) {
+__device__ __forceinline__ void pull_link(const ConnDev &C, const uint32_t *ring, PullStage *st, int32_t *err,
+                                          PullSweep &sw, int l, uint32_t rec, float w, long long n) {
     bool ok;
-    const uint32_t word = pull_bits(C, rec, n, ok);
+    const uint32_t word = pull_bits(C, ring, rec, n, ok);
     pull_apply(C, st, err, sw, l, rec, word, ok, w);
 }
 
 // The links [c0, c1) of a landed chunk in buffer b, PULL_BATCH per lane at a time: their bit words all in
 // flight before any is used.
-__device__ __forceinline__ void pull_chunk(const ConnDev &C, PullStage *st, int32_t *err, PullSweep &sw, int b,
-                                           int c0, int c1, long long n) {
+__device__ __forceinline__ void pull_chunk(const ConnDev &C, const uint32_t *ring, PullStage *st, int32_t *err,
+                                           PullSweep &sw, int b, int c0, int c1, long long n) {
     const int lane = threadIdx.x & 31;
     for (int base = c0 + lane; base < c1; base += 32 * PULL_BATCH) {
         uint32_t rec[PULL_BATCH], word[PULL_BATCH];
@@ -463,7 +480,7 @@ __device__ __forceinline__ void pull_chunk(const ConnDev &C, PullStage *st, int3
             if (l < c1) {
                 rec[q] = st->link[b][l - c0];
                 w[q] = C.homogeneous ? 0.f : st->w[b][l - c0];
-                word[q] = pull_bits(C, rec[q], n, ok[q]);
+                word[q] = pull_bits(C, ring, rec[q], n, ok[q]);
             }
         }
 #pragma unroll
@@ -476,8 +493,8 @@ __device__ __forceinline__ void pull_chunk(const ConnDev &C, PullStage *st, int3
 
 // One connection's intake of the warp's nq rows (from neuron wbase); returns the lane's own row sum.
 template <bool INL>
-__device__ __forceinline__ long long pull_staged(const ConnDev &C, PullStage *st, int32_t *err, int wbase, int nq,
-                                                 long long n) {
+__device__ __forceinline__ long long pull_staged(const ConnDev &C, const uint32_t *ring, PullStage *st, int32_t *err,
+                                                 unsigned long long *events, int wbase, int nq, long long n) {
     const int lane = threadIdx.x & 31;
     if (lane <= nq) st->ptr[lane] = __ldg(C.ptr + wbase + lane);
     if (lane == 0 && nq == 32) st->ptr[32] = __ldg(C.ptr + wbase + 32);
@@ -491,9 +508,9 @@ __device__ __forceinline__ long long pull_staged(const ConnDev &C, PullStage *st
         if (n_chunks > 0) pull_issue(st, C, a0, a1, 0);
         if (n_chunks > 1) pull_issue(st, C, a0, a1, 1);
     }
-    PullSweep sw{0, 0};
+    PullSweep sw{0, 0, 0u};
     for (int l = L0 + lane; l < a0; l += 32)  // the head
-        pull_link(C, st, err, sw, l, __ldg(C.link + l), C.homogeneous ? 0.f : __ldg(C.w + l), n);
+        pull_link(C, ring, st, err, sw, l, __ldg(C.link + l), C.homogeneous ? 0.f : __ldg(C.w + l), n);
     bool lost = false;
     for (int k = 0; k < n_chunks; ++k) {
         const int b = k & 1;
@@ -503,10 +520,10 @@ __device__ __forceinline__ long long pull_staged(const ConnDev &C, PullStage *st
         if (lane == 0) st->uses[b] += 1;
         if (lost) {  // the chunk did not land in time: its links (and the rest) loaded directly
             for (int l = c0 + lane; l < c1; l += 32)
-                pull_link(C, st, err, sw, l, __ldg(C.link + l), C.homogeneous ? 0.f : __ldg(C.w + l), n);
+                pull_link(C, ring, st, err, sw, l, __ldg(C.link + l), C.homogeneous ? 0.f : __ldg(C.w + l), n);
             continue;
         }
-        pull_chunk(C, st, err, sw, b, c0, c1, n);
+        pull_chunk(C, ring, st, err, sw, b, c0, c1, n);
         __syncwarp();  // every lane done with buffer b before it is refilled
         if (lane == 0 && k + 2 < n_chunks) pull_issue(st, C, a0, a1, k + 2);
     }
@@ -517,27 +534,44 @@ __device__ __forceinline__ long long pull_staged(const ConnDev &C, PullStage *st
         }
     }
     for (int l = max(a1, L0) + lane; l < L1; l += 32)  // the tail
-        pull_link(C, st, err, sw, l, __ldg(C.link + l), C.homogeneous ? 0.f : __ldg(C.w + l), n);
+        pull_link(C, ring, st, err, sw, l, __ldg(C.link + l), C.homogeneous ? 0.f : __ldg(C.w + l), n);
     if (sw.part) atomicAdd(reinterpret_cast<unsigned long long *>(&st->sum[sw.q]), (unsigned long long)sw.part);
+    const unsigned hits = __reduce_add_sync(FULL, sw.hits);
+    if (lane == 0 && hits) atomicAdd(events, (unsigned long long)hits);
     __syncwarp();
     const long long mine = lane < nq ? st->sum[lane] : 0;
     __syncwarp();
     return mine;
 }
 
+// Every pull connection into the tile's population (called by every thread of the block). A source whose
+// whole spike-bit ring fits the launch's ring cache (a.ring_cache_words, in dynamic shared memory after the
+// warps' PullStages) is copied there first -- its rows of steps before n are final, the row of step n is not
+// read -- so that the links' bit tests are shared-memory loads.
 template <bool INL>
 __device__ __forceinline__ long long pull_intake(const StepArgs &a, const PopDev &P, int first, int count,
                                                  long long n, PullStage *stage) {
+    extern __shared__ __align__(128) unsigned char n2b_dyn_smem[];
     const int wbase = first + (threadIdx.x & ~31);
     const int nq = min(32, first + count - wbase);
-    if (nq <= 0) return 0;
     long long mine = 0;
     for (int c = P.pull_first; c < P.pull_first + P.n_pull; ++c) {
         const ConnDev &C = pull_at<INL>(a, c);
+        const int ring_words = (C.src_bit_mask + 1) * C.src_words;
+        const uint32_t *ring = nullptr;
+        if (stage != nullptr && ring_words <= a.ring_cache_words) {  // the same for every thread of the block
+            uint32_t *cache = reinterpret_cast<uint32_t *>(reinterpret_cast<PullStage *>(n2b_dyn_smem) +
+                                                           (blockDim.x >> 5));
+            __syncthreads();  // every warp done with the cache's previous ring
+            for (int k = threadIdx.x; k < ring_words; k += blockDim.x) cache[k] = __ldcg(C.src_bits + k);
+            __syncthreads();
+            ring = cache;
+        }
+        if (nq <= 0) continue;
         if (stage != nullptr && C.staged && !stage->broken)
-            mine += pull_staged<INL>(C, stage, a.err, wbase, nq, n);
+            mine += pull_staged<INL>(C, ring, stage, a.err, a.counters, wbase, nq, n);
         else
-            mine += pull_walk<INL>(C, a.err, wbase, nq, n);
+            mine += pull_walk<INL>(C, ring, a.err, a.counters, wbase, nq, n);
     }
     return mine;
 }
@@ -813,7 +847,7 @@ __device__ __forceinline__ void cache_rows(const StepArgs &a, const PopDev &P, i
 
 // One tile of one step. CACHED: the tile's Neuron is held in registers by the caller across steps (loaded
 // before the window, stored after it) and its row bounds are in s_cache; otherwise both come from memory.
-template <int NPB, bool INL, bool CACHED>
+template <int NPB, bool INL, bool CACHED, bool PULL>
 __device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n, const int4 tile, int k, Neuron &nr,
                                            const int *s_cache, Scratch<NPB> &sc, const SConn *s_conn,
                                            PullStage *stage) {
@@ -845,7 +879,7 @@ __device__ __forceinline__ void tile_phase(const StepArgs &a, const long long n,
     if (model == 3) {  // N2B_MODEL_POISSON_SOURCE
         fire = live && draw(P, j, n, 1u) < P.fire_threshold;
     } else {
-        if (P.n_pull > 0) acc += pull_intake<INL>(a, P, tile.y, tile.z, n, stage);
+        if (PULL && P.n_pull > 0) acc += pull_intake<INL>(a, P, tile.y, tile.z, n, stage);
         if (live) {
             *slot = 0;
             if (P.ext_len > 0) acc += (long long)poisson_count(P, draw(P, j, n, 0u)) * P.ext_wfx;
@@ -994,7 +1028,7 @@ __device__ __forceinline__ void far_phase(const StepArgs &a, const long long n, 
     }
 }
 
-template <int NPB, bool INL, int FG>
+template <int NPB, bool INL, int FG, bool PULL = true>
 __device__ __forceinline__ void step_body(const StepArgs &a, const long long n, int k, Neuron *cached,
                                           const int *s_cache, const SConn *s_conn, PullStage *stage) {
     __shared__ Scratch<NPB> sc;
@@ -1016,9 +1050,9 @@ __device__ __forceinline__ void step_body(const StepArgs &a, const long long n, 
     const int t = blockIdx.x;
     if (t < a.n_tiles) {
         if (cached != nullptr)
-            tile_phase<NPB, INL, true>(a, n, tile_at<INL, NPB>(a, t), k, *cached, s_cache, sc, s_conn, stage);
+            tile_phase<NPB, INL, true, PULL>(a, n, tile_at<INL, NPB>(a, t), k, *cached, s_cache, sc, s_conn, stage);
         else
-            tile_phase<NPB, INL, false>(a, n, tile_at<INL, NPB>(a, t), k, nr, nullptr, sc, s_conn, stage);
+            tile_phase<NPB, INL, false, PULL>(a, n, tile_at<INL, NPB>(a, t), k, nr, nullptr, sc, s_conn, stage);
     }
     if (dyn) {
         __shared__ int s_tile;
@@ -1028,7 +1062,7 @@ __device__ __forceinline__ void step_body(const StepArgs &a, const long long n, 
             const int u = (int)gridDim.x + s_tile;  // every thread reads it before the tile's first barrier
             if (u >= a.n_tiles) break;
             if (threadIdx.x == 0) next = atomicAdd(claim, 1);
-            tile_phase<NPB, INL, false>(a, n, tile_at<INL, NPB>(a, u), k, nr, nullptr, sc, s_conn, stage);
+            tile_phase<NPB, INL, false, PULL>(a, n, tile_at<INL, NPB>(a, u), k, nr, nullptr, sc, s_conn, stage);
         }
     }
     N2B_STAMP(a, k, 2);
@@ -1065,18 +1099,15 @@ __device__ __forceinline__ void red_release_add(unsigned *p, unsigned v) {
     asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-__device__ __forceinline__ unsigned ld_relaxed(const unsigned *p) {
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
     unsigned v;
-    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
 
-__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
-
 
 // Grid-wide barrier k (0, 1, ...) of a cooperative launch: every block adds 1 to one counter with release
-// semantics (its writes before its arrival) and polls, with relaxed loads and one acquire fence at the end,
-// until the counter holds
+// semantics (its writes before its arrival) and waits, with acquire loads, until the counter holds
 // (k + 1) * gridDim.x -- the counter starts each launch at 0 (advance_kernel clears it after every launch).
 // Every wait is bounded (a.bar_limit_ns, BAR_LIMIT_NS by default): a timeout sets error word 4 and the abort
 // word, and the kernel winds down instead of hanging. Returns false once aborted. A wait ends in every case:
@@ -1092,12 +1123,9 @@ __device__ __forceinline__ bool grid_sync(const StepArgs &a, unsigned k) {
         int ok = 1;
         unsigned long long t0 = 0;
         for (int spin = 0;; ++spin) {
-            // relaxed polls, one acquire fence once the count is there (a fence-based acquire pattern: cheaper
-            // than an acquire load per poll)
-            if ((int)(ld_relaxed(bar + BAR_COUNT) - target) >= 0) {
-                fence_acq_rel();
-                break;
-            }
+            // acquire polls (measured: relaxed polls with one fence.acq_rel at the end cost ~0.4-0.9 us more per
+            // step, the fence being the slower)
+            if ((int)(ld_acquire(bar + BAR_COUNT) - target) >= 0) break;
             if (*(volatile unsigned *)(bar + BAR_ABORT)) { ok = 0; break; }
             if (spin == 0) t0 = globaltimer();
             else if (globaltimer() - t0 > a.bar_limit_ns) {
@@ -1115,9 +1143,9 @@ __device__ __forceinline__ bool grid_sync(const StepArgs &a, unsigned k) {
 }
 
 // A window of n_steps steps in one cooperative launch (every block resident), steps separated by grid_sync.
-// DENSE: three blocks per SM (registers capped for it; far items two at a time), for networks with more tiles
-// than two blocks per SM hold -- every tile then keeps a block of its own; otherwise two blocks per SM and far
-// items four at a time.
+// DENSE: three blocks per SM (registers capped for it; far items two at a time; no pull connections), for
+// networks with more tiles than two blocks per SM hold -- every tile then keeps a block of its own; otherwise
+// two blocks per SM and far items four at a time.
 template <int NPB, bool INL, bool DENSE>
 __global__ void __launch_bounds__(NPB, DENSE ? 3 : 2)
     persistent_kernel(const __grid_constant__ StepArgs a, const int n_steps) {
@@ -1138,7 +1166,7 @@ __global__ void __launch_bounds__(NPB, DENSE ? 3 : 2)
     PullStage *stage = warp_stage(a);
     __syncthreads();
     for (int k = 0; k < n_steps; ++k) {
-        step_body<NPB, INL, DENSE ? 2 : 4>(a, n0 + k, k, &mine, s_cache, s_conn, stage);
+        step_body<NPB, INL, DENSE ? 2 : 4, !DENSE>(a, n0 + k, k, &mine, s_cache, s_conn, stage);
         if (!grid_sync(a, (unsigned)k)) break;
         N2B_STAMP(a, k, 4);
     }

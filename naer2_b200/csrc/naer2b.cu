@@ -388,13 +388,17 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     int want = (opt && opt->grid > 0) ? opt->grid
                                       : (persistent ? std::max(sms, L.n_tiles + sms / 2) : 2 * sms);
     int grid = std::max(L.n_tiles, want);
-    // the staged pull: a PullStage per warp in dynamic shared memory, when the network has pull connections
-    const size_t dyn = pull.empty() ? 0 : sizeof(n2b::PullStage) * (size_t)(block / 32);
+    // the staged pull: a PullStage per warp in dynamic shared memory, when the network has pull connections, and
+    // after them a cache for the largest pull source's spike-bit ring up to RING_CACHE_MAX words
+    int32_t ring_words = 0;
+    for (const n2b::ConnDev &C : pull) ring_words = std::max(ring_words, (C.src_bit_mask + 1) * C.src_words);
+    if (ring_words > n2b::RING_CACHE_MAX) ring_words = 0;  // too large: every source read from global memory
+    const size_t dyn = pull.empty() ? 0 : sizeof(n2b::PullStage) * (size_t)(block / 32) + sizeof(uint32_t) * ring_words;
     int most = 0;
     int rc2 = coresident_blocks(block, inl, false, device, dyn, &most);  // also raises the kernels' dynamic limit
     if (rc2) return rc2;
     bool dense = false;
-    if (persistent && L.n_tiles > most) {  // more tiles than blocks: the denser kernel, if it holds more
+    if (persistent && L.n_tiles > most && pull.empty()) {  // more tiles than blocks: the denser kernel (push only)
         int most3 = 0;
         rc2 = coresident_blocks(block, inl, true, device, dyn, &most3);
         if (rc2) return rc2;
@@ -438,6 +442,7 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     a.bar_limit_ns = (opt && opt->barrier_limit_ns > 0) ? (unsigned long long)opt->barrier_limit_ns
                                                          : n2b::BAR_LIMIT_NS;
     a.pull_staged = dyn > 0;
+    a.ring_cache_words = ring_words;
     a.n_pops = n_pops;
     a.n_push = L.n_push;
     if (inl) {

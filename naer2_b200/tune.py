@@ -99,7 +99,11 @@ def autotune(net, steps: int = 300, warmup: int = 100, blocks=(128, 256), persis
         mode_sets = [{}] + ([pulls] if pulls else [])
         best = (us, 256, None, True, {})
         t0 = time.perf_counter()
-        for block, grid, pers, modes in itertools.product(blocks, grids, persistent, mode_sets):
+        # pull sets also try 64-neuron tiles: a pulled row is walked by its tile's warps, so smaller tiles spread
+        # the pulls over more SMs
+        cands = [(b, g, p, m) for m in mode_sets for b in (tuple(blocks) + ((64,) if m and 64 not in blocks else ()))
+                 for g in grids for p in persistent]
+        for block, grid, pers, modes in cands:
             if (block, grid, pers, len(modes)) == (256, None, True, 0):
                 continue
             net.block, net.grid, net.persistent, net.tuned = block, grid, pers, dict(modes)
