@@ -351,16 +351,17 @@ __device__ __forceinline__ long long pull_walk(const ConnDev &C, const uint32_t 
 // increasing order, following the rows by their offsets (kept in shared memory), and adds a row's partial sum
 // into the row's shared slot when it leaves the row.
 constexpr int PULL_CH = 256;                        // links per staging chunk
+constexpr int PULL_BUFS = 2;                        // chunks in flight per warp
 constexpr int RING_CACHE_MAX = 8192;                // words of a pull source's ring copied to shared memory, at most
 constexpr unsigned PULL_WAIT_POLLS = 1u << 22;      // polls of a chunk's mbarrier before it counts as lost
 
 struct alignas(16) PullStage {  // one per warp, in dynamic shared memory
-    uint32_t link[2][PULL_CH];
-    float w[2][PULL_CH];
-    unsigned long long bar[2];
+    uint32_t link[PULL_BUFS][PULL_CH];
+    float w[PULL_BUFS][PULL_CH];
+    unsigned long long bar[PULL_BUFS];
     long long sum[32];
     int32_t ptr[33];
-    uint32_t uses[2];   // completions of each buffer's mbarrier so far (its next parity)
+    uint32_t uses[PULL_BUFS];   // completions of each buffer's mbarrier so far (its next parity)
     int32_t broken;     // a chunk was lost: the rest of the launch walks instead of staging
 };
 
@@ -370,7 +371,7 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 
 __device__ __forceinline__ void pull_stage_init(PullStage *st) {
     if ((threadIdx.x & 31) == 0) {
-        for (int b = 0; b < 2; ++b) {
+        for (int b = 0; b < PULL_BUFS; ++b) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&st->bar[b])) : "memory");
             st->uses[b] = 0;
         }
@@ -379,9 +380,9 @@ __device__ __forceinline__ void pull_stage_init(PullStage *st) {
     }
 }
 
-// Lane 0: chunk k of the aligned range [a0, a1) into buffer k & 1.
+// Lane 0: chunk k of the aligned range [a0, a1) into buffer k mod PULL_BUFS.
 __device__ __forceinline__ void pull_issue(PullStage *st, const ConnDev &C, int a0, int a1, int k) {
-    const int b = k & 1;
+    const int b = k % PULL_BUFS;
     const int c0 = a0 + k * PULL_CH, c1 = min(a1, c0 + PULL_CH);
     const uint32_t bytes = (uint32_t)(c1 - c0) * 4u;  // a multiple of 16: a0, a1 and PULL_CH are multiples of 4
     const uint32_t bar = smem_u32(&st->bar[b]);
@@ -398,14 +399,16 @@ __device__ __forceinline__ void pull_issue(PullStage *st, const ConnDev &C, int 
                      : "memory");
 }
 
-// Every lane: wait (bounded) until buffer b's chunk has landed; false if it did not within the limit (twice).
+// Every lane: wait (bounded) until buffer b's chunk has landed; false if it did not within the limit. The wait
+// polls with the non-blocking mbarrier.test_wait: try_wait may suspend the warp for a time slice before it
+// looks again, which measured ~3.7 us per chunk here against well under a microsecond of copy.
 __device__ __forceinline__ bool pull_wait(PullStage *st, int b) {
     const uint32_t bar = smem_u32(&st->bar[b]);
     const uint32_t parity = st->uses[b] & 1u;
     for (unsigned it = 0; it < 2 * PULL_WAIT_POLLS; ++it) {
         uint32_t ok;
         asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
             : "=r"(ok)
             : "r"(bar), "r"(parity)
             : "memory");
@@ -505,15 +508,14 @@ __device__ __forceinline__ long long pull_staged(const ConnDev &C, const uint32_
     if (a1 <= a0) a0 = a1 = L1;  // too short to stage: every link loaded directly
     const int n_chunks = (a1 - a0 + PULL_CH - 1) / PULL_CH;
     if (lane == 0) {
-        if (n_chunks > 0) pull_issue(st, C, a0, a1, 0);
-        if (n_chunks > 1) pull_issue(st, C, a0, a1, 1);
+        for (int k = 0; k < PULL_BUFS && k < n_chunks; ++k) pull_issue(st, C, a0, a1, k);
     }
     PullSweep sw{0, 0, 0u};
     for (int l = L0 + lane; l < a0; l += 32)  // the head
         pull_link(C, ring, st, err, sw, l, __ldg(C.link + l), C.homogeneous ? 0.f : __ldg(C.w + l), n);
     bool lost = false;
     for (int k = 0; k < n_chunks; ++k) {
-        const int b = k & 1;
+        const int b = k % PULL_BUFS;
         const int c0 = a0 + k * PULL_CH, c1 = min(a1, c0 + PULL_CH);
         if (!lost && !pull_wait(st, b)) lost = true;
         __syncwarp();
@@ -525,7 +527,7 @@ __device__ __forceinline__ long long pull_staged(const ConnDev &C, const uint32_
         }
         pull_chunk(C, ring, st, err, sw, b, c0, c1, n);
         __syncwarp();  // every lane done with buffer b before it is refilled
-        if (lane == 0 && k + 2 < n_chunks) pull_issue(st, C, a0, a1, k + 2);
+        if (lane == 0 && k + PULL_BUFS < n_chunks) pull_issue(st, C, a0, a1, k + PULL_BUFS);
     }
     if (lost) {
         if (lane == 0) {
