@@ -94,11 +94,18 @@ typedef struct n2b_population {
  *   PUSH: rows per source neuron (ptr[n_src + 1]), index = target neuron;
  *   PULL: rows per target neuron (ptr[n_tgt + 1]), index = source neuron.
  * w: per-link weight, or NULL for `weight` on every link.
- * split (PUSH only, optional): per source row, the first link of delay >= 2
+ * split (optional), PUSH: per source row, the first link of delay >= 2
  *   steps, the row's delay-1 links all before it. The spiking neuron's block
  *   delivers [ptr[s], split[s]) in the step itself; [split[s], ptr[s+1]) goes
  *   to a work list every block of the next step's launch shares. NULL: the
- *   spiking neuron's block delivers the whole row. */
+ *   spiking neuron's block delivers the whole row.
+ * split (optional), PULL: [n_tgt + 1] row offsets of a second CSR in the same
+ *   link array holding every link of delay >= 2 steps (split[0] >= ptr[n_tgt]):
+ *   ptr's rows then hold only delay-1 links, pulled by the target's block in the
+ *   step; split's rows are pulled one step ahead (at step n for the slot of step
+ *   n + 1), 32 targets per warp, by every block, each target's sum added to its
+ *   arrival slot with one reduction. NULL: ptr's rows hold every link, all
+ *   pulled by the target's block in the step. */
 typedef struct n2b_connection {
     int32_t src;
     int32_t tgt;

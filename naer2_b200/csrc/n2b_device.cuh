@@ -70,13 +70,16 @@ struct alignas(16) ConnDev {
     int32_t src_bit_mask, src_words, has_split, staged;  // staged (pull): link (and w) 16-byte aligned
     long long wfx;        // homogeneous weight, fixed point of the target
     float wscale;         // 2^shift of the target (exact)
-    float pad2;
+    int32_t item0;        // pull with split: its first item (32 targets each) of the grid-wide pull
+    int32_t n_items;      // ... and its items (0: none)
+    int32_t ring_off;     // pull: word offset of its source ring's copy in the ring cache (-1: not cached)
     const int32_t *ptr;
     const uint32_t *link;
     const float *w;
     long long *tgt_acc;
     const uint32_t *src_bits;
-    const int32_t *split;  // push: per source, its row's first link of delay >= 2 (NULL: none deferred)
+    const int32_t *split;  // push: per source, its row's first link of delay >= 2 (NULL: none deferred);
+                           // pull: the delay >= 2 rows' offsets (NULL: ptr's rows hold every link)
 };
 
 struct StepArgs {
@@ -97,6 +100,9 @@ struct StepArgs {
     int32_t trace_steps;
     int32_t pull_staged;   // the launch has a PullStage per warp in dynamic shared memory
     int32_t ring_cache_words;  // ... and after them a copy of a pull source's spike-bit ring of at most this size
+    int32_t ring_cache_all;    // every pull source's ring fits the cache at its ring_off (the grid-wide pull)
+    int32_t pull_items;        // items of the grid-wide pull (the delay >= 2 rows, 32 targets each)
+    int32_t n_pull;
     int32_t item_cap;
     int32_t n_tiles;
     int32_t offset;        // this launch's step = *step + offset (per-step launches)
@@ -302,58 +308,32 @@ __device__ __forceinline__ bool pd14(const PopDev &P, float in, float &v, float 
     return fire;
 }
 
-// ------------------------------------------------------------------ pull intake
-
-// Every pull connection into the population: each warp walks the incoming
-// rows of its 32 neurons one after another, the lanes striding a row
-// (coalesced link loads), testing each link's source bit in the ring row of
-// step n - delay; the warp's sum lands in the row's owner lane. The plain walk:
-// used for connections whose rows are not 16-byte aligned, and where the launch
-// has no staging memory.
-template <bool INL>
-__device__ __forceinline__ long long pull_walk(const ConnDev &C, const uint32_t *ring, int32_t *err,
-                                               unsigned long long *events, int wbase, int nq, long long n) {
-    const int lane = threadIdx.x & 31;
-    long long mine = 0;
-    unsigned hits = 0;
-    for (int q = 0; q < nq; ++q) {
-        const int jq = wbase + q;
-        const int r0 = __ldg(C.ptr + jq), r1 = __ldg(C.ptr + jq + 1);
-        long long part = 0;
-        for (int l = r0 + lane; l < r1; l += 32) {
-            const uint32_t rec = __ldg(C.link + l);
-            const int d = (int)(rec >> 24), s = (int)(rec & 0xFFFFFFu);
-            if (d >= 1 && d <= C.src_bit_mask && s < C.src_n) {
-                const size_t at = (size_t)((n - d) & C.src_bit_mask) * C.src_words + (s >> 5);
-                const uint32_t word = ring ? ring[at] : __ldcg(C.src_bits + at);
-                if ((word >> (s & 31)) & 1u) {
-                    part += C.homogeneous ? C.wfx : weight_fx(__ldg(C.w + l), C.wscale);
-                    ++hits;
-                }
-            } else {
-                atomicAdd(err + 1, 1);
-            }
-        }
-        part = warp_sum64(part);
-        if (lane == q) mine += part;
-    }
-    hits = __reduce_add_sync(FULL, hits);
-    if (lane == 0 && hits) atomicAdd(events, (unsigned long long)hits);
-    return mine;
+// One synaptic event: a 64-bit reduction into an arrival slot, issued as a reduction (no value comes back).
+// No memory clobber: nothing in the step reads an arrival slot after adding to it before the step's barrier
+// (a grid barrier or the launch boundary), which orders the slot's reads.
+__device__ __forceinline__ void red_add_u64(long long *p, long long v) {
+    asm volatile("red.global.add.u64 [%0], %1;" ::"l"(p), "l"(v));
 }
 
-// The staged pull (the reference's pull intake, fused.py:1626-1965, with its link runs staged through shared
-// memory): the warp's incoming links -- one contiguous range of the pull CSR, rows of its 32 neurons -- stream
-// into shared memory by 1-D bulk copies (cp.async.bulk, completion counted on an mbarrier), PULL_CH links per
-// chunk, two chunks in flight; the lanes gather the staged links against the source's spike-bit ring. Only
-// this GPU's own memory is read, and no copy is multicast. The range's 16-byte aligned interior is copied;
-// its ragged head and tail (fewer than 4 links each) are loaded directly. Each lane sweeps its links in
-// increasing order, following the rows by their offsets (kept in shared memory), and adds a row's partial sum
-// into the row's shared slot when it leaves the row.
+// ------------------------------------------------------------------ pull intake
+
+// The pull (the reference's pull intake, fused.py:1626-1965, with its link runs staged through shared memory):
+// a warp takes the incoming rows of 32 consecutive targets of one connection -- one contiguous range of the
+// pull CSR -- streamed into shared memory by 1-D bulk copies (cp.async.bulk, completion counted on an
+// mbarrier), PULL_CH links per chunk, PULL_BUFS chunks in flight, and gathers the staged links against the
+// source's spike-bit ring (copied to shared memory when small). Only this GPU's own memory is read, and no copy
+// is multicast. The range's 16-byte aligned interior is copied; its ragged head and tail (fewer than 4 links
+// each) are loaded directly, as is every link of a connection whose arrays are not 16-byte aligned. Each lane
+// sweeps its links (lane, lane + 32, ...) in increasing order, following the rows by their offsets (in shared
+// memory, the current row's end in a register), counts a row's links whose source spiked and adds the row's
+// sum into the row's shared slot when it leaves the row.
+// Two pulls use it: the delay-1 rows (every row without a split) by the target's own block in the step, and
+// the delay >= 2 rows of split connections one step ahead, by every warp of the grid (pull_far_phase).
 constexpr int PULL_CH = 256;                        // links per staging chunk
 constexpr int PULL_BUFS = 2;                        // chunks in flight per warp
-constexpr int RING_CACHE_MAX = 8192;                // words of a pull source's ring copied to shared memory, at most
+constexpr int RING_CACHE_MAX = 8192;                // words of pull sources' rings copied to shared memory, at most
 constexpr unsigned PULL_WAIT_POLLS = 1u << 22;      // polls of a chunk's mbarrier before it counts as lost
+constexpr int PULL_BATCH = 4;                       // links per lane whose spike-bit words are loaded together
 
 struct alignas(16) PullStage {  // one per warp, in dynamic shared memory
     uint32_t link[PULL_BUFS][PULL_CH];
@@ -362,7 +342,7 @@ struct alignas(16) PullStage {  // one per warp, in dynamic shared memory
     long long sum[32];
     int32_t ptr[33];
     uint32_t uses[PULL_BUFS];   // completions of each buffer's mbarrier so far (its next parity)
-    int32_t broken;     // a chunk was lost: the rest of the launch walks instead of staging
+    int32_t broken;     // a chunk was lost: the rest of the launch loads links directly
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -399,9 +379,8 @@ __device__ __forceinline__ void pull_issue(PullStage *st, const ConnDev &C, int 
                      : "memory");
 }
 
-// Every lane: wait (bounded) until buffer b's chunk has landed; false if it did not within the limit. The wait
-// polls with the non-blocking mbarrier.test_wait: try_wait may suspend the warp for a time slice before it
-// looks again, which measured ~3.7 us per chunk here against well under a microsecond of copy.
+// Every lane: wait (bounded) until buffer b's chunk has landed; false if it did not within the limit. Polls with
+// the non-blocking mbarrier.test_wait.
 __device__ __forceinline__ bool pull_wait(PullStage *st, int b) {
     const uint32_t bar = smem_u32(&st->bar[b]);
     const uint32_t parity = st->uses[b] & 1u;
@@ -417,102 +396,106 @@ __device__ __forceinline__ bool pull_wait(PullStage *st, int b) {
     return false;
 }
 
+// One warp's sweep state and constants. HOMOG: one weight for every link (rows counted, the sum made at the
+// row's end); RING: the source's ring is the shared-memory copy.
+template <bool HOMOG, bool RING>
 struct PullSweep {
-    int q;          // the lane's current row (warp-relative)
-    long long part; // its partial sum in that row
-    unsigned hits;  // links whose source spiked (the synaptic events of the pull)
+    const uint32_t *ring;  // the source's spike-bit ring (shared-memory copy or global)
+    PullStage *st;
+    int nlo, mask, words, src_n, min_d;
+    long long wfx;
+    float wscale;
+    int q, end;       // the lane's current row (warp-relative) and its end
+    long long part;   // per-link weights: the row's partial sum
+    int cnt;          // single weight: the row's spiking links
+    unsigned hits;    // links whose source spiked (the synaptic events of the pull)
+    int bad;          // links out of range
+
+    __device__ __forceinline__ uint32_t bits(uint32_t rec, bool &ok) const {
+        const int d = (int)(rec >> 24), s = (int)(rec & 0xFFFFFFu);
+        ok = d >= min_d && d <= mask && s < src_n;
+        const int at = ((nlo - d) & mask) * words + (s >> 5);
+        return ok ? (RING ? ring[at] : __ldcg(ring + at)) : 0u;
+    }
+
+    __device__ __forceinline__ void flush() {
+        if (HOMOG) {
+            if (cnt) atomicAdd(reinterpret_cast<unsigned long long *>(&st->sum[q]), (unsigned long long)(cnt * wfx));
+            cnt = 0;
+        } else {
+            if (part) atomicAdd(reinterpret_cast<unsigned long long *>(&st->sum[q]), (unsigned long long)part);
+            part = 0;
+        }
+    }
+
+    __device__ __forceinline__ void apply(int l, uint32_t rec, uint32_t word, bool ok, float w) {
+        while (l >= end) {  // left the row (rows may be empty)
+            flush();
+            ++q;
+            end = st->ptr[q + 1];
+        }
+        if (!ok) {
+            ++bad;
+            return;
+        }
+        const unsigned hit = (word >> (rec & 31u)) & 1u;  // rec & 31 = s & 31 (the index is the low 24 bits)
+        hits += hit;
+        if (HOMOG) cnt += (int)hit;
+        else if (hit) part += weight_fx(w, wscale);
+    }
 };
 
-constexpr int PULL_BATCH = 4;  // staged links per lane whose spike-bit words are loaded together
-
-// Whether a link word is in range, and its source's spike-bit word of step n - delay. A plain load (cached in
-// L1): the ring rows a pull reads were written before the last grid barrier or launch boundary, whose acquire
-// makes them visible to the block, and a source's ring is small, so its rows stay in L1 across a warp's links.
-// ring: the source's ring copied into shared memory for this connection (small rings), else null.
-__device__ __forceinline__ uint32_t pull_bits(const ConnDev &C, const uint32_t *ring, uint32_t rec, long long n,
-                                              bool &ok) {
-    const int d = (int)(rec >> 24), s = (int)(rec & 0xFFFFFFu);
-    ok = d >= 1 && d <= C.src_bit_mask && s < C.src_n;
-    if (!ok) return 0u;
-    const size_t at = (size_t)((n - d) & C.src_bit_mask) * C.src_words + (s >> 5);
-    return ring ? ring[at] : C.src_bits[at];
-}
-
-// Link l (the lane's links in increasing order) into the lane's row sums: leave the rows l is past, then add.
-__device__ __forceinline__ void pull_apply(const ConnDev &C, PullStage *st, int32_t *err, PullSweep &sw, int l,
-                                           uint32_t rec, uint32_t word, bool ok, float w) {
-    while (l >= st->ptr[sw.q + 1]) {  // left the row (rows may be empty)
-        if (sw.part) atomicAdd(reinterpret_cast<unsigned long long *>(&st->sum[sw.q]), (unsigned long long)sw.part);
-        sw.part = 0;
-        ++sw.q;
-    }
-    if (!ok) {
-        atomicAdd(err + 1, 1);
-        return;
-    }
-    const int s = (int)(rec & 0xFFFFFFu);
-    if ((word >> (s & 31)) & 1u) {
-        sw.part += C.homogeneous ? C.wfx : weight_fx(w, C.wscale);
-        ++sw.hits;
-    }
-}
-
-__device__ __forceinline__ void pull_link(const ConnDev &C, const uint32_t *ring, PullStage *st, int32_t *err,
-                                          PullSweep &sw, int l, uint32_t rec, float w, long long n) {
-    bool ok;
-    const uint32_t word = pull_bits(C, ring, rec, n, ok);
-    pull_apply(C, st, err, sw, l, rec, word, ok, w);
-}
-
-// The links [c0, c1) of a landed chunk in buffer b, PULL_BATCH per lane at a time: their bit words all in
-// flight before any is used.
-__device__ __forceinline__ void pull_chunk(const ConnDev &C, const uint32_t *ring, PullStage *st, int32_t *err,
-                                           PullSweep &sw, int b, int c0, int c1, long long n) {
+// The rows [t0, t0 + nq) of `rows` (ptr, or split's delay >= 2 rows) of connection C against the ring rows of
+// steps n_read - d; returns the lane's own row sum (lanes < nq).
+template <bool HOMOG, bool RING>
+__device__ __forceinline__ long long pull_rows(const ConnDev &C, const uint32_t *ring, PullStage *st, int32_t *err,
+                                               unsigned long long *events, const int32_t *rows, int t0, int nq,
+                                               long long n_read, int min_d) {
     const int lane = threadIdx.x & 31;
-    for (int base = c0 + lane; base < c1; base += 32 * PULL_BATCH) {
+    if (lane <= nq) st->ptr[lane] = __ldg(rows + t0 + lane);
+    if (lane == 0 && nq == 32) st->ptr[32] = __ldg(rows + t0 + 32);
+    st->sum[lane] = 0;
+    __syncwarp();
+    PullSweep<HOMOG, RING> sw;
+    sw.ring = ring;
+    sw.st = st;
+    sw.nlo = (int)n_read;  // the ring rows' index mod the depth: only the low bits matter
+    sw.mask = C.src_bit_mask;
+    sw.words = C.src_words;
+    sw.src_n = C.src_n;
+    sw.min_d = min_d;
+    sw.wfx = C.wfx;
+    sw.wscale = C.wscale;
+    sw.q = 0;
+    sw.end = st->ptr[1];
+    sw.part = 0;
+    sw.cnt = 0;
+    sw.hits = 0;
+    sw.bad = 0;
+    const int L0 = st->ptr[0], L1 = st->ptr[nq];
+    const bool staged = C.staged && !st->broken;
+    int a0 = (L0 + 3) & ~3, a1 = L1 & ~3;
+    if (!staged || a1 <= a0) a0 = a1 = L1;  // nothing to stage: every link loaded directly
+    const int n_chunks = (a1 - a0 + PULL_CH - 1) / PULL_CH;
+    if (lane == 0)
+        for (int k = 0; k < PULL_BUFS && k < n_chunks; ++k) pull_issue(st, C, a0, a1, k);
+    // the head (or every link): direct loads, PULL_BATCH per lane in flight
+    for (int base = L0 + lane; base < a0; base += 32 * PULL_BATCH) {
         uint32_t rec[PULL_BATCH], word[PULL_BATCH];
         float w[PULL_BATCH];
         bool ok[PULL_BATCH];
 #pragma unroll
-        for (int q = 0; q < PULL_BATCH; ++q) {
-            const int l = base + 32 * q;
-            rec[q] = 0u;
-            w[q] = 0.f;
-            word[q] = 0u;
-            ok[q] = false;
-            if (l < c1) {
-                rec[q] = st->link[b][l - c0];
-                w[q] = C.homogeneous ? 0.f : st->w[b][l - c0];
-                word[q] = pull_bits(C, ring, rec[q], n, ok[q]);
-            }
+        for (int k = 0; k < PULL_BATCH; ++k) {
+            const int l = base + 32 * k;
+            rec[k] = l < a0 ? __ldg(C.link + l) : 0u;
+            w[k] = (!HOMOG && l < a0) ? __ldg(C.w + l) : 0.f;
         }
 #pragma unroll
-        for (int q = 0; q < PULL_BATCH; ++q) {
-            const int l = base + 32 * q;
-            if (l < c1) pull_apply(C, st, err, sw, l, rec[q], word[q], ok[q], w[q]);
-        }
+        for (int k = 0; k < PULL_BATCH; ++k) word[k] = sw.bits(rec[k], ok[k]);
+#pragma unroll
+        for (int k = 0; k < PULL_BATCH; ++k)
+            if (base + 32 * k < a0) sw.apply(base + 32 * k, rec[k], word[k], ok[k], w[k]);
     }
-}
-
-// One connection's intake of the warp's nq rows (from neuron wbase); returns the lane's own row sum.
-template <bool INL>
-__device__ __forceinline__ long long pull_staged(const ConnDev &C, const uint32_t *ring, PullStage *st, int32_t *err,
-                                                 unsigned long long *events, int wbase, int nq, long long n) {
-    const int lane = threadIdx.x & 31;
-    if (lane <= nq) st->ptr[lane] = __ldg(C.ptr + wbase + lane);
-    if (lane == 0 && nq == 32) st->ptr[32] = __ldg(C.ptr + wbase + 32);
-    st->sum[lane] = 0;
-    __syncwarp();
-    const int L0 = st->ptr[0], L1 = st->ptr[nq];
-    int a0 = (L0 + 3) & ~3, a1 = L1 & ~3;
-    if (a1 <= a0) a0 = a1 = L1;  // too short to stage: every link loaded directly
-    const int n_chunks = (a1 - a0 + PULL_CH - 1) / PULL_CH;
-    if (lane == 0) {
-        for (int k = 0; k < PULL_BUFS && k < n_chunks; ++k) pull_issue(st, C, a0, a1, k);
-    }
-    PullSweep sw{0, 0, 0u};
-    for (int l = L0 + lane; l < a0; l += 32)  // the head
-        pull_link(C, ring, st, err, sw, l, __ldg(C.link + l), C.homogeneous ? 0.f : __ldg(C.w + l), n);
     bool lost = false;
     for (int k = 0; k < n_chunks; ++k) {
         const int b = k % PULL_BUFS;
@@ -520,62 +503,130 @@ __device__ __forceinline__ long long pull_staged(const ConnDev &C, const uint32_
         if (!lost && !pull_wait(st, b)) lost = true;
         __syncwarp();
         if (lane == 0) st->uses[b] += 1;
-        if (lost) {  // the chunk did not land in time: its links (and the rest) loaded directly
-            for (int l = c0 + lane; l < c1; l += 32)
-                pull_link(C, ring, st, err, sw, l, __ldg(C.link + l), C.homogeneous ? 0.f : __ldg(C.w + l), n);
-            continue;
+        for (int base = c0 + lane; base < c1; base += 32 * PULL_BATCH) {
+            uint32_t rec[PULL_BATCH], word[PULL_BATCH];
+            float w[PULL_BATCH];
+            bool ok[PULL_BATCH];
+#pragma unroll
+            for (int q = 0; q < PULL_BATCH; ++q) {
+                const int l = base + 32 * q;
+                rec[q] = 0u;
+                w[q] = 0.f;
+                if (l < c1) {  // a lost chunk (did not land in time): its links loaded directly
+                    rec[q] = lost ? __ldg(C.link + l) : st->link[b][l - c0];
+                    if (!HOMOG) w[q] = lost ? __ldg(C.w + l) : st->w[b][l - c0];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < PULL_BATCH; ++q) word[q] = sw.bits(rec[q], ok[q]);
+#pragma unroll
+            for (int q = 0; q < PULL_BATCH; ++q)
+                if (base + 32 * q < c1) sw.apply(base + 32 * q, rec[q], word[q], ok[q], w[q]);
         }
-        pull_chunk(C, ring, st, err, sw, b, c0, c1, n);
         __syncwarp();  // every lane done with buffer b before it is refilled
-        if (lane == 0 && k + PULL_BUFS < n_chunks) pull_issue(st, C, a0, a1, k + PULL_BUFS);
+        if (!lost && lane == 0 && k + PULL_BUFS < n_chunks) pull_issue(st, C, a0, a1, k + PULL_BUFS);
     }
-    if (lost) {
-        if (lane == 0) {
-            atomicAdd(err + 5, 1);
-            st->broken = 1;
-        }
+    if (lost && lane == 0) {
+        atomicAdd(err + 5, 1);
+        st->broken = 1;
     }
-    for (int l = max(a1, L0) + lane; l < L1; l += 32)  // the tail
-        pull_link(C, ring, st, err, sw, l, __ldg(C.link + l), C.homogeneous ? 0.f : __ldg(C.w + l), n);
-    if (sw.part) atomicAdd(reinterpret_cast<unsigned long long *>(&st->sum[sw.q]), (unsigned long long)sw.part);
+    for (int base = max(a1, L0) + lane; base < L1; base += 32) {  // the tail (fewer than 4 links)
+        const uint32_t rec = __ldg(C.link + base);
+        bool ok;
+        const uint32_t word = sw.bits(rec, ok);
+        sw.apply(base, rec, word, ok, HOMOG ? 0.f : __ldg(C.w + base));
+    }
+    sw.flush();
     const unsigned hits = __reduce_add_sync(FULL, sw.hits);
-    if (lane == 0 && hits) atomicAdd(events, (unsigned long long)hits);
+    const int bad = __reduce_add_sync(FULL, sw.bad);
+    if (lane == 0) {
+        if (hits) atomicAdd(events, (unsigned long long)hits);
+        if (bad) atomicAdd(err + 1, bad);
+    }
     __syncwarp();
     const long long mine = lane < nq ? st->sum[lane] : 0;
     __syncwarp();
     return mine;
 }
 
-// Every pull connection into the tile's population (called by every thread of the block). A source whose
-// whole spike-bit ring fits the launch's ring cache (a.ring_cache_words, in dynamic shared memory after the
-// warps' PullStages) is copied there first -- its rows of steps before n are final, the row of step n is not
-// read -- so that the links' bit tests are shared-memory loads.
+template <bool RING>
+__device__ __forceinline__ long long pull_rows_any(const ConnDev &C, const uint32_t *ring, PullStage *st,
+                                                   int32_t *err, unsigned long long *events, const int32_t *rows,
+                                                   int t0, int nq, long long n_read, int min_d) {
+    return C.homogeneous ? pull_rows<true, RING>(C, ring, st, err, events, rows, t0, nq, n_read, min_d)
+                         : pull_rows<false, RING>(C, ring, st, err, events, rows, t0, nq, n_read, min_d);
+}
+
+// The launch's ring cache, after the warps' PullStages in dynamic shared memory.
+__device__ __forceinline__ uint32_t *ring_cache() {
+    extern __shared__ __align__(128) unsigned char n2b_dyn_smem[];
+    return reinterpret_cast<uint32_t *>(reinterpret_cast<PullStage *>(n2b_dyn_smem) + (blockDim.x >> 5));
+}
+
+__device__ __forceinline__ void copy_ring(uint32_t *dst, const ConnDev &C) {
+    const int words = (C.src_bit_mask + 1) * C.src_words;
+    for (int k = threadIdx.x; k < words; k += blockDim.x) dst[k] = __ldcg(C.src_bits + k);
+}
+
+// The in-step pull of the tile's population (every thread of the block): each pull connection's rows of ptr --
+// all its links, or, with a split, its delay-1 links -- for the warp's 32 neurons, against ring rows n - d. A
+// source whose whole ring fits the ring cache is copied there first (its rows of steps before n are final).
 template <bool INL>
 __device__ __forceinline__ long long pull_intake(const StepArgs &a, const PopDev &P, int first, int count,
                                                  long long n, PullStage *stage) {
-    extern __shared__ __align__(128) unsigned char n2b_dyn_smem[];
     const int wbase = first + (threadIdx.x & ~31);
     const int nq = min(32, first + count - wbase);
     long long mine = 0;
     for (int c = P.pull_first; c < P.pull_first + P.n_pull; ++c) {
         const ConnDev &C = pull_at<INL>(a, c);
         const int ring_words = (C.src_bit_mask + 1) * C.src_words;
-        const uint32_t *ring = nullptr;
-        if (stage != nullptr && ring_words <= a.ring_cache_words) {  // the same for every thread of the block
-            uint32_t *cache = reinterpret_cast<uint32_t *>(reinterpret_cast<PullStage *>(n2b_dyn_smem) +
-                                                           (blockDim.x >> 5));
+        const bool cached = ring_words <= a.ring_cache_words;  // the same for every thread of the block
+        uint32_t *cache = ring_cache();
+        if (cached) {
             __syncthreads();  // every warp done with the cache's previous ring
-            for (int k = threadIdx.x; k < ring_words; k += blockDim.x) cache[k] = __ldcg(C.src_bits + k);
+            copy_ring(cache, C);
             __syncthreads();
-            ring = cache;
         }
         if (nq <= 0) continue;
-        if (stage != nullptr && C.staged && !stage->broken)
-            mine += pull_staged<INL>(C, ring, stage, a.err, a.counters, wbase, nq, n);
-        else
-            mine += pull_walk<INL>(C, ring, a.err, a.counters, wbase, nq, n);
+        // (a network with pull connections always has its PullStages: the launch's dynamic shared memory)
+        mine += cached ? pull_rows_any<true>(C, cache, stage, a.err, a.counters, C.ptr, wbase, nq, n, 1)
+                       : pull_rows_any<false>(C, C.src_bits, stage, a.err, a.counters, C.ptr, wbase, nq, n, 1);
     }
     return mine;
+}
+
+// The grid-wide pull (every thread of every block, after the step's far items): the delay >= 2 rows of every
+// split pull connection, for the arrival slot of step n + 1 -- ring rows (n + 1) - d, d >= 2, all written
+// before this step -- 32 targets per warp, warps taking items grid-stride, each target's sum added to its slot
+// with one reduction (slot n + 1 is read after the step's barrier). With every pull source's ring in the cache
+// together, the block copies them all first.
+template <int NPB, bool INL>
+__device__ __forceinline__ void pull_far_phase(const StepArgs &a, const long long n, PullStage *stage) {
+    if (a.pull_items == 0 || stage == nullptr) return;  // the same for every thread of the launch
+    uint32_t *cache = ring_cache();
+    if (a.ring_cache_all) {
+        __syncthreads();
+        for (int c = 0; c < a.n_pull; ++c) {
+            const ConnDev &C = pull_at<INL>(a, c);
+            if (C.n_items > 0 && C.ring_off >= 0) copy_ring(cache + C.ring_off, C);
+        }
+        __syncthreads();
+    }
+    const int lane = threadIdx.x & 31;
+    const int W = (int)gridDim.x * (NPB / 32);
+    int c = 0;
+    for (int it = (int)blockIdx.x * (NPB / 32) + (int)(threadIdx.x >> 5); it < a.pull_items; it += W) {
+        while (c + 1 < a.n_pull && !(it >= pull_at<INL>(a, c).item0 &&
+                                     it < pull_at<INL>(a, c).item0 + pull_at<INL>(a, c).n_items))
+            ++c;  // items rise with the connection index: the search moves forward only
+        const ConnDev &C = pull_at<INL>(a, c);
+        const int t0 = (it - C.item0) * 32, nq = min(32, C.tgt_n - t0);
+        const bool cached = a.ring_cache_all && C.ring_off >= 0;
+        const long long sum =
+            cached ? pull_rows_any<true>(C, cache + C.ring_off, stage, a.err, a.counters, C.split, t0, nq, n + 1, 2)
+                   : pull_rows_any<false>(C, C.src_bits, stage, a.err, a.counters, C.split, t0, nq, n + 1, 2);
+        if (lane < nq && sum) red_add_u64(C.tgt_acc + (size_t)((n + 1) & C.tgt_acc_mask) * (size_t)C.tgt_n + t0 + lane, sum);
+    }
 }
 
 // ------------------------------------------------------------------ delivery
@@ -625,12 +676,6 @@ __device__ __forceinline__ float link_weight(const C_ &C, int l) {
     return C.homogeneous ? 0.f : __ldg(C.w + l);
 }
 
-// One synaptic event: a 64-bit reduction into an arrival slot, issued as a reduction (no value comes back).
-// No memory clobber: nothing in the step reads an arrival slot after adding to it before the step's barrier
-// (a grid barrier or the launch boundary), which orders the slot's reads.
-__device__ __forceinline__ void red_add_u64(long long *p, long long v) {
-    asm volatile("red.global.add.u64 [%0], %1;" ::"l"(p), "l"(v));
-}
 
 // One link word (and its weight) into the target's arrival slot (n + delay) mod D; out-of-range links
 // counted, not written.
@@ -1069,6 +1114,7 @@ __device__ __forceinline__ void step_body(const StepArgs &a, const long long n, 
     }
     N2B_STAMP(a, k, 2);
     far_phase<NPB, INL, FG>(a, n, s_conn, far_n);
+    if (PULL) pull_far_phase<NPB, INL>(a, n, stage);
     N2B_STAMP(a, k, 3);
 }
 

@@ -141,7 +141,6 @@ int validate(const n2b_population *pops, int32_t n_pops, const n2b_connection *c
         if (T.n > 0 && (!T.acc || !pow2(T.acc_depth))) return fail(N2B_EINVAL, at + "target has no arrival slots");
         if (C.mode == N2B_PULL && S.n > 0 && (!S.bits || !pow2(S.bit_depth)))
             return fail(N2B_EINVAL, at + "a pull connection needs the source's spike-bit ring");
-        if (C.mode == N2B_PULL && C.split) return fail(N2B_EINVAL, at + "split is for push connections");
         if (S.n > 0 && (int64_t)C.n_links > ((int64_t)1 << 31) - 1) return fail(N2B_EINVAL, at + "more than 2^31 links");
     }
     return N2B_OK;
@@ -327,8 +326,9 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
         D.w = C.w;
         D.tgt_acc = reinterpret_cast<long long *>(T.acc);
         D.src_bits = S.bits;
-        D.has_split = C.mode == N2B_PUSH && C.split != nullptr;
-        D.split = C.mode == N2B_PUSH ? C.split : nullptr;
+        D.has_split = C.split != nullptr;
+        D.split = C.split;
+        D.ring_off = -1;
         // pull rows stream through shared memory by bulk copies, which need 16-byte aligned sources
         D.staged = C.mode == N2B_PULL && (reinterpret_cast<uintptr_t>(C.link) & 15) == 0 &&
                    (C.w == nullptr || (reinterpret_cast<uintptr_t>(C.w) & 15) == 0);
@@ -344,6 +344,27 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
             if (conns[c].mode == N2B_PULL && conns[c].tgt == p) pull.push_back(conn_dev(conns[c]));
         pd[p].n_pull = (int32_t)pull.size() - pd[p].pull_first;
     }
+    // the pull: a PullStage per warp in dynamic shared memory when the network has pull connections, and after
+    // them a ring cache -- for the largest pull source's spike-bit ring (the in-step pull, one connection at a
+    // time) and, when they fit together, every split connection's source ring at its ring_off (the grid-wide
+    // pull), up to RING_CACHE_MAX words; the grid-wide pull's items, 32 targets each, numbered by connection
+    int32_t max_ring = 0, total_ring = 0, pull_items = 0;
+    for (n2b::ConnDev &C : pull) {
+        const int32_t w = (C.src_bit_mask + 1) * C.src_words;
+        max_ring = std::max(max_ring, w);
+        if (C.has_split) {
+            C.ring_off = total_ring;
+            total_ring += w;
+            C.item0 = pull_items;
+            C.n_items = (C.tgt_n + 31) / 32;
+            pull_items += C.n_items;
+        }
+    }
+    const int32_t ring_words = max_ring <= n2b::RING_CACHE_MAX ? max_ring : 0;  // 0: sources read from global
+    const bool ring_all = total_ring > 0 && total_ring <= n2b::RING_CACHE_MAX;
+    if (!ring_all)
+        for (n2b::ConnDev &C : pull) C.ring_off = -1;
+    const int32_t cache_words = std::max(ring_words, ring_all ? total_ring : 0);
     // tiles: the largest populations' first (their blocks start first)
     std::vector<int32_t> order(n_pops);
     for (int32_t p = 0; p < n_pops; ++p) order[p] = p;
@@ -388,12 +409,7 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     int want = (opt && opt->grid > 0) ? opt->grid
                                       : (persistent ? std::max(sms, L.n_tiles + sms / 2) : 2 * sms);
     int grid = std::max(L.n_tiles, want);
-    // the staged pull: a PullStage per warp in dynamic shared memory, when the network has pull connections, and
-    // after them a cache for the largest pull source's spike-bit ring up to RING_CACHE_MAX words
-    int32_t ring_words = 0;
-    for (const n2b::ConnDev &C : pull) ring_words = std::max(ring_words, (C.src_bit_mask + 1) * C.src_words);
-    if (ring_words > n2b::RING_CACHE_MAX) ring_words = 0;  // too large: every source read from global memory
-    const size_t dyn = pull.empty() ? 0 : sizeof(n2b::PullStage) * (size_t)(block / 32) + sizeof(uint32_t) * ring_words;
+    const size_t dyn = pull.empty() ? 0 : sizeof(n2b::PullStage) * (size_t)(block / 32) + sizeof(uint32_t) * cache_words;
     int most = 0;
     int rc2 = coresident_blocks(block, inl, false, device, dyn, &most);  // also raises the kernels' dynamic limit
     if (rc2) return rc2;
@@ -443,6 +459,9 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
                                                          : n2b::BAR_LIMIT_NS;
     a.pull_staged = dyn > 0;
     a.ring_cache_words = ring_words;
+    a.ring_cache_all = ring_all;
+    a.pull_items = pull_items;
+    a.n_pull = (int32_t)pull.size();
     a.n_pops = n_pops;
     a.n_push = L.n_push;
     if (inl) {

@@ -32,7 +32,7 @@ import torch
 
 from . import _lib
 from .models import params_of
-from .topology import delay_steps, pack_links, pull_form, push_form
+from .topology import delay_steps, pack_links, pull_split_form, push_form
 
 MAX_SHIFT = 40
 
@@ -199,7 +199,7 @@ def describe(net, modes: dict | None = None, forms: bool = True) -> NetDesc:
                                   steps=steps, warr=warr))
             continue
         if mode == "pull":
-            ptr, link, perm = pull_form(topo, steps, n_tgt)
+            ptr, link, perm, split = pull_split_form(topo, steps, n_tgt)
         elif mode == "push":
             ptr, link, perm, split = push_form(topo, steps, n_tgt)
         else:

@@ -185,6 +185,31 @@ def push_form(topo: Topology, steps: torch.Tensor, n_tgt: int):
     return off.to(torch.int32), pack_links(tgt[perm], steps[perm]), perm, split
 
 
+def pull_split_form(topo: Topology, steps: torch.Tensor, n_tgt: int):
+    """(ptr int32 [n_tgt + 1], link int32 [n_links], perm int64 [n_links], fptr int32 [n_tgt + 1]): the pull
+    form in two parts of one link array: first every target's delay-1 links (rows ptr[j]..ptr[j+1], pulled in
+    the step itself), then every target's links of delay >= 2 (rows fptr[j]..fptr[j+1], fptr[0] = ptr[n_tgt],
+    pulled one step ahead by any block); canonical order within a row; perm[k] is the canonical link at
+    position k."""
+    tgt = topo.target_indices
+    off = topo.source_offsets.to(tgt.device)
+    steps = steps.to(tgt.device)
+    src = _rows(off)
+    far = (steps >= 2).to(torch.int64)
+    perm = torch.argsort(far * n_tgt + tgt, stable=True)
+    if tgt.numel():
+        near_counts = torch.bincount(tgt[far == 0], minlength=n_tgt)
+        far_counts = torch.bincount(tgt[far == 1], minlength=n_tgt)
+    else:
+        near_counts = far_counts = torch.zeros(n_tgt, dtype=torch.int64, device=tgt.device)
+    ptr = torch.zeros(n_tgt + 1, dtype=torch.int64, device=tgt.device)
+    ptr[1:] = torch.cumsum(near_counts, 0)
+    fptr = torch.zeros(n_tgt + 1, dtype=torch.int64, device=tgt.device)
+    fptr[1:] = torch.cumsum(far_counts, 0)
+    fptr += ptr[-1]
+    return ptr.to(torch.int32), pack_links(src[perm], steps[perm]), perm, fptr.to(torch.int32)
+
+
 def pull_form(topo: Topology, steps: torch.Tensor, n_tgt: int):
     """(ptr int32 [n_tgt + 1], link int32 [n_links], perm int64 [n_links]): the links sorted by target (stable:
     canonical order within a target); perm[k] is the canonical link at pull position k."""

@@ -13,7 +13,7 @@ from naer2_b200.models import LIF, PD14_neuron, Poisson_source, params_of
 from naer2_b200.networks import brunel
 from naer2_b200.patterns import all_to_all, fixed_indegree, fixed_outdegree, one_to_one
 from naer2_b200.runtime import describe, fixed_shift, next_pow2
-from naer2_b200.topology import Topology, delay_steps, pull_form, push_form
+from naer2_b200.topology import Topology, delay_steps, pull_form, pull_split_form, push_form
 from naer2_b200.types import IndexBox, Points, Region
 
 
@@ -185,6 +185,13 @@ def test_push_and_pull_forms():
     assert pperm.tolist() == [1, 4, 2, 0, 3]
     with pytest.raises(ValueError):
         push_form(topo, torch.from_numpy(steps), 2)  # a target outside the population
+    # the split pull form: every target's delay-1 links, then every target's delay >= 2 links
+    sptr, slink, sperm, fptr = pull_split_form(topo, torch.from_numpy(steps), 3)
+    assert sptr.tolist() == [0, 1, 1, 2] and fptr.tolist() == [2, 3, 4, 5]
+    sw = slink.to(torch.int64) & 0xFFFFFFFF
+    assert (sw >> 24).tolist() == [1, 1, 4, 2, 3] and (sw & 0xFFFFFF).tolist() == [0, 1, 1, 0, 0]
+    assert sperm.tolist() == [1, 3, 4, 2, 0]
+    assert sorted(sperm.tolist()) == list(range(5))
 
 
 def test_describe_brunel():
