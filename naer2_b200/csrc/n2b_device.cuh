@@ -8,8 +8,9 @@
 // over the blocks; every block then shares the far deliveries of step n - 1.
 //   1. intake: each neuron's due arrival slot acc[n mod D][j] (int64 fixed
 //      point, read and cleared), plus every pull connection's gather of its
-//      incoming links against the source's spike-bit ring, plus the external
-//      Poisson events -- all one exact integer sum, converted to float once;
+//      incoming links (its delay-1 links where the connection is split)
+//      against the source's spike-bit ring, plus the external Poisson events
+//      -- all one exact integer sum, converted to float once;
 //   2. the model's update and send (one thread per neuron);
 //   3. spike-ring write: one __ballot_sync word per warp into the bit ring
 //      (and the raster), the warp's spikes compacted with __popc into the
@@ -22,7 +23,11 @@
 //   5. far delivery: every block takes items of step n - 1's list (grid
 //      stride, from the last block down: blocks without a tile first), one
 //      link per thread, into slots (n - 1 + delay) mod D, all >= n + 1:
-//      never the slot this step reads.
+//      never the slot this step reads;
+//   6. the grid-wide pull: the delay >= 2 links of split pull connections,
+//      gathered one step ahead for slot n + 1 (ring rows of steps <= n - 1),
+//      32 targets per warp over every warp of the grid, one reduction per
+//      target.
 // Integer adds make every interleaving give the same sums. A step's slot is
 // complete when it is read: the previous step ended (launch boundary or grid
 // barrier) after every add into it.
@@ -31,7 +36,7 @@
 // networks ride in the kernel parameters (no dependent load before the state
 // loads), each neuron's outgoing row bounds are loaded with its state, the
 // Poisson inversion is a branch-free count over an inline table, and the far
-// items are taken two at a time.
+// items are taken several at a time.
 #pragma once
 #include <stdint.h>
 
