@@ -75,9 +75,12 @@ struct alignas(16) ConnDev {
     int32_t src_bit_mask, src_words, has_split, staged;  // staged (pull): link (and w) 16-byte aligned
     long long wfx;        // homogeneous weight, fixed point of the target
     float wscale;         // 2^shift of the target (exact)
-    int32_t item0;        // pull with split: its first item (32 targets each) of the grid-wide pull
+    int32_t item0;        // pull with split: its first item (PULL_ITEM links) of the grid-wide pull
     int32_t n_items;      // ... and its items (0: none)
     int32_t ring_off;     // pull: word offset of its source ring's copy in the ring cache (-1: not cached)
+    int32_t far0;         // pull with split: the first delay >= 2 link (split[0])
+    int32_t n_links;
+    const int32_t *item_row;  // pull with split: each item's first row
     const int32_t *ptr;
     const uint32_t *link;
     const float *w;
@@ -104,9 +107,10 @@ struct StepArgs {
     unsigned long long bar_limit_ns;  // persistent windows: a grid barrier wait gives up after this long
     int32_t trace_steps;
     int32_t pull_staged;   // the launch has a PullStage per warp in dynamic shared memory
+    int32_t pull_stage_bytes;  // ... of this size each (pull_stage_bytes)
     int32_t ring_cache_words;  // ... and after them a copy of a pull source's spike-bit ring of at most this size
     int32_t ring_cache_all;    // every pull source's ring fits the cache at its ring_off (the grid-wide pull)
-    int32_t pull_items;        // items of the grid-wide pull (the delay >= 2 rows, 32 targets each)
+    int32_t pull_items;        // items of the grid-wide pull (the delay >= 2 rows, PULL_ITEM links each)
     int32_t n_pull;
     int32_t item_cap;
     int32_t n_tiles;
@@ -322,33 +326,49 @@ __device__ __forceinline__ void red_add_u64(long long *p, long long v) {
 
 // ------------------------------------------------------------------ pull intake
 
-// The pull (the reference's pull intake, fused.py:1626-1965, with its link runs staged through shared memory):
-// a warp takes the incoming rows of 32 consecutive targets of one connection -- one contiguous range of the
-// pull CSR -- streamed into shared memory by 1-D bulk copies (cp.async.bulk, completion counted on an
-// mbarrier), PULL_CH links per chunk, PULL_BUFS chunks in flight, and gathers the staged links against the
-// source's spike-bit ring (copied to shared memory when small). Only this GPU's own memory is read, and no copy
-// is multicast. The range's 16-byte aligned interior is copied; its ragged head and tail (fewer than 4 links
-// each) are loaded directly, as is every link of a connection whose arrays are not 16-byte aligned. Each lane
-// sweeps its links (lane, lane + 32, ...) in increasing order, following the rows by their offsets (in shared
-// memory, the current row's end in a register), counts a row's links whose source spiked and adds the row's
-// sum into the row's shared slot when it leaves the row.
-// Two pulls use it: the delay-1 rows (every row without a split) by the target's own block in the step, and
-// the delay >= 2 rows of split connections one step ahead, by every warp of the grid (pull_far_phase).
-constexpr int PULL_CH = 256;                        // links per staging chunk
-constexpr int PULL_BUFS = 2;                        // chunks in flight per warp
+// The pull (the reference's pull intake, fused.py:1626-1965): a warp sweeps one contiguous run of links of a
+// pull CSR -- rows in target order -- in batches of 32 consecutive links, one per lane. Every lane follows its
+// link's row by the row offsets (the row's end in a register) and looks its source's bit up in the spike-bit
+// ring (copied to shared memory when small); the warp then sums the batch row by row without atomics: with a
+// single weight the rows' spiking links are counted from a ballot (popc over each row's lanes), with per-link
+// weights by a segmented shuffle scan. A row still open at the batch's end is carried in registers into the
+// next batch, so every row of the run is handed on exactly once, by one lane, with its total.
+// The run's links stream into shared memory by 1-D bulk copies (cp.async.bulk, completion counted on an
+// mbarrier): PULL_CH links per chunk, PULL_BUFS chunks in flight. Only this GPU's own memory is read, and no
+// copy is multicast. The run's 16-byte aligned interior is copied; its ragged head and tail (fewer than 4
+// links each) are loaded directly, as is every link of a connection whose arrays are not 16-byte aligned.
+// Two pulls use it: the delay-1 rows (every row without a split) by the target's own block in the step, for
+// the warp's 32 neurons, and the delay >= 2 rows of split connections one step ahead, by every warp of the
+// grid in runs of PULL_ITEM links (pull_far_phase).
+constexpr int PULL_CH = 512;                        // links per staging chunk
+constexpr int PULL_BUFS = 3;                        // chunks in flight per warp
+constexpr int PULL_ITEM = 2048;                     // links per item of the grid-wide pull (a multiple of PULL_CH)
 constexpr int RING_CACHE_MAX = 8192;                // words of pull sources' rings copied to shared memory, at most
 constexpr unsigned PULL_WAIT_POLLS = 1u << 22;      // polls of a chunk's mbarrier before it counts as lost
-constexpr int PULL_BATCH = 4;                       // links per lane whose spike-bit words are loaded together
+constexpr int PULL_BATCH = 4;                       // batches whose link records are loaded together
 
-struct alignas(16) PullStage {  // one per warp, in dynamic shared memory
-    uint32_t link[PULL_BUFS][PULL_CH];
-    float w[PULL_BUFS][PULL_CH];
+// One warp's staging area in dynamic shared memory: this header, then PULL_BUFS chunks of link records and,
+// when the launch has a pull connection with per-link weights, PULL_BUFS chunks of weights.
+struct alignas(16) PullStage {
     unsigned long long bar[PULL_BUFS];
-    long long sum[32];
-    int32_t ptr[33];
+    long long sum[32];          // the in-step pull: the warp's 32 rows' totals
+    int32_t ptr[33];            // ... and their offsets
     uint32_t uses[PULL_BUFS];   // completions of each buffer's mbarrier so far (its next parity)
-    int32_t broken;     // a chunk was lost: the rest of the launch loads links directly
+    int32_t broken;             // a chunk was lost: the rest of the launch loads links directly
 };
+constexpr size_t PULL_HEAD_BYTES = (sizeof(PullStage) + 15) & ~size_t(15);
+
+__host__ __device__ constexpr size_t pull_stage_bytes(bool weighted) {
+    return PULL_HEAD_BYTES + sizeof(uint32_t) * PULL_BUFS * PULL_CH * (weighted ? 2 : 1);
+}
+
+__device__ __forceinline__ uint32_t *stage_link(PullStage *st, int b) {
+    return reinterpret_cast<uint32_t *>(reinterpret_cast<char *>(st) + PULL_HEAD_BYTES) + b * PULL_CH;
+}
+
+__device__ __forceinline__ float *stage_w(PullStage *st, int b) {  // launches with weighted pull connections
+    return reinterpret_cast<float *>(stage_link(st, PULL_BUFS)) + b * PULL_CH;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -374,12 +394,12 @@ __device__ __forceinline__ void pull_issue(PullStage *st, const ConnDev &C, int 
     const uint32_t total = C.homogeneous ? bytes : 2u * bytes;
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(total) : "memory");
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(st->link[b])),
+                     smem_u32(stage_link(st, b))),
                  "l"(__cvta_generic_to_global(C.link + c0)), "r"(bytes), "r"(bar)
                  : "memory");
     if (!C.homogeneous)
         asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                         smem_u32(st->w[b])),
+                         smem_u32(stage_w(st, b))),
                      "l"(__cvta_generic_to_global(C.w + c0)), "r"(bytes), "r"(bar)
                      : "memory");
 }
@@ -401,133 +421,171 @@ __device__ __forceinline__ bool pull_wait(PullStage *st, int b) {
     return false;
 }
 
-// One warp's sweep state and constants. HOMOG: one weight for every link (rows counted, the sum made at the
-// row's end); RING: the source's ring is the shared-memory copy.
+// One warp's sweep over a run of links of a pull CSR whose rows' offsets are `rows` (rows below qmax).
+// HOMOG: one weight for every link; RING: the source's ring is the shared-memory copy.
+// The open row (the row of the last link swept) is the same in every lane: a batch wholly inside it only adds
+// each lane's spiking links (or their weights) to the lane's own part, with no exchange between lanes; a batch
+// that reaches past it folds the parts into the row's total (one warp reduction) and sums the batch row by row.
 template <bool HOMOG, bool RING>
-struct PullSweep {
+struct PullPass {
     const uint32_t *ring;  // the source's spike-bit ring (shared-memory copy or global)
-    PullStage *st;
-    int nlo, mask, words, src_n, min_d;
+    const int32_t *rows;   // row offsets (global, or the warp's copy in shared memory)
+    int nlo, mask, words, src_n, min_d, qmax;
     long long wfx;
     float wscale;
-    int q, end;       // the lane's current row (warp-relative) and its end
-    long long part;   // per-link weights: the row's partial sum
-    int cnt;          // single weight: the row's spiking links
+    int cq, cend;     // the open row and its end
+    long long csum;   // its total, but for the lanes' parts since the last fold:
+    long long lpart;  // per-link weights: the lane's part
+    int lcnt;         // single weight: the lane's spiking links
     unsigned hits;    // links whose source spiked (the synaptic events of the pull)
     int bad;          // links out of range
 
-    __device__ __forceinline__ uint32_t bits(uint32_t rec, bool &ok) const {
+    __device__ __forceinline__ uint32_t bits(uint32_t rec, bool valid, bool &ok) const {
         const int d = (int)(rec >> 24), s = (int)(rec & 0xFFFFFFu);
-        ok = d >= min_d && d <= mask && s < src_n;
+        ok = valid && d >= min_d && d <= mask && s < src_n;
         const int at = ((nlo - d) & mask) * words + (s >> 5);
         return ok ? (RING ? ring[at] : __ldcg(ring + at)) : 0u;
     }
 
-    __device__ __forceinline__ void flush() {
+    __device__ __forceinline__ void fold() {
         if (HOMOG) {
-            if (cnt) atomicAdd(reinterpret_cast<unsigned long long *>(&st->sum[q]), (unsigned long long)(cnt * wfx));
-            cnt = 0;
+            csum += (long long)__reduce_add_sync(FULL, (unsigned)lcnt) * wfx;
+            lcnt = 0;
         } else {
-            if (part) atomicAdd(reinterpret_cast<unsigned long long *>(&st->sum[q]), (unsigned long long)part);
-            part = 0;
+            long long x = lpart;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(FULL, x, off);
+            csum += x;
+            lpart = 0;
         }
     }
 
-    __device__ __forceinline__ void apply(int l, uint32_t rec, uint32_t word, bool ok, float w) {
-        while (l >= end) {  // left the row (rows may be empty)
-            flush();
-            ++q;
-            end = st->ptr[q + 1];
-        }
-        if (!ok) {
-            ++bad;
+    // One batch (every lane of the warp): links [b, min(b + 32, r1)), the lane's link b + lane (`valid` below
+    // r1) with its record, ring word and weight. emit(row, total) is called once per finished row, by one lane.
+    template <class Emit>
+    __device__ __forceinline__ void batch(int b, int r1, bool valid, uint32_t rec, uint32_t word, bool ok, float w,
+                                          Emit &emit) {
+        const int lane = threadIdx.x & 31;
+        bad += (int)(valid && !ok);
+        const unsigned hit = ok ? (word >> (rec & 31u)) & 1u : 0u;  // rec & 31 = s & 31
+        hits += hit;
+        if (min(b + 32, r1) <= cend) {  // the whole batch in the open row
+            if (HOMOG) lcnt += (int)hit;
+            else if (hit) lpart += weight_fx(w, wscale);
             return;
         }
-        const unsigned hit = (word >> (rec & 31u)) & 1u;  // rec & 31 = s & 31 (the index is the low 24 bits)
-        hits += hit;
-        if (HOMOG) cnt += (int)hit;
-        else if (hit) part += weight_fx(w, wscale);
+        fold();
+        int q = cq, end = cend;
+        const int l = min(b + lane, r1 - 1);  // lanes past the batch's last link: that link
+        while (l >= end && q + 1 < qmax) {    // rows may be empty
+            ++q;
+            end = rows[q + 1];
+        }
+        const int qn = __shfl_down_sync(FULL, q, 1);
+        const unsigned ends = __ballot_sync(FULL, lane == 31 || qn != q);  // the last lane of every row
+        if (cq != __shfl_sync(FULL, q, 0)) {  // the open row ended with the previous batch
+            if (lane == 0) emit(cq, csum);
+            csum = 0;
+        }
+        const unsigned below = ends & ((1u << lane) - 1u);
+        const int start = below ? 32 - __clz(below) : 0;  // the first lane of the lane's row
+        long long seg;
+        if (HOMOG) {
+            const unsigned m = ((2u << lane) - 1u) & ~((1u << start) - 1u);
+            seg = (long long)__popc(__ballot_sync(FULL, hit != 0u) & m) * wfx;
+        } else {
+            seg = hit ? weight_fx(w, wscale) : 0;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {  // segmented inclusive scan
+                const long long y = __shfl_up_sync(FULL, seg, off);
+                if (lane - off >= start) seg += y;
+            }
+        }
+        if (start == 0) seg += csum;  // the batch's first row continues the open row (csum is 0 otherwise)
+        if (((ends >> lane) & 1u) && lane != 31) emit(q, seg);
+        csum = __shfl_sync(FULL, seg, 31);
+        cq = __shfl_sync(FULL, q, 31);
+        cend = __shfl_sync(FULL, end, 31);
+    }
+
+    // The links [r0, r1) of the pass, their records at lk[l - base] (and weights at wk[l - base]): shared-memory
+    // chunks (SMEM) or the connection's arrays (base 0), PULL_BATCH batches loaded together.
+    template <bool SMEM, class Emit>
+    __device__ __forceinline__ void run(const uint32_t *lk, const float *wk, int base, int r0, int r1, Emit &emit) {
+        const int lane = threadIdx.x & 31;
+        for (int b0 = r0; b0 < r1; b0 += 32 * PULL_BATCH) {
+            uint32_t rec[PULL_BATCH], word[PULL_BATCH];
+            float w[PULL_BATCH];
+            bool ok[PULL_BATCH];
+#pragma unroll
+            for (int k = 0; k < PULL_BATCH; ++k) {
+                const int l = b0 + 32 * k + lane;
+                rec[k] = 0u;
+                w[k] = 0.f;
+                if (l < r1) {
+                    rec[k] = SMEM ? lk[l - base] : __ldg(lk + (l - base));
+                    if (!HOMOG) w[k] = SMEM ? wk[l - base] : __ldg(wk + (l - base));
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < PULL_BATCH; ++k) word[k] = bits(rec[k], b0 + 32 * k + lane < r1, ok[k]);
+#pragma unroll
+            for (int k = 0; k < PULL_BATCH; ++k)
+                if (b0 + 32 * k < r1)
+                    batch(b0 + 32 * k, r1, b0 + 32 * k + lane < r1, rec[k], word[k], ok[k], w[k], emit);
+        }
     }
 };
 
-// The rows [t0, t0 + nq) of `rows` (ptr, or split's delay >= 2 rows) of connection C against the ring rows of
-// steps n_read - d; returns the lane's own row sum (lanes < nq).
-template <bool HOMOG, bool RING>
-__device__ __forceinline__ long long pull_rows(const ConnDev &C, const uint32_t *ring, PullStage *st, int32_t *err,
-                                               unsigned long long *events, const int32_t *rows, int t0, int nq,
-                                               long long n_read, int min_d) {
+// The pass over links [L0, L1) (L0 < L1) of connection C, the first in row q0 of `rows` or a later one (rows
+// before it empty), rows below qmax, against the ring rows of steps n_read - d (d >= min_d); each row the pass
+// reaches goes to emit(row, total) once.
+template <bool HOMOG, bool RING, class Emit>
+__device__ __forceinline__ void pull_pass(const ConnDev &C, const uint32_t *ring, PullStage *st, int32_t *err,
+                                          unsigned long long *events, const int32_t *rows, int q0, int qmax, int L0,
+                                          int L1, long long n_read, int min_d, Emit &emit) {
     const int lane = threadIdx.x & 31;
-    if (lane <= nq) st->ptr[lane] = __ldg(rows + t0 + lane);
-    if (lane == 0 && nq == 32) st->ptr[32] = __ldg(rows + t0 + 32);
-    st->sum[lane] = 0;
-    __syncwarp();
-    PullSweep<HOMOG, RING> sw;
-    sw.ring = ring;
-    sw.st = st;
-    sw.nlo = (int)n_read;  // the ring rows' index mod the depth: only the low bits matter
-    sw.mask = C.src_bit_mask;
-    sw.words = C.src_words;
-    sw.src_n = C.src_n;
-    sw.min_d = min_d;
-    sw.wfx = C.wfx;
-    sw.wscale = C.wscale;
-    sw.q = 0;
-    sw.end = st->ptr[1];
-    sw.part = 0;
-    sw.cnt = 0;
-    sw.hits = 0;
-    sw.bad = 0;
-    const int L0 = st->ptr[0], L1 = st->ptr[nq];
-    const bool staged = C.staged && !st->broken;
+    PullPass<HOMOG, RING> p;
+    p.ring = ring;
+    p.rows = rows;
+    p.nlo = (int)n_read;  // the ring rows' index mod the depth: only the low bits matter
+    p.mask = C.src_bit_mask;
+    p.words = C.src_words;
+    p.src_n = C.src_n;
+    p.min_d = min_d;
+    p.qmax = qmax;
+    p.wfx = C.wfx;
+    p.wscale = C.wscale;
+    int q = q0, end = rows[q0 + 1];
+    while (L0 >= end && q + 1 < qmax) {  // the row of link L0 (the same in every lane)
+        ++q;
+        end = rows[q + 1];
+    }
+    p.cq = q;
+    p.cend = end;
+    p.csum = 0;
+    p.lpart = 0;
+    p.lcnt = 0;
+    p.hits = 0;
+    p.bad = 0;
+    const bool staged = C.staged && !__shfl_sync(FULL, st->broken, 0);  // lane 0 sets it: its value for all
     int a0 = (L0 + 3) & ~3, a1 = L1 & ~3;
     if (!staged || a1 <= a0) a0 = a1 = L1;  // nothing to stage: every link loaded directly
     const int n_chunks = (a1 - a0 + PULL_CH - 1) / PULL_CH;
     if (lane == 0)
         for (int k = 0; k < PULL_BUFS && k < n_chunks; ++k) pull_issue(st, C, a0, a1, k);
-    // the head (or every link): direct loads, PULL_BATCH per lane in flight
-    for (int base = L0 + lane; base < a0; base += 32 * PULL_BATCH) {
-        uint32_t rec[PULL_BATCH], word[PULL_BATCH];
-        float w[PULL_BATCH];
-        bool ok[PULL_BATCH];
-#pragma unroll
-        for (int k = 0; k < PULL_BATCH; ++k) {
-            const int l = base + 32 * k;
-            rec[k] = l < a0 ? __ldg(C.link + l) : 0u;
-            w[k] = (!HOMOG && l < a0) ? __ldg(C.w + l) : 0.f;
-        }
-#pragma unroll
-        for (int k = 0; k < PULL_BATCH; ++k) word[k] = sw.bits(rec[k], ok[k]);
-#pragma unroll
-        for (int k = 0; k < PULL_BATCH; ++k)
-            if (base + 32 * k < a0) sw.apply(base + 32 * k, rec[k], word[k], ok[k], w[k]);
-    }
+    p.template run<false>(C.link, C.w, 0, L0, a0, emit);  // the head (or every link)
     bool lost = false;
     for (int k = 0; k < n_chunks; ++k) {
         const int b = k % PULL_BUFS;
         const int c0 = a0 + k * PULL_CH, c1 = min(a1, c0 + PULL_CH);
-        if (!lost && !pull_wait(st, b)) lost = true;
+        if (!lost) lost = __any_sync(FULL, !pull_wait(st, b));  // the same in every lane
         __syncwarp();
         if (lane == 0) st->uses[b] += 1;
-        for (int base = c0 + lane; base < c1; base += 32 * PULL_BATCH) {
-            uint32_t rec[PULL_BATCH], word[PULL_BATCH];
-            float w[PULL_BATCH];
-            bool ok[PULL_BATCH];
-#pragma unroll
-            for (int q = 0; q < PULL_BATCH; ++q) {
-                const int l = base + 32 * q;
-                rec[q] = 0u;
-                w[q] = 0.f;
-                if (l < c1) {  // a lost chunk (did not land in time): its links loaded directly
-                    rec[q] = lost ? __ldg(C.link + l) : st->link[b][l - c0];
-                    if (!HOMOG) w[q] = lost ? __ldg(C.w + l) : st->w[b][l - c0];
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < PULL_BATCH; ++q) word[q] = sw.bits(rec[q], ok[q]);
-#pragma unroll
-            for (int q = 0; q < PULL_BATCH; ++q)
-                if (base + 32 * q < c1) sw.apply(base + 32 * q, rec[q], word[q], ok[q], w[q]);
-        }
+        if (lost)  // a chunk that did not land in time: its links loaded directly
+            p.template run<false>(C.link, C.w, 0, c0, c1, emit);
+        else
+            p.template run<true>(stage_link(st, b), HOMOG ? nullptr : stage_w(st, b), c0, c0, c1, emit);
         __syncwarp();  // every lane done with buffer b before it is refilled
         if (!lost && lane == 0 && k + PULL_BUFS < n_chunks) pull_issue(st, C, a0, a1, k + PULL_BUFS);
     }
@@ -535,50 +593,58 @@ __device__ __forceinline__ long long pull_rows(const ConnDev &C, const uint32_t 
         atomicAdd(err + 5, 1);
         st->broken = 1;
     }
-    for (int base = max(a1, L0) + lane; base < L1; base += 32) {  // the tail (fewer than 4 links)
-        const uint32_t rec = __ldg(C.link + base);
-        bool ok;
-        const uint32_t word = sw.bits(rec, ok);
-        sw.apply(base, rec, word, ok, HOMOG ? 0.f : __ldg(C.w + base));
-    }
-    sw.flush();
-    const unsigned hits = __reduce_add_sync(FULL, sw.hits);
-    const int bad = __reduce_add_sync(FULL, sw.bad);
+    p.template run<false>(C.link, C.w, 0, max(a1, L0), L1, emit);  // the tail (fewer than 4 links)
+    p.fold();
+    if (lane == 0) emit(p.cq, p.csum);
+    const unsigned hits = __reduce_add_sync(FULL, p.hits);
+    const int bad = __reduce_add_sync(FULL, p.bad);
     if (lane == 0) {
         if (hits) atomicAdd(events, (unsigned long long)hits);
         if (bad) atomicAdd(err + 1, bad);
     }
-    __syncwarp();
-    const long long mine = lane < nq ? st->sum[lane] : 0;
-    __syncwarp();
-    return mine;
 }
 
-template <bool RING>
-__device__ __forceinline__ long long pull_rows_any(const ConnDev &C, const uint32_t *ring, PullStage *st,
-                                                   int32_t *err, unsigned long long *events, const int32_t *rows,
-                                                   int t0, int nq, long long n_read, int min_d) {
-    return C.homogeneous ? pull_rows<true, RING>(C, ring, st, err, events, rows, t0, nq, n_read, min_d)
-                         : pull_rows<false, RING>(C, ring, st, err, events, rows, t0, nq, n_read, min_d);
+template <bool RING, class Emit>
+__device__ __forceinline__ void pull_pass_any(const ConnDev &C, const uint32_t *ring, PullStage *st, int32_t *err,
+                                              unsigned long long *events, const int32_t *rows, int q0, int qmax,
+                                              int L0, int L1, long long n_read, int min_d, Emit &emit) {
+    if (C.homogeneous)
+        pull_pass<true, RING>(C, ring, st, err, events, rows, q0, qmax, L0, L1, n_read, min_d, emit);
+    else
+        pull_pass<false, RING>(C, ring, st, err, events, rows, q0, qmax, L0, L1, n_read, min_d, emit);
 }
 
 // The launch's ring cache, after the warps' PullStages in dynamic shared memory.
-__device__ __forceinline__ uint32_t *ring_cache() {
+__device__ __forceinline__ uint32_t *ring_cache(const StepArgs &a) {
     extern __shared__ __align__(128) unsigned char n2b_dyn_smem[];
-    return reinterpret_cast<uint32_t *>(reinterpret_cast<PullStage *>(n2b_dyn_smem) + (blockDim.x >> 5));
+    return reinterpret_cast<uint32_t *>(n2b_dyn_smem + (size_t)a.pull_stage_bytes * (blockDim.x >> 5));
 }
 
-__device__ __forceinline__ void copy_ring(uint32_t *dst, const ConnDev &C) {
-    const int words = (C.src_bit_mask + 1) * C.src_words;
-    for (int k = threadIdx.x; k < words; k += blockDim.x) dst[k] = __ldcg(C.src_bits + k);
+// Words [first, first + count) of C's source ring into dst (at the same offsets), every thread of the block;
+// 16-byte loads where both sides allow them, several in flight per thread.
+__device__ __forceinline__ void copy_ring(uint32_t *dst, const ConnDev &C, int first, int count) {
+    const uint32_t *s = C.src_bits + first;
+    uint32_t *d = dst + first;
+    if ((((uintptr_t)s | (uintptr_t)d) & 15u) == 0 && (count & 3) == 0) {
+        const uint4 *s4 = reinterpret_cast<const uint4 *>(s);
+        uint4 *d4 = reinterpret_cast<uint4 *>(d);
+#pragma unroll 4
+        for (int k = threadIdx.x; k < (count >> 2); k += blockDim.x) d4[k] = __ldcg(s4 + k);
+    } else {
+#pragma unroll 4
+        for (int k = threadIdx.x; k < count; k += blockDim.x) d[k] = __ldcg(s + k);
+    }
 }
 
 // The in-step pull of the tile's population (every thread of the block): each pull connection's rows of ptr --
-// all its links, or, with a split, its delay-1 links -- for the warp's 32 neurons, against ring rows n - d. A
-// source whose whole ring fits the ring cache is copied there first (its rows of steps before n are final).
+// all its links, or, with a split, its delay-1 links -- for the warp's 32 neurons, against ring rows n - d;
+// returns the lane's own neuron's total. A source whose whole ring fits the ring cache is copied there first:
+// with a split only ring row n - 1 (the delay-1 links' row), else the whole ring (its rows of steps before n are
+// final). The warp's row offsets are copied to its PullStage.
 template <bool INL>
 __device__ __forceinline__ long long pull_intake(const StepArgs &a, const PopDev &P, int first, int count,
                                                  long long n, PullStage *stage) {
+    const int lane = threadIdx.x & 31;
     const int wbase = first + (threadIdx.x & ~31);
     const int nq = min(32, first + count - wbase);
     long long mine = 0;
@@ -586,38 +652,57 @@ __device__ __forceinline__ long long pull_intake(const StepArgs &a, const PopDev
         const ConnDev &C = pull_at<INL>(a, c);
         const int ring_words = (C.src_bit_mask + 1) * C.src_words;
         const bool cached = ring_words <= a.ring_cache_words;  // the same for every thread of the block
-        uint32_t *cache = ring_cache();
+        uint32_t *cache = ring_cache(a);
         if (cached) {
             __syncthreads();  // every warp done with the cache's previous ring
-            copy_ring(cache, C);
+            if (C.has_split)
+                copy_ring(cache, C, (int)((n - 1) & C.src_bit_mask) * C.src_words, C.src_words);
+            else
+                copy_ring(cache, C, 0, ring_words);
             __syncthreads();
         }
         if (nq <= 0) continue;
         // (a network with pull connections always has its PullStages: the launch's dynamic shared memory)
-        mine += cached ? pull_rows_any<true>(C, cache, stage, a.err, a.counters, C.ptr, wbase, nq, n, 1)
-                       : pull_rows_any<false>(C, C.src_bits, stage, a.err, a.counters, C.ptr, wbase, nq, n, 1);
+        if (lane <= nq) stage->ptr[lane] = __ldg(C.ptr + wbase + lane);
+        if (lane == 0 && nq == 32) stage->ptr[32] = __ldg(C.ptr + wbase + 32);
+        stage->sum[lane] = 0;
+        __syncwarp();
+        const int L0 = stage->ptr[0], L1 = stage->ptr[nq];
+        if (L1 > L0) {  // the same for every lane
+            auto emit = [&](int q, long long v) { stage->sum[q] = v; };  // q: the warp's row, below nq
+            if (cached)
+                pull_pass_any<true>(C, cache, stage, a.err, a.counters, stage->ptr, 0, nq, L0, L1, n, 1, emit);
+            else
+                pull_pass_any<false>(C, C.src_bits, stage, a.err, a.counters, stage->ptr, 0, nq, L0, L1, n, 1,
+                                     emit);
+        }
+        __syncwarp();
+        mine += stage->sum[lane];
+        __syncwarp();
     }
-    return mine;
+    return lane < nq ? mine : 0;
 }
 
 // The grid-wide pull (every thread of every block, after the step's far items): the delay >= 2 rows of every
 // split pull connection, for the arrival slot of step n + 1 -- ring rows (n + 1) - d, d >= 2, all written
-// before this step -- 32 targets per warp, warps taking items grid-stride, each target's sum added to its slot
-// with one reduction (slot n + 1 is read after the step's barrier). With every pull source's ring in the cache
-// together, the block copies them all first.
+// before this step -- in items of PULL_ITEM links (item k of a connection: its links [PULL_ITEM (k0 + k),
+// PULL_ITEM (k0 + k + 1)) within the delay >= 2 region, k0 = far0 / PULL_ITEM; its first row in item_row[k]),
+// warps taking items grid-stride. Each row an item finishes is added to its slot with one reduction (slot n + 1
+// is read after the step's barrier). With every pull source's ring in the cache together, the block copies them
+// all first.
 template <int NPB, bool INL>
 __device__ __forceinline__ void pull_far_phase(const StepArgs &a, const long long n, PullStage *stage) {
     if (a.pull_items == 0 || stage == nullptr) return;  // the same for every thread of the launch
-    uint32_t *cache = ring_cache();
+    uint32_t *cache = ring_cache(a);
     if (a.ring_cache_all) {
         __syncthreads();
         for (int c = 0; c < a.n_pull; ++c) {
             const ConnDev &C = pull_at<INL>(a, c);
-            if (C.n_items > 0 && C.ring_off >= 0) copy_ring(cache + C.ring_off, C);
+            if (C.n_items > 0 && C.ring_off >= 0)
+                copy_ring(cache + C.ring_off, C, 0, (C.src_bit_mask + 1) * C.src_words);
         }
         __syncthreads();
     }
-    const int lane = threadIdx.x & 31;
     const int W = (int)gridDim.x * (NPB / 32);
     int c = 0;
     for (int it = (int)blockIdx.x * (NPB / 32) + (int)(threadIdx.x >> 5); it < a.pull_items; it += W) {
@@ -625,13 +710,37 @@ __device__ __forceinline__ void pull_far_phase(const StepArgs &a, const long lon
                                      it < pull_at<INL>(a, c).item0 + pull_at<INL>(a, c).n_items))
             ++c;  // items rise with the connection index: the search moves forward only
         const ConnDev &C = pull_at<INL>(a, c);
-        const int t0 = (it - C.item0) * 32, nq = min(32, C.tgt_n - t0);
-        const bool cached = a.ring_cache_all && C.ring_off >= 0;
-        const long long sum =
-            cached ? pull_rows_any<true>(C, cache + C.ring_off, stage, a.err, a.counters, C.split, t0, nq, n + 1, 2)
-                   : pull_rows_any<false>(C, C.src_bits, stage, a.err, a.counters, C.split, t0, nq, n + 1, 2);
-        if (lane < nq && sum) red_add_u64(C.tgt_acc + (size_t)((n + 1) & C.tgt_acc_mask) * (size_t)C.tgt_n + t0 + lane, sum);
+        const int k = it - C.item0, k0 = C.far0 / PULL_ITEM;
+        const int L0 = max(C.far0, (k0 + k) * PULL_ITEM), L1 = min(C.n_links, (k0 + k + 1) * PULL_ITEM);
+        if (L1 <= L0) continue;
+        long long *slot = C.tgt_acc + (size_t)((n + 1) & C.tgt_acc_mask) * (size_t)C.tgt_n;
+        auto emit = [&](int q, long long v) {
+            if (v) red_add_u64(slot + q, v);
+        };
+        const int q0 = __ldg(C.item_row + k);
+        if (a.ring_cache_all && C.ring_off >= 0)
+            pull_pass_any<true>(C, cache + C.ring_off, stage, a.err, a.counters, C.split, q0, C.tgt_n, L0, L1, n + 1,
+                                2, emit);
+        else
+            pull_pass_any<false>(C, C.src_bits, stage, a.err, a.counters, C.split, q0, C.tgt_n, L0, L1, n + 1, 2,
+                                 emit);
     }
+}
+
+// Set-up: the first row of every item of a split pull connection's grid-wide pull -- the row r holding link
+// PULL_ITEM (k0 + k) (or far0, for item 0), the last r with split[r] <= that link.
+__global__ void pull_item_rows_kernel(const int32_t *split, int32_t tgt_n, int32_t far0, int32_t n_items,
+                                      int32_t *item_row) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_items) return;
+    const int l = max(far0, (far0 / PULL_ITEM + k) * PULL_ITEM);
+    int lo = 0, hi = tgt_n;  // split[lo] <= l (split[0] = far0); answer in [lo, hi)
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (split[mid] <= l) lo = mid;
+        else hi = mid;
+    }
+    item_row[k] = lo;
 }
 
 // ------------------------------------------------------------------ delivery
@@ -1127,7 +1236,7 @@ __device__ __forceinline__ void step_body(const StepArgs &a, const long long n, 
 __device__ __forceinline__ PullStage *warp_stage(const StepArgs &a) {
     extern __shared__ __align__(128) unsigned char n2b_dyn_smem[];
     if (!a.pull_staged) return nullptr;
-    PullStage *st = reinterpret_cast<PullStage *>(n2b_dyn_smem) + (threadIdx.x >> 5);
+    PullStage *st = reinterpret_cast<PullStage *>(n2b_dyn_smem + (size_t)a.pull_stage_bytes * (threadIdx.x >> 5));
     pull_stage_init(st);
     return st;
 }

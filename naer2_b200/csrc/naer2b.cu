@@ -62,7 +62,7 @@ namespace {
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 struct Layout {
-    size_t pops, push, pull, tiles, step, rec0, err, counters, items, item_count, barrier, total;
+    size_t pops, push, pull, tiles, step, rec0, err, counters, items, item_count, barrier, pull_rows, total;
     int32_t n_push, n_pull, n_tiles, item_cap;
 };
 
@@ -82,6 +82,9 @@ Layout layout(const n2b_population *pops, int32_t n_pops, const n2b_connection *
             cap += (int64_t)conns[c].n_links / block + pops[conns[c].src].n + 1;
     }
     L.item_cap = (int32_t)std::min<int64_t>(cap, (int64_t)1 << 30);
+    int64_t item_rows = 0;  // the grid-wide pull's items' first rows: PULL_ITEM links each, at most
+    for (int32_t c = 0; c < n_conns; ++c)
+        if (conns[c].mode == N2B_PULL && conns[c].split) item_rows += conns[c].n_links / n2b::PULL_ITEM + 2;
     for (int32_t p = 0; p < n_pops; ++p) L.n_tiles += (pops[p].n + block - 1) / block;
     size_t o = 0;
     L.pops = o; o = align256(o + sizeof(n2b::PopDev) * std::max(n_pops, 1));
@@ -95,6 +98,7 @@ Layout layout(const n2b_population *pops, int32_t n_pops, const n2b_connection *
     L.item_count = o; o = align256(o + sizeof(int32_t) * 9);  // list lengths, tile and far-chunk counters
     L.items = o; o = align256(o + sizeof(int4) * 3 * (size_t)L.item_cap);
     L.barrier = o; o = align256(o + sizeof(unsigned) * n2b::BAR_WORDS);
+    L.pull_rows = o; o = align256(o + sizeof(int32_t) * (size_t)std::max<int64_t>(item_rows, 1));
     L.total = o;
     return L;
 }
@@ -329,6 +333,7 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
         D.has_split = C.split != nullptr;
         D.split = C.split;
         D.ring_off = -1;
+        D.n_links = C.n_links;
         // pull rows stream through shared memory by bulk copies, which need 16-byte aligned sources
         D.staged = C.mode == N2B_PULL && (reinterpret_cast<uintptr_t>(C.link) & 15) == 0 &&
                    (C.w == nullptr || (reinterpret_cast<uintptr_t>(C.w) & 15) == 0);
@@ -348,15 +353,32 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     // them a ring cache -- for the largest pull source's spike-bit ring (the in-step pull, one connection at a
     // time) and, when they fit together, every split connection's source ring at its ring_off (the grid-wide
     // pull), up to RING_CACHE_MAX words; the grid-wide pull's items, 32 targets each, numbered by connection
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    char *ws = static_cast<char *>(workspace);
+    // a split pull connection's first delay >= 2 link (read back once) and its items of PULL_ITEM links
+    std::vector<int32_t> far0(pull.size(), 0);
+    for (size_t c = 0; c < pull.size(); ++c)
+        if (pull[c].has_split && pull[c].tgt_n > 0)
+            N2B_CUDA(cudaMemcpyAsync(&far0[c], pull[c].split, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    N2B_CUDA(cudaStreamSynchronize(s));
     int32_t max_ring = 0, total_ring = 0, pull_items = 0;
-    for (n2b::ConnDev &C : pull) {
+    size_t item_rows = 0;
+    for (size_t c = 0; c < pull.size(); ++c) {
+        n2b::ConnDev &C = pull[c];
         const int32_t w = (C.src_bit_mask + 1) * C.src_words;
         max_ring = std::max(max_ring, w);
         if (C.has_split) {
+            if (far0[c] < 0 || far0[c] > C.n_links)
+                return fail(N2B_EINVAL, "a pull connection's split offsets lie outside its links");
             C.ring_off = total_ring;
             total_ring += w;
+            C.far0 = far0[c];
             C.item0 = pull_items;
-            C.n_items = (C.tgt_n + 31) / 32;
+            C.n_items = (C.tgt_n > 0 && far0[c] < C.n_links)
+                            ? (C.n_links + n2b::PULL_ITEM - 1) / n2b::PULL_ITEM - far0[c] / n2b::PULL_ITEM
+                            : 0;
+            C.item_row = reinterpret_cast<const int32_t *>(ws + L.pull_rows) + item_rows;
+            item_rows += (size_t)C.n_items;
             pull_items += C.n_items;
         }
     }
@@ -372,8 +394,6 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     for (int32_t p : order)
         for (int32_t f = 0; f < pops[p].n; f += block) tiles.push_back(make_int4(p, f, std::min(block, pops[p].n - f), 0));
 
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    char *ws = static_cast<char *>(workspace);
     // the first entries of every Poisson table, inline (read back once)
     for (int32_t p = 0; p < n_pops; ++p) {
         const int32_t k = std::min(pops[p].ext_len, n2b::EXT_INLINE);
@@ -388,6 +408,10 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
         N2B_CUDA(cudaMemcpyAsync(ws + L.pull, pull.data(), sizeof(n2b::ConnDev) * pull.size(), cudaMemcpyHostToDevice, s));
     if (!tiles.empty())
         N2B_CUDA(cudaMemcpyAsync(ws + L.tiles, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, s));
+    for (const n2b::ConnDev &C : pull)
+        if (C.n_items > 0)
+            n2b::pull_item_rows_kernel<<<(C.n_items + 127) / 128, 128, 0, s>>>(
+                C.split, C.tgt_n, C.far0, C.n_items, const_cast<int32_t *>(C.item_row));
     n2b::set_step_kernel<<<1, 1, 0, s>>>(reinterpret_cast<long long *>(ws + L.step), 0,
                                          reinterpret_cast<int32_t *>(ws + L.item_count));
     n2b::set_kernel<<<1, 1, 0, s>>>(reinterpret_cast<long long *>(ws + L.rec0), 0);
@@ -409,7 +433,10 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     int want = (opt && opt->grid > 0) ? opt->grid
                                       : (persistent ? std::max(sms, L.n_tiles + sms / 2) : 2 * sms);
     int grid = std::max(L.n_tiles, want);
-    const size_t dyn = pull.empty() ? 0 : sizeof(n2b::PullStage) * (size_t)(block / 32) + sizeof(uint32_t) * cache_words;
+    bool weighted_pull = false;
+    for (const n2b::ConnDev &C : pull) weighted_pull = weighted_pull || !C.homogeneous;
+    const size_t stage_bytes = n2b::pull_stage_bytes(weighted_pull);
+    const size_t dyn = pull.empty() ? 0 : stage_bytes * (size_t)(block / 32) + sizeof(uint32_t) * cache_words;
     int most = 0;
     int rc2 = coresident_blocks(block, inl, false, device, dyn, &most);  // also raises the kernels' dynamic limit
     if (rc2) return rc2;
@@ -458,6 +485,7 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     a.bar_limit_ns = (opt && opt->barrier_limit_ns > 0) ? (unsigned long long)opt->barrier_limit_ns
                                                          : n2b::BAR_LIMIT_NS;
     a.pull_staged = dyn > 0;
+    a.pull_stage_bytes = (int32_t)stage_bytes;
     a.ring_cache_words = ring_words;
     a.ring_cache_all = ring_all;
     a.pull_items = pull_items;

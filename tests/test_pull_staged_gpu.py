@@ -43,6 +43,39 @@ def test_ragged_rows_with_weights_all_pull_match_oracle(cuda, persistent):
     assert net.runtime.status()[_lib.ERR_PULL_STAGE] == 0
 
 
+def sparse_rows_net(seed):
+    """2,000 LIF targets pulling from two Poisson populations by fixed out-degree, delays uniform in 1-20 steps:
+    300 sources x 2 links (single weight; in-degree ~0.3: most rows empty, the rest a link or two) and 3,000
+    sources x 40 links with per-link weights (in-degree ~60: 59 items of the grid-wide pull, rows shorter than a
+    batch and rows crossing batches, chunks and items)."""
+    from naer2_b200 import philox
+    from naer2_b200.models import LIF, Poisson_source
+    from naer2_b200.patterns import fixed_outdegree
+
+    rng = np.random.Generator(np.random.Philox(key=seed))
+    a = Poisson_source(rate=0.5) * 300
+    b = Poisson_source(rate=0.2) * 3000
+    t = LIF(tau=20.0, theta=20.0, V_r=10.0, t_ref=2.0) * 2000
+    a.seed, b.seed, t.seed = (seed << 8) | 1, (seed << 8) | 2, (seed << 8) | 3
+    t.V = torch.from_numpy((philox.uniform(seed, 2000, stream=1) * 20.0).astype(np.float32))
+    for k, (src, deg, w) in enumerate(((a, 2, 6.0), (b, 40, None))):
+        c = src >> fixed_outdegree(k=deg, seed=(seed << 8) | (16 + k)) >> t
+        c.weight = w if w is not None else torch.from_numpy(rng.uniform(0.05, 0.15, c.shape[0]).astype(np.float32))
+        c.delay = torch.from_numpy((rng.integers(1, 21, c.shape[0]) * 0.1).astype(np.float32))
+    net = t.network
+    net.resolution = 0.1
+    return net
+
+
+@pytest.mark.parametrize("persistent", [True, False], ids=["persistent", "per-step"])
+def test_short_and_empty_rows_all_pull_match_oracle(cuda, persistent):
+    net = sparse_rows_net(seed=31)
+    gr, orr, gs, os_, cnt, ev = run_both(net, 400, chunk=150, modes=all_pull(net), persistent=persistent)
+    assert sum(r.sum() for r in gr[2:]) > 500  # the targets fire
+    assert_identical(gr, orr, gs, os_)
+    assert net.runtime.status()[_lib.ERR_PULL_STAGE] == 0
+
+
 def test_unaligned_rows_walk_and_match_the_staged_path(cuda):
     """The same pull network twice through the C ABI: once as built (16-byte aligned rows: staged), once with
     every pull connection's link and weight arrays moved to an address 4 bytes past a 16-byte boundary (not
