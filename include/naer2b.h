@@ -124,7 +124,8 @@ typedef struct n2b_options {
     int32_t device;  /* CUDA device ordinal of every pointer */
     int32_t grid;    /* blocks per launch (0: per-step launches two per SM and at least one per tile;
                         persistent one per SM, at least tiles + half an SM's worth, at most the co-resident
-                        blocks, each looping over its tiles) */
+                        blocks, each looping over its tiles; persistent with a split pull connection: every
+                        co-resident block, which all share its delay >= 2 rows) */
     int32_t persistent; /* 1: a window of steps is one cooperative launch, steps separated by a grid
                            barrier; 0: one launch per step */
     int32_t reserved;

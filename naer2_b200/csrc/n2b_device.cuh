@@ -102,6 +102,7 @@ struct StepArgs {
     int4 *items;           // 3 work lists of item_cap entries: (push connection, first link, end link, 0)
     int32_t *item_count;   // their lengths; step n appends to list n mod 3, reads n - 1's
     int32_t *tile_claim;   // per step n mod 3: tiles past the first gridDim.x claimed so far
+    int32_t *pull_claim;   // per step n mod 3: grid-wide pull items past every warp's first claimed so far
     unsigned *barrier;     // persistent kernel: the arrival counter, the abort word
     unsigned long long *trace;  // N2B_TRACE builds: per step and block, %globaltimer at each phase (else unused)
     unsigned long long bar_limit_ns;  // persistent windows: a grid barrier wait gives up after this long
@@ -342,10 +343,12 @@ __device__ __forceinline__ void red_add_u64(long long *p, long long v) {
 // grid in runs of PULL_ITEM links (pull_far_phase).
 constexpr int PULL_CH = 512;                        // links per staging chunk
 constexpr int PULL_BUFS = 3;                        // chunks in flight per warp
-constexpr int PULL_ITEM = 2048;                     // links per item of the grid-wide pull (a multiple of PULL_CH)
+constexpr int PULL_ITEM = 1024;                     // links per item of the grid-wide pull (a multiple of PULL_CH)
 constexpr int RING_CACHE_MAX = 8192;                // words of pull sources' rings copied to shared memory, at most
 constexpr unsigned PULL_WAIT_POLLS = 1u << 22;      // polls of a chunk's mbarrier before it counts as lost
 constexpr int PULL_BATCH = 4;                       // batches whose link records are loaded together
+static_assert(PULL_BATCH == 4, "a whole group inside the open row: four links per lane, one 16-byte load");
+constexpr int PULL_SHORT_ROWS = 48;                 // in-step pull: rows this short on average, a lane per row
 
 // One warp's staging area in dynamic shared memory: this header, then PULL_BUFS chunks of link records and,
 // when the launch has a pull connection with per-link weights, PULL_BUFS chunks of weights.
@@ -404,6 +407,25 @@ __device__ __forceinline__ void pull_issue(PullStage *st, const ConnDev &C, int 
                      : "memory");
 }
 
+// Lane 0: the aligned range [a0, a1) (at most PULL_BUFS * PULL_CH links) into the stage's buffers taken as one,
+// completion on buffer 0's mbarrier.
+__device__ __forceinline__ void pull_issue_range(PullStage *st, const ConnDev &C, int a0, int a1) {
+    const uint32_t bytes = (uint32_t)(a1 - a0) * 4u;  // a multiple of 16
+    const uint32_t bar = smem_u32(&st->bar[0]);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                 "r"(C.homogeneous ? bytes : 2u * bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(stage_link(st, 0))),
+                 "l"(__cvta_generic_to_global(C.link + a0)), "r"(bytes), "r"(bar)
+                 : "memory");
+    if (!C.homogeneous)
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_u32(stage_w(st, 0))),
+                     "l"(__cvta_generic_to_global(C.w + a0)), "r"(bytes), "r"(bar)
+                     : "memory");
+}
+
 // Every lane: wait (bounded) until buffer b's chunk has landed; false if it did not within the limit. Polls with
 // the non-blocking mbarrier.test_wait.
 __device__ __forceinline__ bool pull_wait(PullStage *st, int b) {
@@ -449,6 +471,7 @@ struct PullPass {
 
     __device__ __forceinline__ void fold() {
         if (HOMOG) {
+            hits += (unsigned)lcnt;  // (single weight: the parts are the hits)
             csum += (long long)__reduce_add_sync(FULL, (unsigned)lcnt) * wfx;
             lcnt = 0;
         } else {
@@ -460,6 +483,24 @@ struct PullPass {
         }
     }
 
+    // A link of the open row into the lane's part.
+    __device__ __forceinline__ void add(unsigned hit, float w) {
+        if (HOMOG) {
+            lcnt += (int)hit;
+        } else {
+            hits += hit;
+            if (hit) lpart += weight_fx(w, wscale);
+        }
+    }
+
+    // One link of a whole group inside the open row.
+    __device__ __forceinline__ void open_link(uint32_t rec, float w) {
+        bool ok;
+        const uint32_t word = bits(rec, true, ok);
+        bad += (int)!ok;
+        add(ok ? (word >> (rec & 31u)) & 1u : 0u, w);
+    }
+
     // One batch (every lane of the warp): links [b, min(b + 32, r1)), the lane's link b + lane (`valid` below
     // r1) with its record, ring word and weight. emit(row, total) is called once per finished row, by one lane.
     template <class Emit>
@@ -468,12 +509,11 @@ struct PullPass {
         const int lane = threadIdx.x & 31;
         bad += (int)(valid && !ok);
         const unsigned hit = ok ? (word >> (rec & 31u)) & 1u : 0u;  // rec & 31 = s & 31
-        hits += hit;
         if (min(b + 32, r1) <= cend) {  // the whole batch in the open row
-            if (HOMOG) lcnt += (int)hit;
-            else if (hit) lpart += weight_fx(w, wscale);
+            add(hit, w);
             return;
         }
+        hits += hit;
         fold();
         int q = cq, end = cend;
         const int l = min(b + lane, r1 - 1);  // lanes past the batch's last link: that link
@@ -514,6 +554,24 @@ struct PullPass {
     __device__ __forceinline__ void run(const uint32_t *lk, const float *wk, int base, int r0, int r1, Emit &emit) {
         const int lane = threadIdx.x & 31;
         for (int b0 = r0; b0 < r1; b0 += 32 * PULL_BATCH) {
+            if (SMEM) {
+                // whole groups inside the open row: a lane takes four consecutive links per group (one 16-byte
+                // load: lk is 16-byte aligned and b0 - base a multiple of 4), the order within a row being free
+                const int lim = min(r1, cend);
+                if (b0 + 32 * PULL_BATCH <= lim) {
+                    for (; b0 + 32 * PULL_BATCH <= lim; b0 += 32 * PULL_BATCH) {
+                        const uint4 r4 = *reinterpret_cast<const uint4 *>(lk + (b0 - base) + 4 * lane);
+                        float4 w4 = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (!HOMOG) w4 = *reinterpret_cast<const float4 *>(wk + (b0 - base) + 4 * lane);
+                        open_link(r4.x, w4.x);
+                        open_link(r4.y, w4.y);
+                        open_link(r4.z, w4.z);
+                        open_link(r4.w, w4.w);
+                    }
+                    b0 -= 32 * PULL_BATCH;  // (the loop's increment)
+                    continue;
+                }
+            }
             uint32_t rec[PULL_BATCH], word[PULL_BATCH];
             float w[PULL_BATCH];
             bool ok[PULL_BATCH];
@@ -636,11 +694,71 @@ __device__ __forceinline__ void copy_ring(uint32_t *dst, const ConnDev &C, int f
     }
 }
 
+// The in-step pull over short rows: lane q sums row q alone (links [r0, r1) of C, in order, four loads in
+// flight), no exchange between lanes; lanes without a row pass r0 = r1. Links [a0, a1) are read from the
+// stage's buffers (st non-null: the warp's staged range), the others from C's arrays. Returns the row total.
+template <bool HOMOG, bool RING>
+__device__ __forceinline__ long long pull_lane_row(const ConnDev &C, const uint32_t *ring, int32_t *err,
+                                                   unsigned long long *events, int r0, int r1, long long n_read,
+                                                   PullStage *st, int a0, int a1) {
+    const uint32_t *slink = st ? stage_link(st, 0) : nullptr;
+    const float *sw = (st && !HOMOG) ? stage_w(st, 0) : nullptr;
+    PullPass<HOMOG, RING> p;  // (its ring lookup only)
+    p.ring = ring;
+    p.nlo = (int)n_read;
+    p.mask = C.src_bit_mask;
+    p.words = C.src_words;
+    p.src_n = C.src_n;
+    p.min_d = 1;
+    long long part = 0;
+    int cnt = 0, bad = 0;
+    unsigned hits = 0;
+    for (int l = r0; l < r1; l += 4) {
+        uint32_t rec[4], word[4];
+        float w[4];
+        bool ok[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int m = l + k;
+            const bool in_stage = slink != nullptr && m >= a0 && m < a1;
+            rec[k] = m < r1 ? (in_stage ? slink[m - a0] : __ldg(C.link + m)) : 0u;
+            w[k] = (!HOMOG && m < r1) ? (in_stage ? sw[m - a0] : __ldg(C.w + m)) : 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) word[k] = p.bits(rec[k], l + k < r1, ok[k]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            bad += (int)(l + k < r1 && !ok[k]);
+            const unsigned hit = ok[k] ? (word[k] >> (rec[k] & 31u)) & 1u : 0u;
+            hits += hit;
+            if (HOMOG) cnt += (int)hit;
+            else if (hit) part += weight_fx(w[k], C.wscale);
+        }
+    }
+    hits = __reduce_add_sync(FULL, hits);
+    bad = __reduce_add_sync(FULL, bad);
+    if ((threadIdx.x & 31) == 0) {
+        if (hits) atomicAdd(events, (unsigned long long)hits);
+        if (bad) atomicAdd(err + 1, bad);
+    }
+    return HOMOG ? (long long)cnt * C.wfx : part;
+}
+
+template <bool RING>
+__device__ __forceinline__ long long pull_lane_row_any(const ConnDev &C, const uint32_t *ring, int32_t *err,
+                                                       unsigned long long *events, int r0, int r1, long long n_read,
+                                                       PullStage *st, int a0, int a1) {
+    return C.homogeneous ? pull_lane_row<true, RING>(C, ring, err, events, r0, r1, n_read, st, a0, a1)
+                         : pull_lane_row<false, RING>(C, ring, err, events, r0, r1, n_read, st, a0, a1);
+}
+
 // The in-step pull of the tile's population (every thread of the block): each pull connection's rows of ptr --
 // all its links, or, with a split, its delay-1 links -- for the warp's 32 neurons, against ring rows n - d;
 // returns the lane's own neuron's total. A source whose whole ring fits the ring cache is copied there first:
 // with a split only ring row n - 1 (the delay-1 links' row), else the whole ring (its rows of steps before n are
-// final). The warp's row offsets are copied to its PullStage.
+// final). The warp's row offsets are copied to its PullStage; rows shorter than PULL_SHORT_ROWS links on
+// average are summed a lane per row (their links staged by one bulk copy, issued before the ring's copy), longer
+// ones swept by the whole warp (pull_pass).
 template <bool INL>
 __device__ __forceinline__ long long pull_intake(const StepArgs &a, const PopDev &P, int first, int count,
                                                  long long n, PullStage *stage) {
@@ -653,6 +771,24 @@ __device__ __forceinline__ long long pull_intake(const StepArgs &a, const PopDev
         const int ring_words = (C.src_bit_mask + 1) * C.src_words;
         const bool cached = ring_words <= a.ring_cache_words;  // the same for every thread of the block
         uint32_t *cache = ring_cache(a);
+        // (a network with pull connections always has its PullStages: the launch's dynamic shared memory)
+        int L0 = 0, L1 = 0, a0 = 0, a1 = 0;
+        bool short_rows = false, pre = false;
+        if (nq > 0) {
+            if (lane <= nq) stage->ptr[lane] = __ldg(C.ptr + wbase + lane);
+            if (lane == 0 && nq == 32) stage->ptr[32] = __ldg(C.ptr + wbase + 32);
+            stage->sum[lane] = 0;
+            __syncwarp();
+            L0 = stage->ptr[0];
+            L1 = stage->ptr[nq];
+            short_rows = L1 - L0 < PULL_SHORT_ROWS * nq;  // the same for every lane
+            // short rows: the warp's whole range (its aligned interior) in one copy, in flight under the ring's
+            a0 = (L0 + 3) & ~3;
+            a1 = L1 & ~3;
+            pre = short_rows && C.staged && a1 > a0 && a1 - a0 <= PULL_BUFS * PULL_CH &&
+                  !__shfl_sync(FULL, stage->broken, 0);
+            if (pre && lane == 0) pull_issue_range(stage, C, a0, a1);
+        }
         if (cached) {
             __syncthreads();  // every warp done with the cache's previous ring
             if (C.has_split)
@@ -662,23 +798,34 @@ __device__ __forceinline__ long long pull_intake(const StepArgs &a, const PopDev
             __syncthreads();
         }
         if (nq <= 0) continue;
-        // (a network with pull connections always has its PullStages: the launch's dynamic shared memory)
-        if (lane <= nq) stage->ptr[lane] = __ldg(C.ptr + wbase + lane);
-        if (lane == 0 && nq == 32) stage->ptr[32] = __ldg(C.ptr + wbase + 32);
-        stage->sum[lane] = 0;
-        __syncwarp();
-        const int L0 = stage->ptr[0], L1 = stage->ptr[nq];
-        if (L1 > L0) {  // the same for every lane
+        if (short_rows) {  // a lane per row
+            bool lost = false;
+            if (pre) {
+                lost = __any_sync(FULL, !pull_wait(stage, 0));  // the same in every lane
+                __syncwarp();
+                if (lane == 0) {
+                    stage->uses[0] += 1;
+                    if (lost) {
+                        atomicAdd(a.err + 5, 1);
+                        stage->broken = 1;
+                    }
+                }
+            }
+            PullStage *from = (pre && !lost) ? stage : nullptr;
+            const int r0 = lane < nq ? stage->ptr[lane] : 0, r1 = lane < nq ? stage->ptr[lane + 1] : 0;
+            mine += cached ? pull_lane_row_any<true>(C, cache, a.err, a.counters, r0, r1, n, from, a0, a1)
+                           : pull_lane_row_any<false>(C, C.src_bits, a.err, a.counters, r0, r1, n, from, a0, a1);
+        } else if (L1 > L0) {  // the warp sweeps the rows together
             auto emit = [&](int q, long long v) { stage->sum[q] = v; };  // q: the warp's row, below nq
             if (cached)
                 pull_pass_any<true>(C, cache, stage, a.err, a.counters, stage->ptr, 0, nq, L0, L1, n, 1, emit);
             else
                 pull_pass_any<false>(C, C.src_bits, stage, a.err, a.counters, stage->ptr, 0, nq, L0, L1, n, 1,
                                      emit);
+            __syncwarp();
+            mine += stage->sum[lane];
         }
-        __syncwarp();
-        mine += stage->sum[lane];
-        __syncwarp();
+        __syncwarp();  // every lane done with the stage before its next use
     }
     return lane < nq ? mine : 0;
 }
@@ -687,7 +834,8 @@ __device__ __forceinline__ long long pull_intake(const StepArgs &a, const PopDev
 // split pull connection, for the arrival slot of step n + 1 -- ring rows (n + 1) - d, d >= 2, all written
 // before this step -- in items of PULL_ITEM links (item k of a connection: its links [PULL_ITEM (k0 + k),
 // PULL_ITEM (k0 + k + 1)) within the delay >= 2 region, k0 = far0 / PULL_ITEM; its first row in item_row[k]),
-// warps taking items grid-stride. Each row an item finishes is added to its slot with one reduction (slot n + 1
+// every warp taking item (its index in the grid) first, then the step's next unclaimed one until none is left
+// (blocks whose tiles took longer take fewer). Each row an item finishes is added to its slot with one reduction (slot n + 1
 // is read after the step's barrier). With every pull source's ring in the cache together, the block copies them
 // all first.
 template <int NPB, bool INL>
@@ -704,14 +852,18 @@ __device__ __forceinline__ void pull_far_phase(const StepArgs &a, const long lon
         __syncthreads();
     }
     const int W = (int)gridDim.x * (NPB / 32);
+    int *claim = a.pull_claim + (int)(n % 3);
     int c = 0;
-    for (int it = (int)blockIdx.x * (NPB / 32) + (int)(threadIdx.x >> 5); it < a.pull_items; it += W) {
+    for (int it = (int)blockIdx.x * (NPB / 32) + (int)(threadIdx.x >> 5); it < a.pull_items;) {
+        int next = 0;
+        if ((threadIdx.x & 31) == 0) next = W + atomicAdd(claim, 1);  // the warp's next item, in flight under this one
         while (c + 1 < a.n_pull && !(it >= pull_at<INL>(a, c).item0 &&
                                      it < pull_at<INL>(a, c).item0 + pull_at<INL>(a, c).n_items))
-            ++c;  // items rise with the connection index: the search moves forward only
+            ++c;  // a warp's items rise, and with them the connection index: the search moves forward only
         const ConnDev &C = pull_at<INL>(a, c);
         const int k = it - C.item0, k0 = C.far0 / PULL_ITEM;
         const int L0 = max(C.far0, (k0 + k) * PULL_ITEM), L1 = min(C.n_links, (k0 + k + 1) * PULL_ITEM);
+        it = __shfl_sync(FULL, next, 0);
         if (L1 <= L0) continue;
         long long *slot = C.tgt_acc + (size_t)((n + 1) & C.tgt_acc_mask) * (size_t)C.tgt_n;
         auto emit = [&](int q, long long v) {
@@ -1199,6 +1351,7 @@ __device__ __forceinline__ void step_body(const StepArgs &a, const long long n, 
         atomicExch(a.item_count + (int)((n + 1) % 3), 0);
         atomicExch(a.tile_claim + (int)((n + 1) % 3), 0);
         atomicExch(a.tile_claim + 3 + (int)((n + 1) % 3), 0);
+        atomicExch(a.pull_claim + (int)((n + 1) % 3), 0);
     }
     // tile blockIdx.x first (a persistent launch holds it in registers); with fewer blocks than tiles, the
     // tiles past the first gridDim.x are claimed one at a time from the step's counter, so that blocks whose
@@ -1228,6 +1381,7 @@ __device__ __forceinline__ void step_body(const StepArgs &a, const long long n, 
     }
     N2B_STAMP(a, k, 2);
     far_phase<NPB, INL, FG>(a, n, s_conn, far_n);
+    N2B_STAMP(a, k, 5);
     if (PULL) pull_far_phase<NPB, INL>(a, n, stage);
     N2B_STAMP(a, k, 3);
 }
@@ -1347,7 +1501,7 @@ __global__ void zero_kernel(int32_t *err, int n_err, unsigned long long *counter
 }
 __global__ void set_step_kernel(long long *step, long long value, int32_t *item_count) {
     *step = value;
-    for (int k = 0; k < 9; ++k) item_count[k] = 0;  // list lengths, tile counters, far-chunk counters
+    for (int k = 0; k < 12; ++k) item_count[k] = 0;  // list lengths, tile, far-chunk and pull-item counters
 }
 
 }  // namespace n2b

@@ -95,7 +95,7 @@ Layout layout(const n2b_population *pops, int32_t n_pops, const n2b_connection *
     L.rec0 = o; o = align256(o + sizeof(long long));
     L.err = o; o = align256(o + sizeof(int32_t) * N2B_ERR_WORDS);
     L.counters = o; o = align256(o + sizeof(unsigned long long) * (2 + std::max(n_pops, 1)));
-    L.item_count = o; o = align256(o + sizeof(int32_t) * 9);  // list lengths, tile and far-chunk counters
+    L.item_count = o; o = align256(o + sizeof(int32_t) * 12);  // list lengths, tile, far-chunk, pull counters
     L.items = o; o = align256(o + sizeof(int4) * 3 * (size_t)L.item_cap);
     L.barrier = o; o = align256(o + sizeof(unsigned) * n2b::BAR_WORDS);
     L.pull_rows = o; o = align256(o + sizeof(int32_t) * (size_t)std::max<int64_t>(item_rows, 1));
@@ -452,6 +452,8 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     }
     if (persistent) {
         if (most < 1) return fail(N2B_ECUDA, "the persistent kernel cannot be resident");
+        // a grid-wide pull is spread over every warp of the launch: by default as many blocks as can be resident
+        if (pull_items > 0 && !(opt && opt->grid > 0)) want = most;
         grid = std::min(std::min(want, most), n2b::BAR_MAX_BLOCKS);
         grid = std::max(grid, 1);
     }
@@ -478,6 +480,7 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     a.items = reinterpret_cast<int4 *>(ws + L.items);
     a.item_count = reinterpret_cast<int32_t *>(ws + L.item_count);
     a.tile_claim = a.item_count + 3;
+    a.pull_claim = a.item_count + 9;
     a.item_cap = L.item_cap;
     a.n_tiles = L.n_tiles;
     a.offset = 0;
