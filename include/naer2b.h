@@ -103,9 +103,9 @@ typedef struct n2b_population {
  *   link array holding every link of delay >= 2 steps (split[0] >= ptr[n_tgt]):
  *   ptr's rows then hold only delay-1 links, pulled by the target's block in the
  *   step; split's rows are pulled one step ahead (at step n for the slot of step
- *   n + 1), 32 targets per warp, by every block, each target's sum added to its
- *   arrival slot with one reduction. NULL: ptr's rows hold every link, all
- *   pulled by the target's block in the step. */
+ *   n + 1) by every warp of the launch in runs of 1024 links, each row's sum of a
+ *   run added to its arrival slot with one reduction. NULL: ptr's rows hold every
+ *   link, all pulled by the target's block in the step. */
 typedef struct n2b_connection {
     int32_t src;
     int32_t tgt;
@@ -124,8 +124,9 @@ typedef struct n2b_options {
     int32_t device;  /* CUDA device ordinal of every pointer */
     int32_t grid;    /* blocks per launch (0: per-step launches two per SM and at least one per tile;
                         persistent one per SM, at least tiles + half an SM's worth, at most the co-resident
-                        blocks, each looping over its tiles; persistent with a split pull connection: every
-                        co-resident block, which all share its delay >= 2 rows) */
+                        blocks, each looping over its tiles; persistent with a split pull connection or with
+                        more tiles than two blocks per SM hold (the three-per-SM kernel): every co-resident
+                        block) */
     int32_t persistent; /* 1: a window of steps is one cooperative launch, steps separated by a grid
                            barrier; 0: one launch per step */
     int32_t reserved;

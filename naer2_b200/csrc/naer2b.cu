@@ -452,8 +452,10 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     }
     if (persistent) {
         if (most < 1) return fail(N2B_ECUDA, "the persistent kernel cannot be resident");
-        // a grid-wide pull is spread over every warp of the launch: by default as many blocks as can be resident
-        if (pull_items > 0 && !(opt && opt->grid > 0)) want = most;
+        // a grid-wide pull is spread over every warp of the launch, and the dense kernel's tile-free blocks take
+        // the far items (PD14: 7.17 us per step at 444 blocks against 7.65 at 379): by default as many blocks
+        // as can be resident
+        if ((pull_items > 0 || dense) && !(opt && opt->grid > 0)) want = most;
         grid = std::min(std::min(want, most), n2b::BAR_MAX_BLOCKS);
         grid = std::max(grid, 1);
     }
