@@ -76,6 +76,19 @@ def test_short_and_empty_rows_all_pull_match_oracle(cuda, persistent):
     assert net.runtime.status()[_lib.ERR_PULL_STAGE] == 0
 
 
+@pytest.mark.parametrize("persistent", [True, False], ids=["persistent", "per-step"])
+@pytest.mark.parametrize("grid", [1, 5, 37])
+def test_grid_wide_pull_on_any_grid_matches_oracle(cuda, grid, persistent):
+    """The delay >= 2 rows' items claimed by however many warps the launch has (one block: its eight warps take
+    all 59+ items of the weighted connection in turn): the oracle's rasters and state for any grid."""
+    net = sparse_rows_net(seed=32)
+    net.grid = grid
+    gr, orr, gs, os_, cnt, ev = run_both(net, 300, modes=all_pull(net), persistent=persistent)
+    assert net.runtime.opt.grid == grid
+    assert sum(r.sum() for r in gr[2:]) > 300
+    assert_identical(gr, orr, gs, os_)
+
+
 def test_unaligned_rows_walk_and_match_the_staged_path(cuda):
     """The same pull network twice through the C ABI: once as built (16-byte aligned rows: staged), once with
     every pull connection's link and weight arrays moved to an address 4 bytes past a 16-byte boundary (not
