@@ -1442,7 +1442,9 @@ __device__ __forceinline__ bool grid_sync(const StepArgs &a, unsigned k) {
             // acquire polls (measured: relaxed polls with one fence.acq_rel at the end cost ~0.4-0.9 us more per
             // step, the fence being the slower)
             if ((int)(ld_acquire(bar + BAR_COUNT) - target) >= 0) break;
-            if (*(volatile unsigned *)(bar + BAR_ABORT)) { ok = 0; break; }
+            // the abort word every 16th poll (a load after the acquire waits for it: reading it on every poll
+            // would double the poll's round trip); it is only set by a wait that gave up
+            if ((spin & 15) == 15 && *(volatile unsigned *)(bar + BAR_ABORT)) { ok = 0; break; }
             if (spin == 0) t0 = globaltimer();
             else if (globaltimer() - t0 > a.bar_limit_ns) {
                 atomicExch(bar + BAR_ABORT, 1u);
