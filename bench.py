@@ -547,7 +547,8 @@ def _summarise_choices(choices: list) -> dict | None:
         return None
     out = {}
     for c in choices:
-        key = f"block {c['block']}, {'persistent' if c['persistent'] else 'per-step'}, pull {c['pull']}"
+        grid = "default grid" if not c.get("grid") else "every co-resident block" if c["grid"] >= 1 << 16 else f"grid {c['grid']}"
+        key = f"block {c['block']}, {'persistent' if c['persistent'] else 'per-step'}, {grid}, pull {c['pull']}"
         out[key] = out.get(key, 0) + 1
     return out
 

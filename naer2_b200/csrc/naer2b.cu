@@ -352,7 +352,8 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
     // the pull: a PullStage per warp in dynamic shared memory when the network has pull connections, and after
     // them a ring cache -- for the largest pull source's spike-bit ring (the in-step pull, one connection at a
     // time) and, when they fit together, every split connection's source ring at its ring_off (the grid-wide
-    // pull), up to RING_CACHE_MAX words; the grid-wide pull's items, 32 targets each, numbered by connection
+    // pull), up to RING_CACHE_MAX words; the grid-wide pull's items, PULL_ITEM links each, numbered by
+    // connection, their first rows found by a set-up kernel
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     char *ws = static_cast<char *>(workspace);
     // a split pull connection's first delay >= 2 link (read back once) and its items of PULL_ITEM links
@@ -623,7 +624,7 @@ int n2b_reset_counters(n2b_net *net, void *stream) {
 
 #ifdef N2B_TRACE
 // Trace builds only (not part of the C ABI): phase stamps of the next persistent window's first `steps` steps
-// into trace[steps][grid][6] (device memory).
+// into trace[steps][grid][TRACE_PHASES] (device memory).
 int n2b_trace(n2b_net *net, unsigned long long *trace, int32_t steps, int32_t *grid) {
     if (!net) return fail(N2B_EINVAL, "net is NULL");
     net->args.trace = trace;

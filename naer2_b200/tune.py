@@ -1,7 +1,8 @@
 """The autotuner: picks a network's launch configuration by measuring it.
 
 Candidates differ in neurons per block (128 / 256), in how a window is launched (one persistent cooperative
-launch, or one launch per step), in the grid, and in push or pull per connection. The push/pull split comes
+launch, or one launch per step), in the grid (the library's default, or every co-resident block for a
+persistent launch: RESIDENT), and in push or pull per connection. The push/pull split comes
 from a cost model fitted on a short all-push run: per connection, push moves (spikes of its source per step)
 x (its mean row length) link words, scattered into the target's arrival slots, while pull streams every one
 of its links every step against the source's spike bits; pull is a candidate for the connections where its
@@ -77,8 +78,11 @@ def pull_candidates(net, spikes_per_step: list, pull_factor: float = 4.0) -> dic
     return out
 
 
+RESIDENT = 1 << 16  # a persistent launch's grid is capped at the co-resident blocks: this asks for all of them
+
+
 def autotune(net, steps: int = 300, warmup: int = 100, blocks=(128, 256), persistent=(True, False),
-             grids=(None,), pull_factor: float = 4.0, verbose: bool = False) -> dict:
+             grids=(None, RESIDENT), pull_factor: float = 4.0, verbose: bool = False) -> dict:
     """Measure the candidates, keep the fastest; returns the report (every trial's us per step)."""
     if net.device is None or net.device.type != "cuda":
         raise RuntimeError("autotune needs the network on a CUDA device")
@@ -102,7 +106,7 @@ def autotune(net, steps: int = 300, warmup: int = 100, blocks=(128, 256), persis
         # pull sets also try 64-neuron tiles: a pulled row is walked by its tile's warps, so smaller tiles spread
         # the pulls over more SMs
         cands = [(b, g, p, m) for m in mode_sets for b in (tuple(blocks) + ((64,) if m and 64 not in blocks else ()))
-                 for g in grids for p in persistent]
+                 for g in grids for p in persistent if p or g != RESIDENT]  # (per-step launches: not RESIDENT)
         for block, grid, pers, modes in cands:
             if (block, grid, pers, len(modes)) == (256, None, True, 0):
                 continue
