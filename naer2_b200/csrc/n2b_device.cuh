@@ -452,7 +452,7 @@ template <bool HOMOG, bool RING>
 struct PullPass {
     const uint32_t *ring;  // the source's spike-bit ring (shared-memory copy or global)
     const int32_t *rows;   // row offsets (global, or the warp's copy in shared memory)
-    int nlo, mask, words, src_n, min_d, qmax;
+    int nlo, mask, words, src_n, min_d, dspan, qmax;
     long long wfx;
     float wscale;
     int cq, cend;     // the open row and its end
@@ -464,7 +464,8 @@ struct PullPass {
 
     __device__ __forceinline__ uint32_t bits(uint32_t rec, bool valid, bool &ok) const {
         const int d = (int)(rec >> 24), s = (int)(rec & 0xFFFFFFu);
-        ok = valid && d >= min_d && d <= mask && s < src_n;
+        // min_d <= d <= mask as one unsigned compare (dspan = mask - min_d; min_d 256 when no delay fits)
+        ok = valid && (unsigned)(d - min_d) <= (unsigned)dspan && s < src_n;
         const int at = ((nlo - d) & mask) * words + (s >> 5);
         return ok ? (RING ? ring[at] : __ldcg(ring + at)) : 0u;
     }
@@ -496,9 +497,9 @@ struct PullPass {
     // One link of a whole group inside the open row.
     __device__ __forceinline__ void open_link(uint32_t rec, float w) {
         bool ok;
-        const uint32_t word = bits(rec, true, ok);
+        const uint32_t word = bits(rec, true, ok);  // 0 when the link is out of range
         bad += (int)!ok;
-        add(ok ? (word >> (rec & 31u)) & 1u : 0u, w);
+        add((word >> (rec & 31u)) & 1u, w);
     }
 
     // One batch (every lane of the warp): links [b, min(b + 32, r1)), the lane's link b + lane (`valid` below
@@ -610,7 +611,8 @@ __device__ __forceinline__ void pull_pass(const ConnDev &C, const uint32_t *ring
     p.mask = C.src_bit_mask;
     p.words = C.src_words;
     p.src_n = C.src_n;
-    p.min_d = min_d;
+    p.min_d = C.src_bit_mask >= min_d ? min_d : 256;  // (no 8-bit delay is 256 or more)
+    p.dspan = C.src_bit_mask >= min_d ? C.src_bit_mask - min_d : 0;
     p.qmax = qmax;
     p.wfx = C.wfx;
     p.wscale = C.wscale;
@@ -709,7 +711,8 @@ __device__ __forceinline__ long long pull_lane_row(const ConnDev &C, const uint3
     p.mask = C.src_bit_mask;
     p.words = C.src_words;
     p.src_n = C.src_n;
-    p.min_d = 1;
+    p.min_d = C.src_bit_mask >= 1 ? 1 : 256;
+    p.dspan = C.src_bit_mask >= 1 ? C.src_bit_mask - 1 : 0;
     long long part = 0;
     int cnt = 0, bad = 0;
     unsigned hits = 0;
