@@ -302,6 +302,17 @@ int n2b_jit_compile(const char *source, const char *kernel_name, const char *con
 int n2b_jit_launch(n2b_jit_kernel *k, uint32_t grid, uint32_t block, const void *params, size_t params_bytes,
                    void *stream);
 
+/* A window of steps of a transpiled network in one call (the per-step loop of
+ * naer2/network.py:80-152 over the populations' generated kernels): for each
+ * step n = step0 .. step0 + n_steps - 1, and in it each kernel k in order, one
+ * launch of kernels[k] (grids[k] x blocks[k] threads; grid 0: skipped) with a
+ * copy of params[k] (params_bytes[k] >= 32) whose leading fields are set for
+ * the step: the int64 step at offset 0 = n, the fp32 t at offset 24 =
+ * (n + 1) dt and t0 at offset 28 = n dt, each rounded from double. */
+int n2b_jit_launch_window(n2b_jit_kernel *const *kernels, const uint32_t *grids, const uint32_t *blocks,
+                          const void *const *params, const size_t *params_bytes, int32_t n_kernels, int64_t step0,
+                          int64_t n_steps, double dt, void *stream);
+
 /* Unload the kernel. */
 int n2b_jit_destroy(n2b_jit_kernel *k);
 

@@ -89,6 +89,8 @@ SIGNATURES = {
     "n2b_jit_compile": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_char_p),
                                        ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(_P)]),
     "n2b_jit_launch": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32, _P, ctypes.c_size_t, _P]),
+    "n2b_jit_launch_window": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64,
+                                             ctypes.c_double, _P]),
     "n2b_jit_destroy": (ctypes.c_int, [_P]),
     "n2b_run_static": (ctypes.c_int, [ctypes.POINTER(Population), ctypes.c_int32, ctypes.POINTER(Connection),
                                       ctypes.c_int32, ctypes.POINTER(Options), ctypes.c_int64, ctypes.c_int64,

@@ -9,6 +9,7 @@
 #include <dlfcn.h>
 #include <nvrtc.h>
 
+#include <cstring>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -153,6 +154,41 @@ int n2b_jit_launch(n2b_jit_kernel *k, uint32_t grid, uint32_t block, const void 
         void *args[] = {const_cast<void *>(params)};
         e = cudaLaunchKernel(reinterpret_cast<const void *>(k->kernel), dim3(grid), dim3(block), args, 0,
                              reinterpret_cast<cudaStream_t>(stream));
+    }
+    if (e != cudaSuccess) return n2b_host::set_error(N2B_ECUDA, std::string("launch: ") + cudaGetErrorString(e));
+    return N2B_OK;
+}
+
+int n2b_jit_launch_window(n2b_jit_kernel *const *kernels, const uint32_t *grids, const uint32_t *blocks,
+                          const void *const *params, const size_t *params_bytes, int32_t n_kernels, int64_t step0,
+                          int64_t n_steps, double dt, void *stream) {
+    if (n_kernels < 0 || n_steps < 0 || (n_kernels > 0 && (!kernels || !grids || !blocks || !params || !params_bytes)))
+        return n2b_host::set_error(N2B_EINVAL, "bad arguments");
+    std::vector<std::vector<unsigned char>> copy(n_kernels);
+    for (int32_t k = 0; k < n_kernels; ++k) {
+        if (!kernels[k] || !params[k] || params_bytes[k] < 32 || blocks[k] == 0 || blocks[k] > 1024)
+            return n2b_host::set_error(N2B_EINVAL, "bad kernel " + std::to_string(k));
+        if (kernels[k]->device != kernels[0]->device)
+            return n2b_host::set_error(N2B_EINVAL, "the kernels are loaded on different devices");
+        copy[k].assign(static_cast<const unsigned char *>(params[k]),
+                       static_cast<const unsigned char *>(params[k]) + params_bytes[k]);
+    }
+    if (n_kernels == 0 || n_steps == 0) return N2B_OK;
+    JitDeviceGuard guard;
+    cudaError_t e = cudaSetDevice(kernels[0]->device);
+    for (int64_t s = 0; e == cudaSuccess && s < n_steps; ++s) {
+        const int64_t n = step0 + s;
+        const float t = (float)((double)(n + 1) * dt), t0 = (float)((double)n * dt);
+        for (int32_t k = 0; e == cudaSuccess && k < n_kernels; ++k) {
+            if (grids[k] == 0) continue;
+            unsigned char *P = copy[k].data();
+            std::memcpy(P, &n, sizeof(n));
+            std::memcpy(P + 24, &t, sizeof(t));
+            std::memcpy(P + 28, &t0, sizeof(t0));
+            void *args[] = {P};  // (the launch copies the parameter block)
+            e = cudaLaunchKernel(reinterpret_cast<const void *>(kernels[k]->kernel), dim3(grids[k]), dim3(blocks[k]),
+                                 args, 0, reinterpret_cast<cudaStream_t>(stream));
+        }
     }
     if (e != cudaSuccess) return n2b_host::set_error(N2B_ECUDA, std::string("launch: ") + cudaGetErrorString(e));
     return N2B_OK;

@@ -283,21 +283,31 @@ class JitRuntime:
     # ------------------------------------------------------------------ stepping
 
     def advance(self, n_steps: int) -> None:
+        """Steps step_count .. step_count + n_steps - 1: per step one launch per population, in order, the whole
+        window in one library call (n2b_jit_launch_window writes each launch's step and times)."""
         lib = _lib.load()
+        n_steps = int(n_steps)
+        if n_steps <= 0:
+            return
         self.stream.wait_stream(torch.cuda.current_stream(self.device))
         step = self.net.step_count
-        for k in range(int(n_steps)):
-            n = step + k
-            for kern, P, p in zip(self.kernels, self.params, self.pops):
-                P.step, P.t, P.t0 = n, (n + 1) * self.dt, n * self.dt
-                per = BLOCK if self.exact else NPB_C  # neurons per block (clocked: SCAN threads each)
-                size = len(p.shape)
-                grid = (size + per - 1) // per
-                if grid:
-                    threads = BLOCK if self.exact else scan(size) * NPB_C
-                    _lib.check(lib.n2b_jit_launch(kern, grid, threads, ctypes.byref(P), ctypes.sizeof(P), self._s),
-                               "n2b_jit_launch")
-                    self.launches += 1
+        k = len(self.kernels)
+        grids, blocks = (ctypes.c_uint32 * k)(), (ctypes.c_uint32 * k)()
+        kerns, params, sizes = (ctypes.c_void_p * k)(), (ctypes.c_void_p * k)(), (ctypes.c_size_t * k)()
+        for i, (kern, P, p) in enumerate(zip(self.kernels, self.params, self.pops)):
+            per = BLOCK if self.exact else NPB_C  # neurons per block (clocked: SCAN threads each)
+            size = len(p.shape)
+            grids[i] = (size + per - 1) // per
+            blocks[i] = BLOCK if self.exact else scan(size) * NPB_C
+            kerns[i] = kern.value
+            params[i] = ctypes.addressof(P)
+            sizes[i] = ctypes.sizeof(P)
+        _lib.check(lib.n2b_jit_launch_window(kerns, grids, blocks, params, sizes, k, step, n_steps, self.dt,
+                                             self._s), "n2b_jit_launch_window")
+        last = step + n_steps - 1
+        for P in self.params:  # (the fields as the last launch had them)
+            P.step, P.t, P.t0 = last, (last + 1) * self.dt, last * self.dt
+        self.launches += n_steps * sum(1 for g in grids if g)
         torch.cuda.current_stream(self.device).wait_stream(self.stream)
 
     def start_recording(self, steps: int) -> None:
