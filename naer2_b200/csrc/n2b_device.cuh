@@ -26,8 +26,8 @@
 //      never the slot this step reads;
 //   6. the grid-wide pull: the delay >= 2 links of split pull connections,
 //      gathered one step ahead for slot n + 1 (ring rows of steps <= n - 1),
-//      32 targets per warp over every warp of the grid, one reduction per
-//      target.
+//      in runs of PULL_ITEM links claimed by every warp of the grid, one
+//      reduction per row a run finishes.
 // Integer adds make every interleaving give the same sums. A step's slot is
 // complete when it is read: the previous step ended (launch boundary or grid
 // barrier) after every add into it.
