@@ -849,8 +849,10 @@ __device__ __forceinline__ void pull_far_phase(const StepArgs &a, const long lon
         __syncthreads();
         for (int c = 0; c < a.n_pull; ++c) {
             const ConnDev &C = pull_at<INL>(a, c);
-            if (C.n_items > 0 && C.ring_off >= 0)
-                copy_ring(cache + C.ring_off, C, 0, (C.src_bit_mask + 1) * C.src_words);
+            bool first = C.n_items > 0 && C.ring_off >= 0;  // connections of one source share its copy
+            for (int e = 0; first && e < c; ++e)
+                first = !(pull_at<INL>(a, e).n_items > 0 && pull_at<INL>(a, e).ring_off == C.ring_off);
+            if (first) copy_ring(cache + C.ring_off, C, 0, (C.src_bit_mask + 1) * C.src_words);
         }
         __syncthreads();
     }

@@ -371,8 +371,12 @@ int n2b_create(const n2b_population *pops, int32_t n_pops, const n2b_connection 
         if (C.has_split) {
             if (far0[c] < 0 || far0[c] > C.n_links)
                 return fail(N2B_EINVAL, "a pull connection's split offsets lie outside its links");
-            C.ring_off = total_ring;
-            total_ring += w;
+            for (size_t e = 0; e < c && C.ring_off < 0; ++e)  // a source ring already in the cache is shared
+                if (pull[e].has_split && pull[e].src_bits == C.src_bits) C.ring_off = pull[e].ring_off;
+            if (C.ring_off < 0) {
+                C.ring_off = total_ring;
+                total_ring += w;
+            }
             C.far0 = far0[c];
             C.item0 = pull_items;
             C.n_items = (C.tgt_n > 0 && far0[c] < C.n_links)
